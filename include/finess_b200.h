@@ -1,0 +1,152 @@
+/*
+ * finess_b200.h -- C ABI of the B200 (sm_100a) implementation of FINESS's
+ * 2D finite-difference WENO right-hand side and time steppers.
+ *
+ * Every entry point is extern "C", takes plain pointers and sizes, returns an
+ * int status (FIN_OK == 0) and never exits the process.  The C++ relink shim
+ * (finess_b200/csrc/shim/finess_relink.cpp) maps these statuses back onto the
+ * reference's own conventions (printf + exit(1), std::logic_error).
+ *
+ * Array layout at this boundary is the reference's own dTensorBC3 layout
+ * (lib/tensors.h:267-273, lib/tensors.cpp:650-667): a ghosted array
+ *   q(i, j, m),  i = 1-mbc .. mx+mbc,  j = 1-mbc .. my+mbc,  m = 1 .. meqn,
+ * stored with m fastest and i slowest:
+ *   idx = ((i+mbc-1)*(my+2*mbc) + (j+mbc-1))*meqn + (m-1).
+ * "host" entry points take host pointers (pageable or pinned) in that layout;
+ * "_dev" entry points take device pointers in the device layout described
+ * with fin_device_layout().
+ */
+#ifndef FINESS_B200_H
+#define FINESS_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define FIN_ABI_VERSION 1
+
+/* ---- status codes ---------------------------------------------------- */
+enum {
+    FIN_OK = 0,
+    FIN_ERR_ARG = 1,          /* bad argument / unsupported parameter combination */
+    FIN_ERR_CUDA = 2,         /* a CUDA runtime call failed (see fin_last_error) */
+    FIN_ERR_NO_DEVICE = 3,    /* no sm_100 device visible */
+    FIN_ERR_NSTEPS = 4,       /* more than nv steps in one frame (FinSolveRK.cpp:84-92) */
+    FIN_ERR_DT_BOUNDS = 5,    /* dt > max_dt (GetCFL.cpp:43-48) */
+    FIN_ERR_CFL_BOUNDS = 6,   /* cfl > 1e8 (GetCFL.cpp:61-66) */
+    FIN_ERR_NONFINITE = 7,    /* NaN/Inf met in a wave speed or the state */
+    FIN_ERR_UNSUPPORTED = 8,  /* valid in the reference, not built here */
+    FIN_ERR_SIZE = 9          /* a size beyond a documented maximum */
+};
+
+/* ---- enumerations (numeric values follow the reference's enum order) -- */
+enum fin_weno_version { FIN_WENO_FD = 0, FIN_WENO_JS = 1, FIN_WENO_Z = 2 };
+enum fin_time_stepping { FIN_TS_RK = 0, FIN_TS_LXW = 2, FIN_TS_MD = 3 };
+enum fin_bc { FIN_BC_PERIODIC = 0, FIN_BC_TRANSMISSIVE = 1 };
+enum fin_physics { FIN_PHYS_EULER = 0 };
+enum fin_precision {
+    FIN_PREC_FP64 = 0,     /* plain method, FP64 everywhere (the parity form) */
+    FIN_PREC_FP32 = 1,     /* FP32 reconstruction/splitting/projection, FP64 state */
+    FIN_PREC_HYBRID = 2    /* FP32 bulk + troubled-cell indicator: linear FD5 on smooth cells */
+};
+
+/* Parameters of one problem: the fields of parameters.ini that the
+ * reference's hot path reads (python/finess/params/{finess,dim2,weno,euler}.py). */
+typedef struct fin_params {
+    /* [finess] */
+    int meqn, maux;
+    int space_order, time_order;
+    int time_stepping_method;      /* enum fin_time_stepping */
+    int global_alpha, source_term;
+    int nv, verbosity;
+    double initial_dt, max_dt, max_cfl, desired_cfl;
+    /* [grid] */
+    int mx, my, mbc;
+    double xlow, xhigh, ylow, yhigh;
+    /* [weno] */
+    int weno_version;              /* enum fin_weno_version */
+    double epsilon, power_param, alpha_scaling;
+    /* [euler] */
+    double gamma;
+    /* boundary conditions applied as an index remap (the apps' SetBndValues) */
+    int bc_xlow, bc_xhigh, bc_ylow, bc_yhigh;  /* enum fin_bc */
+    /* this library */
+    int physics;                   /* enum fin_physics */
+    int precision;                 /* enum fin_precision */
+} fin_params;
+
+/* Defaults of python/finess/params/finess.py, weno.py and euler.py. */
+void fin_params_default(fin_params* p);
+
+/* Last error message of the calling thread (never NULL). */
+const char* fin_last_error(void);
+
+/* ABI version of the loaded library (FIN_ABI_VERSION it was built with). */
+int fin_abi_version(void);
+
+/* ---- solver handle ---------------------------------------------------- */
+typedef struct fin_solver fin_solver;
+
+/* Allocates the device state for one problem on the current CUDA device.
+ * Replaces the StateVars/dTensorBC3 allocations of FinSolveRK.cpp:44-70. */
+int fin_create(const fin_params* p, fin_solver** out);
+int fin_destroy(fin_solver* s);
+
+/* Copies a host state (reference ghosted layout, interior used) to the device
+ * and sets t.  Replaces StateVars construction + QinitFunc sampling. */
+int fin_set_state(fin_solver* s, const double* q_host, double t);
+/* Copies the device state back (interior written; ghosts filled by the BC
+ * remap, as SetBndValues would). */
+int fin_get_state(fin_solver* s, double* q_host, double* t);
+
+/* ConstructL (lib/2d/ConstructL.cpp:13-408) on a host state.
+ *   q_host:  ghosted input state (only interior cells read; ghosts come
+ *            from the BC remap, i.e. SetBndValues is applied first);
+ *   L_host:  ghosted output, interior written, ghosts untouched
+ *            (the reference leaves them uninitialised);
+ *   smax_host: optional (may be NULL), ghosted (mx+1, my+1, 2) array that
+ *            is max-accumulated exactly as ConstructL.cpp:173,324 do.
+ * GlobalWaveSpd (lib/2d/GlobalWaveSpd.cpp:20-80) runs first when
+ * global_alpha is set. */
+int fin_construct_l(fin_solver* s, const double* q_host, double* L_host, double* smax_host);
+
+/* GlobalWaveSpd (lib/2d/GlobalWaveSpd.cpp:20-80) on a host state. */
+int fin_global_wave_spd(fin_solver* s, const double* q_host, double* alpha1, double* alpha2);
+
+/* FinSolveRK / FinSolveMD / FinSolveLxW on the device state, advancing it
+ * from its t to tend (lib/2d/FinSolveRK.cpp:13-371, FinSolveMD.cpp:21-291,
+ * FinSolveLxW.cpp:16-245).  dtv[1] is the starting dt and receives the next
+ * dt; dtv[2] is max_dt (lib/2d/RunFinpack.cpp:62-63).  dtv has >= 3 entries.
+ * nsteps_out (may be NULL) receives the number of accepted steps. */
+int fin_solve(fin_solver* s, double tend, double* dtv, int* nsteps_out);
+
+/* One time step of exactly dt with no CFL control (benchmarking and
+ * per-step parity); cfl_out (may be NULL) receives GetCFL's value for it. */
+int fin_step_fixed(fin_solver* s, double dt, double* cfl_out);
+
+/* Per-component totals sum(dx*dy*q) over interior cells, accumulated in FP64
+ * with compensated summation (lib/2d/ConSoln.cpp:52-64). totals[meqn]. */
+int fin_conservation_totals(fin_solver* s, double* totals);
+
+/* Device timing of the last fin_solve/fin_step_fixed call: milliseconds
+ * spent in the stage kernels, measured with CUDA events on the solver's stream. */
+int fin_last_kernel_ms(fin_solver* s, double* ms);
+
+/* Counts of kernel launches issued by this solver since creation. */
+int fin_launch_count(fin_solver* s, long long* launches);
+
+/* ---- device-resident interface ---------------------------------------- */
+/* The device keeps each component as its own plane of mx*my values,
+ * j (y) fastest then i (x): plane m starts at m*plane_stride elements. */
+int fin_device_layout(fin_solver* s, size_t* plane_stride, size_t* row_stride);
+/* Device pointer to the solver's current state planes (FP64). */
+int fin_state_device_ptr(fin_solver* s, double** q_dev);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* FINESS_B200_H */

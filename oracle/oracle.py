@@ -1,0 +1,184 @@
+"""ctypes front end of the two CPU checkers.  TEST INFRASTRUCTURE ONLY.
+
+* ``Oracle``: oracle/liboracle.so, the plain-C restatement of the reference's
+  hot path (finess_oracle.c).
+* ``RefLib``: oracle/_ref/libfinref.so, the reference's own sources
+  (lib/2d/ConstructL.cpp, lib/WenoReconstruct.cpp, lib/2d/FinSolveRK.cpp, ...)
+  compiled in place by oracle/Makefile with the harness in ref_harness/.
+
+Both take and return numpy arrays in the reference's ghosted dTensorBC3 layout
+(lib/tensors.h:267-273), shape (mx+2mbc, my+2mbc, meqn).  Only tests/,
+__graft_entry__.smoke() and bench.py's CPU-baseline leg use this module.
+"""
+import ctypes as C
+import os
+import subprocess
+import sys
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(HERE)
+if ROOT not in sys.path:
+    sys.path.insert(0, ROOT)
+
+from finess_b200._abi import FinParams, ghosted_shape, smax_shape  # noqa: E402
+
+_dp = np.ctypeslib.ndpointer(dtype=np.float64, flags="C_CONTIGUOUS")
+ORACLE_SO = os.path.join(HERE, "liboracle.so")
+REF_SO = os.path.join(HERE, "_ref", "libfinref.so")
+
+
+def build_oracle():
+    """Compile liboracle.so (seconds, gcc only) if it is missing or stale."""
+    src = os.path.join(HERE, "finess_oracle.c")
+    if not os.path.exists(ORACLE_SO) or os.path.getmtime(ORACLE_SO) < os.path.getmtime(src):
+        subprocess.check_call(["make", "-s", "-C", HERE], stdout=subprocess.DEVNULL)
+
+
+class Oracle:
+    def __init__(self):
+        build_oracle()
+        lib = C.CDLL(ORACLE_SO)
+        P = C.POINTER(FinParams)
+        lib.oracle_set_bnd.argtypes = [P, _dp]
+        lib.oracle_global_wave_spd.argtypes = [P, _dp, C.POINTER(C.c_double), C.POINTER(C.c_double)]
+        lib.oracle_construct_l.argtypes = [P, _dp, _dp, _dp]
+        lib.oracle_construct_l.restype = C.c_int
+        lib.oracle_construct_lxwl.argtypes = [P, _dp, _dp, _dp, _dp, _dp]
+        lib.oracle_construct_lxwl.restype = C.c_int
+        lib.oracle_construct_integrated_r.argtypes = [P, C.c_double, _dp, _dp, _dp]
+        lib.oracle_construct_integrated_r.restype = C.c_int
+        lib.oracle_weno5.argtypes = [C.c_int, C.c_double, C.c_double, _dp]
+        lib.oracle_weno5.restype = C.c_double
+        lib.oracle_weno_js5_weights.argtypes = [C.c_double, C.c_double, _dp, _dp]
+        lib.oracle_finsolve.argtypes = [P, _dp, C.POINTER(C.c_double), C.c_double, _dp, C.POINTER(C.c_int)]
+        lib.oracle_finsolve.restype = C.c_int
+        lib.oracle_step_fixed.argtypes = [P, _dp, C.c_double, C.POINTER(C.c_double)]
+        lib.oracle_step_fixed.restype = C.c_int
+        lib.oracle_conservation_totals.argtypes = [P, _dp, _dp]
+        self.lib = lib
+
+    def set_bnd(self, p, q):
+        q = np.ascontiguousarray(q, dtype=np.float64).copy()
+        self.lib.oracle_set_bnd(C.byref(p), q)
+        return q
+
+    def global_wave_spd(self, p, q):
+        a1, a2 = C.c_double(), C.c_double()
+        self.lib.oracle_global_wave_spd(C.byref(p), np.ascontiguousarray(q), C.byref(a1), C.byref(a2))
+        return a1.value, a2.value
+
+    def construct_l(self, p, q, smax=None):
+        L = np.zeros(ghosted_shape(p))
+        sm = np.zeros(smax_shape(p)) if smax is None else np.ascontiguousarray(smax).copy()
+        rc = self.lib.oracle_construct_l(C.byref(p), np.ascontiguousarray(q), L, sm)
+        if rc:
+            raise ValueError(f"oracle_construct_l failed: {rc}")
+        return L, sm
+
+    def construct_integrated_r(self, p, dt, q):
+        F = np.zeros(ghosted_shape(p))
+        G = np.zeros(ghosted_shape(p))
+        rc = self.lib.oracle_construct_integrated_r(C.byref(p), dt, np.ascontiguousarray(q), F, G)
+        if rc:
+            raise ValueError(f"oracle_construct_integrated_r failed: {rc}")
+        return F, G
+
+    def construct_lxwl(self, p, q, F, G):
+        L = np.zeros(ghosted_shape(p))
+        sm = np.zeros(smax_shape(p))
+        rc = self.lib.oracle_construct_lxwl(C.byref(p), np.ascontiguousarray(q), np.ascontiguousarray(F),
+                                            np.ascontiguousarray(G), L, sm)
+        if rc:
+            raise ValueError(f"oracle_construct_lxwl failed: {rc}")
+        return L, sm
+
+    def weno5(self, version, eps, pw, u):
+        return self.lib.oracle_weno5(version, eps, pw, np.ascontiguousarray(u, dtype=np.float64))
+
+    def js5_weights(self, eps, pw, u):
+        w = np.zeros(3)
+        self.lib.oracle_weno_js5_weights(eps, pw, np.ascontiguousarray(u, dtype=np.float64), w)
+        return w
+
+    def finsolve(self, p, q, t, tend, dt):
+        q = np.ascontiguousarray(q, dtype=np.float64).copy()
+        tt = C.c_double(t)
+        dtv = np.array([0.0, dt, p.max_dt])
+        n = C.c_int(0)
+        rc = self.lib.oracle_finsolve(C.byref(p), q, C.byref(tt), tend, dtv, C.byref(n))
+        return rc, q, tt.value, dtv[1], n.value
+
+    def step_fixed(self, p, q, dt):
+        q = np.ascontiguousarray(q, dtype=np.float64).copy()
+        cfl = C.c_double(0.0)
+        rc = self.lib.oracle_step_fixed(C.byref(p), q, dt, C.byref(cfl))
+        if rc:
+            raise ValueError(f"oracle_step_fixed failed: {rc}")
+        return q, cfl.value
+
+    def conservation_totals(self, p, q):
+        out = np.zeros(p.meqn)
+        self.lib.oracle_conservation_totals(C.byref(p), np.ascontiguousarray(q), out)
+        return out
+
+
+class RefLib:
+    """The reference's own compiled sources; available where oracle/_ref was built."""
+
+    @staticmethod
+    def available():
+        return os.path.exists(REF_SO)
+
+    def __init__(self):
+        lib = C.CDLL(REF_SO)
+        P = C.POINTER(FinParams)
+        lib.ref_setup.argtypes = [P]
+        lib.ref_set_bnd.argtypes = [_dp]
+        lib.ref_construct_l.argtypes = [_dp, _dp, _dp]
+        lib.ref_construct_l.restype = C.c_int
+        lib.ref_global_wave_spd.argtypes = [_dp, _dp]
+        lib.ref_construct_integrated_r.argtypes = [C.c_double, _dp, _dp, _dp]
+        lib.ref_finsolve.argtypes = [C.c_int, _dp, C.POINTER(C.c_double), C.c_double, _dp]
+        lib.ref_finsolve.restype = C.c_int
+        self.lib = lib
+
+    def setup(self, p):
+        self.lib.ref_setup(C.byref(p))
+
+    def set_bnd(self, p, q):
+        self.setup(p)
+        q = np.ascontiguousarray(q, dtype=np.float64).copy()
+        self.lib.ref_set_bnd(q)
+        return q
+
+    def global_wave_spd(self, p, q):
+        self.setup(p)
+        out = np.zeros(2)
+        self.lib.ref_global_wave_spd(np.ascontiguousarray(q), out)
+        return out[0], out[1]
+
+    def construct_l(self, p, q, smax=None):
+        self.setup(p)
+        L = np.zeros(ghosted_shape(p))
+        sm = np.zeros(smax_shape(p)) if smax is None else np.ascontiguousarray(smax).copy()
+        rc = self.lib.ref_construct_l(np.ascontiguousarray(q), L, sm)
+        if rc:
+            raise ValueError(f"ref_construct_l failed: {rc}")
+        return L, sm
+
+    def construct_integrated_r(self, p, dt, q):
+        self.setup(p)
+        F = np.zeros(ghosted_shape(p))
+        G = np.zeros(ghosted_shape(p))
+        self.lib.ref_construct_integrated_r(dt, np.ascontiguousarray(q), F, G)
+        return F, G
+
+    def finsolve(self, p, q, t, tend, dt):
+        self.setup(p)
+        q = np.ascontiguousarray(q, dtype=np.float64).copy()
+        tt = C.c_double(t)
+        dtv = np.array([0.0, dt, p.max_dt])
+        rc = self.lib.ref_finsolve(p.time_stepping_method, q, C.byref(tt), tend, dtv)
+        return rc, q, tt.value, dtv[1]
