@@ -1,0 +1,791 @@
+// Host driver and C ABI of the B200 WENO right-hand side and time steppers.
+//
+// One fin_solver owns one problem on the current CUDA device: four FP64 state
+// buffers (q^n, two stage registers, q^{n+1}; the accept/reject logic of
+// lib/2d/FinSolveRK.cpp:98-357 needs q^n intact until the CFL check), a
+// small block of reduction slots, and a stream.  The time-step control stays
+// on the host and copies the reference exactly; per step the host reads back
+// 16 bytes (the face-speed maxima) to evaluate GetCFL.
+#include <cuda_runtime.h>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <cmath>
+#include <string>
+#include <vector>
+#include <algorithm>
+#include "finess_b200.h"
+#include "fin_stage.cuh"
+
+using namespace fin;
+
+namespace {
+
+thread_local std::string g_err = "";
+
+int set_err(int code, const std::string& msg)
+{
+    g_err = msg;
+    return code;
+}
+
+#define CK(call)                                                                              \
+    do {                                                                                      \
+        cudaError_t e_ = (call);                                                              \
+        if (e_ != cudaSuccess)                                                                \
+            return set_err(FIN_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_)); \
+    } while (0)
+
+// Tile shape of the stage kernel: 16 x 16 cells, 544 faces over 288 threads
+// (two rounds of the face loop, the second 89% full).
+using Cfg = TileCfg<16, 16, 288>;
+
+// Reduction slots (doubles) in one device block, reset by one memset per step.
+enum { SLOT_SMAX = 0, SLOT_ALPHA = 2, NSLOTS = 2 + 2 * 4 };
+
+}  // namespace
+
+struct fin_solver {
+    fin_params p;
+    double dx, dy;
+    size_t plane;           // elements per component plane
+    double* q[4];           // state buffers (planes); q[cur] holds q^n
+    int cur;                // index of q^n
+    double* slots;          // NSLOTS doubles (+ status word after them)
+    unsigned int* status;
+    double* h_slots;        // pinned mirror
+    double* d_aos;          // staging buffer for the reference ghosted layout
+    size_t aos_elems;
+    double* d_aux;          // second staging / L output buffer (planes)
+    double* d_face_x;       // per-face alpha buffers (only for fin_construct_l)
+    double* d_face_y;
+    cudaStream_t stream;
+    cudaEvent_t ev0, ev1;
+    cudaEvent_t kev[6];     // start/stop of the three stage kernels of the last step
+    bool time_kernels;      // record kev around each stage launch
+    double kernel_ms;       // accumulated stage-kernel time since the last reset
+    long long kernel_launches;
+    double t;               // Qnew.get_t()
+    double step_ms;
+    bool alpha_valid;       // slots hold alpha of q[cur]
+    double last_ms;
+    long long launches;
+};
+
+// ---------------------------------------------------------------------------
+// small kernels
+// ---------------------------------------------------------------------------
+namespace fin {
+
+__global__ void k_wave_spd_max(const double* q, int mx, int my, size_t plane, double gamma,
+                               double* alpha_out, unsigned int* status)
+{
+    __shared__ double red[2][32];
+    double ax = 0.0, ay = 0.0;
+    bool nonfinite = false;
+    const size_t n = size_t(mx) * my;
+    for (size_t g = blockIdx.x * size_t(blockDim.x) + threadIdx.x; g < n; g += size_t(gridDim.x) * blockDim.x) {
+        double Q[MEQN];
+#pragma unroll
+        for (int m = 0; m < MEQN; m++) Q[m] = q[m * plane + g];
+        const double Qy[MEQN] = {Q[0], Q[2], Q[1], Q[3], Q[4]};
+        const double sx = Euler::cell_speed(Euler::cell(gamma, Q));
+        const double sy = Euler::cell_speed(Euler::cell(gamma, Qy));
+        if (!(sx <= 1e300) || !(sy <= 1e300)) nonfinite = true;
+        ax = Max(ax, sx);
+        ay = Max(ay, sy);
+    }
+    if (!(ax <= 1e300)) ax = 0.0;
+    if (!(ay <= 1e300)) ay = 0.0;
+    for (int o = 16; o > 0; o >>= 1) {
+        ax = Max(ax, __shfl_xor_sync(0xffffffffu, ax, o));
+        ay = Max(ay, __shfl_xor_sync(0xffffffffu, ay, o));
+    }
+    const int w = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    if ((threadIdx.x & 31) == 0) { red[0][w] = ax; red[1][w] = ay; }
+    if (nonfinite) atomicOr(status, 1u);
+    __syncthreads();
+    if (threadIdx.x < 2) {
+        double v = 0.0;
+        for (int k = 0; k < nw; k++) v = Max(v, red[threadIdx.x][k]);
+        atomic_max_nonneg(alpha_out + threadIdx.x, v);
+    }
+}
+
+// Ghosted AoS (i, j, m), m fastest, i slowest -> interior planes.
+__global__ void k_aos_to_planes(const double* aos, double* planes, int mx, int my, int mbc, size_t plane)
+{
+    const size_t n = size_t(mx) * my;
+    const int sy = my + 2 * mbc;
+    for (size_t g = blockIdx.x * size_t(blockDim.x) + threadIdx.x; g < n; g += size_t(gridDim.x) * blockDim.x) {
+        const int i = int(g / my), j = int(g - size_t(i) * my);
+        const size_t src = (size_t(i + mbc) * sy + (j + mbc)) * MEQN;
+#pragma unroll
+        for (int m = 0; m < MEQN; m++) planes[m * plane + g] = aos[src + m];
+    }
+}
+
+// Interior planes -> ghosted AoS with the ghost frame filled by the BC remap
+// (what SetBndValues leaves in the reference's arrays).
+__global__ void k_planes_to_aos(const double* planes, double* aos, int mx, int my, int mbc, size_t plane,
+                                int bc0, int bc1, int bc2, int bc3)
+{
+    const int sx = mx + 2 * mbc, sy = my + 2 * mbc;
+    const size_t n = size_t(sx) * sy;
+    for (size_t e = blockIdx.x * size_t(blockDim.x) + threadIdx.x; e < n; e += size_t(gridDim.x) * blockDim.x) {
+        const int ii = int(e / sy), jj = int(e - size_t(ii) * sy);
+        const int gi = bc_remap(ii - mbc, mx, bc0, bc1), gj = bc_remap(jj - mbc, my, bc2, bc3);
+        const size_t g = size_t(gi) * my + gj;
+#pragma unroll
+        for (int m = 0; m < MEQN; m++) aos[e * MEQN + m] = planes[m * plane + g];
+    }
+}
+
+// Interior planes -> interior of a ghosted AoS array, ghosts untouched.
+__global__ void k_planes_to_aos_interior(const double* planes, double* aos, int mx, int my, int mbc, size_t plane)
+{
+    const size_t n = size_t(mx) * my;
+    const int sy = my + 2 * mbc;
+    for (size_t g = blockIdx.x * size_t(blockDim.x) + threadIdx.x; g < n; g += size_t(gridDim.x) * blockDim.x) {
+        const int i = int(g / my), j = int(g - size_t(i) * my);
+        const size_t dst = (size_t(i + mbc) * sy + (j + mbc)) * MEQN;
+#pragma unroll
+        for (int m = 0; m < MEQN; m++) aos[dst + m] = planes[m * plane + g];
+    }
+}
+
+// FMA throughput probe: 8 independent FMA chains per thread, no memory traffic
+// inside the loop.  Used to measure the FP64 and FP32 pipe peaks that the
+// stage kernel's pipe utilisation is quoted against.
+template <class R>
+__global__ void k_fma_peak(R* out, int iters, R a, R b)
+{
+    R x[8];
+#pragma unroll
+    for (int k = 0; k < 8; k++) x[k] = R(threadIdx.x + k);
+    for (int it = 0; it < iters; it++) {
+#pragma unroll
+        for (int k = 0; k < 8; k++) x[k] = x[k] * a + b;
+    }
+    R s = 0;
+#pragma unroll
+    for (int k = 0; k < 8; k++) s += x[k];
+    if (s == R(-1.2345)) out[0] = s;   // keeps the loop live; never true in practice
+}
+
+}  // namespace fin
+
+// ---------------------------------------------------------------------------
+// kernel dispatch
+// ---------------------------------------------------------------------------
+namespace {
+
+template <class R, int VER, bool P2>
+int launch_stage_t(fin_solver* s, const StageArgs& a)
+{
+    const size_t smem = Cfg::smem_bytes<R>();
+    auto kern = k_stage<R, VER, P2, Cfg>;
+    static bool configured = false;   // per instantiation; attribute is per device function
+    if (!configured) {
+        CK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
+        configured = true;
+    }
+    dim3 grid((a.my + Cfg::TJ - 1) / Cfg::TJ, (a.mx + Cfg::TI - 1) / Cfg::TI);
+    kern<<<grid, Cfg::NT, smem, s->stream>>>(a);
+    s->launches++;
+    CK(cudaGetLastError());
+    return FIN_OK;
+}
+
+template <class R>
+int launch_stage_r(fin_solver* s, const StageArgs& a)
+{
+    const bool p2 = s->p.power_param == 2.0;
+    switch (s->p.weno_version) {
+    case FIN_WENO_JS: return p2 ? launch_stage_t<R, FIN_WENO_JS, true>(s, a) : launch_stage_t<R, FIN_WENO_JS, false>(s, a);
+    case FIN_WENO_Z: return p2 ? launch_stage_t<R, FIN_WENO_Z, true>(s, a) : launch_stage_t<R, FIN_WENO_Z, false>(s, a);
+    case FIN_WENO_FD: return launch_stage_t<R, FIN_WENO_FD, true>(s, a);
+    }
+    return set_err(FIN_ERR_ARG, "weno_version");
+}
+
+int launch_stage(fin_solver* s, const StageArgs& a)
+{
+    if (s->p.precision == FIN_PREC_FP64) return launch_stage_r<double>(s, a);
+    if (s->p.precision == FIN_PREC_FP32) return launch_stage_r<float>(s, a);
+    return set_err(FIN_ERR_UNSUPPORTED, "precision form not built");
+}
+
+// A stage launch bracketed by events when kernel timing is on (stage k of 3).
+int launch_stage_timed(fin_solver* s, const StageArgs& a, int k)
+{
+    if (s->time_kernels) CK(cudaEventRecord(s->kev[2 * k], s->stream));
+    int rc = launch_stage(s, a);
+    if (rc) return rc;
+    if (s->time_kernels) CK(cudaEventRecord(s->kev[2 * k + 1], s->stream));
+    return FIN_OK;
+}
+
+// After the stream is synchronised: add the last step's stage-kernel times.
+int collect_kernel_times(fin_solver* s)
+{
+    if (!s->time_kernels) return FIN_OK;
+    for (int k = 0; k < 3; k++) {
+        float ms = 0.f;
+        CK(cudaEventElapsedTime(&ms, s->kev[2 * k], s->kev[2 * k + 1]));
+        s->kernel_ms += ms;
+        s->kernel_launches++;
+    }
+    return FIN_OK;
+}
+
+StageArgs base_args(fin_solver* s)
+{
+    StageArgs a;
+    memset(&a, 0, sizeof(a));
+    a.mx = s->p.mx;
+    a.my = s->p.my;
+    a.plane = s->plane;
+    a.rdx = 1.0 / s->dx;
+    a.rdy = 1.0 / s->dy;
+    a.gamma = s->p.gamma;
+    a.eps = s->p.epsilon;
+    a.pw = s->p.power_param;
+    a.alpha_scaling = s->p.alpha_scaling;
+    a.status = s->status;
+    a.bc[0] = s->p.bc_xlow; a.bc[1] = s->p.bc_xhigh;
+    a.bc[2] = s->p.bc_ylow; a.bc[3] = s->p.bc_yhigh;
+    return a;
+}
+
+int grid_blocks(size_t n)
+{
+    size_t b = (n + 255) / 256;
+    if (b > 148 * 16) b = 148 * 16;
+    if (b < 1) b = 1;
+    return int(b);
+}
+
+double* alpha_slot(fin_solver* s, int buf) { return s->slots + SLOT_ALPHA + 2 * buf; }
+
+// Global alpha of buffer buf into its slot (used when no stage epilogue has
+// produced it: after set_state, or when global_alpha is off it is unused).
+int compute_alpha(fin_solver* s, int buf)
+{
+    CK(cudaMemsetAsync(alpha_slot(s, buf), 0, 2 * sizeof(double), s->stream));
+    const size_t n = size_t(s->p.mx) * s->p.my;
+    k_wave_spd_max<<<grid_blocks(n), 256, 0, s->stream>>>(s->q[buf], s->p.mx, s->p.my, s->plane, s->p.gamma,
+                                                           alpha_slot(s, buf), s->status);
+    s->launches++;
+    CK(cudaGetLastError());
+    return FIN_OK;
+}
+
+int check_status(fin_solver* s)
+{
+    unsigned int st = 0;
+    CK(cudaMemcpyAsync(&st, s->status, sizeof(st), cudaMemcpyDeviceToHost, s->stream));
+    CK(cudaStreamSynchronize(s->stream));
+    if (st & 1u) {
+        CK(cudaMemsetAsync(s->status, 0, sizeof(unsigned int), s->stream));
+        return set_err(FIN_ERR_NONFINITE, "non-finite wave speed or state");
+    }
+    return FIN_OK;
+}
+
+// The stages of one step of size dt from q[cur] into q[nxt] (RK3:
+// FinSolveRK.cpp:158-211 with SetRKinfo.cpp:50-64).  Leaves the face-speed
+// maxima of the step in slots SMAX and alpha(q[nxt]) in its slot.
+int take_stages(fin_solver* s, double dt, int nxt)
+{
+    const fin_params& p = s->p;
+    if (p.time_stepping_method != FIN_TS_RK || p.time_order != 3)
+        return set_err(FIN_ERR_UNSUPPORTED, "only SSP-RK3 (time_order 3) is built");
+    const int qn = s->cur;
+    int reg[2], k = 0;
+    for (int b = 0; b < 4 && k < 2; b++)
+        if (b != qn && b != nxt) reg[k++] = b;
+    const int q1 = reg[0], q2 = reg[1];
+    // reset smax and the alpha slots of the three buffers written this step
+    CK(cudaMemsetAsync(s->slots + SLOT_SMAX, 0, 2 * sizeof(double), s->stream));
+    CK(cudaMemsetAsync(alpha_slot(s, q1), 0, 2 * sizeof(double), s->stream));
+    CK(cudaMemsetAsync(alpha_slot(s, q2), 0, 2 * sizeof(double), s->stream));
+    CK(cudaMemsetAsync(alpha_slot(s, nxt), 0, 2 * sizeof(double), s->stream));
+    const bool ga = p.global_alpha != 0;
+    int rc;
+    StageArgs a = base_args(s);
+    a.smax_out = s->slots + SLOT_SMAX;
+    // stage 1: q1 = 1*q^n + 0*q* + (1*dt) L(q^n)
+    a.qin = s->q[qn]; a.A = s->q[qn]; a.B = nullptr; a.qout = s->q[q1];
+    a.a1 = 1.0; a.a2 = 0.0; a.bdt = 1.0 * dt;
+    a.alpha_in = ga ? alpha_slot(s, qn) : nullptr;
+    a.alpha_out = alpha_slot(s, q1);
+    if ((rc = launch_stage_timed(s, a, 0))) return rc;
+    // stage 2: q2 = 0.75 q^n + 0.25 q1 + (0.25 dt) L(q1)
+    a.qin = s->q[q1]; a.A = s->q[qn]; a.B = s->q[q1]; a.qout = s->q[q2];
+    a.a1 = 0.75; a.a2 = 0.25; a.bdt = 0.25 * dt;
+    a.alpha_in = ga ? alpha_slot(s, q1) : nullptr;
+    a.alpha_out = alpha_slot(s, q2);
+    if ((rc = launch_stage_timed(s, a, 1))) return rc;
+    // stage 3: q^{n+1} = (2/3) q2 + (1/3) q^n + ((2/3) dt) L(q2)
+    a.qin = s->q[q2]; a.A = s->q[q2]; a.B = s->q[qn]; a.qout = s->q[nxt];
+    a.a1 = 2.0e0 / 3.0e0; a.a2 = 1.0e0 / 3.0e0; a.bdt = (2.0e0 / 3.0e0) * dt;
+    a.alpha_in = ga ? alpha_slot(s, q2) : nullptr;
+    a.alpha_out = alpha_slot(s, nxt);
+    if ((rc = launch_stage_timed(s, a, 2))) return rc;
+    return FIN_OK;
+}
+
+// GetCFL (lib/2d/GetCFL.cpp:31-73) from the step's face-speed maxima: the
+// maximum of dt*smax/dx over faces equals dt*max(smax)/dx because the
+// rounded product and quotient are monotone in smax.
+int get_cfl(fin_solver* s, double dt, double dtmax, double* cfl)
+{
+    CK(cudaMemcpyAsync(s->h_slots, s->slots, NSLOTS * sizeof(double), cudaMemcpyDeviceToHost, s->stream));
+    int rc = check_status(s);   // synchronizes the stream
+    if (rc) return rc;
+    if (dt > dtmax) return set_err(FIN_ERR_DT_BOUNDS, "dt is out of bounds");
+    double c = -100.0;
+    c = Max(dt * s->h_slots[SLOT_SMAX] / s->dx, c);
+    c = Max(dt * s->h_slots[SLOT_SMAX + 1] / s->dy, c);
+    if (c > 1.0e8) return set_err(FIN_ERR_CFL_BOUNDS, "CFL number is out of bounds");
+    *cfl = c;
+    return FIN_OK;
+}
+
+int validate(const fin_params* p)
+{
+    if (!p) return set_err(FIN_ERR_ARG, "null params");
+    if (p->physics != FIN_PHYS_EULER || p->meqn != 5) return set_err(FIN_ERR_UNSUPPORTED, "only 2D Euler (meqn 5)");
+    if (p->space_order != 5) return set_err(FIN_ERR_UNSUPPORTED, "space_order must be 5");
+    if (p->weno_version != FIN_WENO_JS && p->weno_version != FIN_WENO_Z && p->weno_version != FIN_WENO_FD)
+        return set_err(FIN_ERR_ARG, "Requested WENO Reconstruction not implemented.");
+    if (p->mx < 1 || p->my < 1) return set_err(FIN_ERR_ARG, "mx, my must be positive");
+    if (p->mbc < 3) return set_err(FIN_ERR_ARG, "mbc must be >= 3 for WENO5");
+    if (p->source_term) return set_err(FIN_ERR_UNSUPPORTED, "source terms are not built");
+    if (!(p->xhigh > p->xlow) || !(p->yhigh > p->ylow)) return set_err(FIN_ERR_ARG, "empty domain");
+    for (int b : {p->bc_xlow, p->bc_xhigh, p->bc_ylow, p->bc_yhigh})
+        if (b != FIN_BC_PERIODIC && b != FIN_BC_TRANSMISSIVE) return set_err(FIN_ERR_ARG, "bad boundary condition");
+    if ((p->bc_xlow == FIN_BC_PERIODIC) != (p->bc_xhigh == FIN_BC_PERIODIC) ||
+        (p->bc_ylow == FIN_BC_PERIODIC) != (p->bc_yhigh == FIN_BC_PERIODIC))
+        return set_err(FIN_ERR_ARG, "periodic boundaries come in pairs");
+    const int H = 3;
+    if ((p->bc_xlow == FIN_BC_PERIODIC && p->mx < H) || (p->bc_ylow == FIN_BC_PERIODIC && p->my < H))
+        return set_err(FIN_ERR_ARG, "periodic direction shorter than the stencil halo");
+    if (p->precision != FIN_PREC_FP64 && p->precision != FIN_PREC_FP32)
+        return set_err(FIN_ERR_UNSUPPORTED, "precision form not built");
+    return FIN_OK;
+}
+
+size_t aos_elems_of(const fin_params& p)
+{
+    return size_t(p.mx + 2 * p.mbc) * (p.my + 2 * p.mbc) * p.meqn;
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------------------
+// C ABI
+// ---------------------------------------------------------------------------
+extern "C" {
+
+void fin_params_default(fin_params* p)
+{
+    memset(p, 0, sizeof(*p));
+    p->meqn = 5; p->maux = 0;
+    p->space_order = 5; p->time_order = 3;
+    p->time_stepping_method = FIN_TS_RK;
+    p->global_alpha = 0; p->source_term = 0;
+    p->nv = 500000; p->verbosity = 0;
+    p->initial_dt = 1e-3; p->max_dt = 1e10; p->max_cfl = 0.45; p->desired_cfl = 0.4;
+    p->mx = 10; p->my = 10; p->mbc = 3;
+    p->xlow = 0; p->xhigh = 1; p->ylow = 0; p->yhigh = 1;
+    p->weno_version = FIN_WENO_JS;
+    p->epsilon = 1e-6; p->power_param = 2.0; p->alpha_scaling = 1.1;
+    p->gamma = 1.4;
+    p->bc_xlow = p->bc_xhigh = p->bc_ylow = p->bc_yhigh = FIN_BC_PERIODIC;
+    p->physics = FIN_PHYS_EULER;
+    p->precision = FIN_PREC_FP64;
+}
+
+const char* fin_last_error(void) { return g_err.c_str(); }
+
+int fin_abi_version(void) { return FIN_ABI_VERSION; }
+
+int fin_create(const fin_params* p, fin_solver** out)
+{
+    if (!out) return set_err(FIN_ERR_ARG, "null out");
+    *out = nullptr;
+    int rc = validate(p);
+    if (rc) return rc;
+    int dev = 0, ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0)
+        return set_err(FIN_ERR_NO_DEVICE, "no CUDA device");
+    CK(cudaGetDevice(&dev));
+    cudaDeviceProp prop;
+    CK(cudaGetDeviceProperties(&prop, dev));
+    if (prop.major != 10) return set_err(FIN_ERR_NO_DEVICE, "this build targets sm_100a (B200)");
+
+    fin_solver* s = new fin_solver();
+    memset(s, 0, sizeof(*s));
+    s->p = *p;
+    s->dx = (p->xhigh - p->xlow) / p->mx;
+    s->dy = (p->yhigh - p->ylow) / p->my;
+    // planes padded to 32 elements (256 B) so every plane starts aligned
+    s->plane = (size_t(p->mx) * p->my + 31) / 32 * 32;
+    s->aos_elems = aos_elems_of(*p);
+    auto fail = [&](cudaError_t e, const char* what) {
+        fin_destroy(s);
+        return set_err(FIN_ERR_CUDA, std::string(what) + ": " + cudaGetErrorString(e));
+    };
+    cudaError_t e;
+    for (int b = 0; b < 4; b++)
+        if ((e = cudaMalloc(&s->q[b], MEQN * s->plane * sizeof(double))) != cudaSuccess) return fail(e, "cudaMalloc state");
+    if ((e = cudaMalloc(&s->slots, NSLOTS * sizeof(double) + 64)) != cudaSuccess) return fail(e, "cudaMalloc slots");
+    s->status = reinterpret_cast<unsigned int*>(s->slots + NSLOTS);
+    if ((e = cudaMallocHost(&s->h_slots, NSLOTS * sizeof(double))) != cudaSuccess) return fail(e, "cudaMallocHost");
+    if ((e = cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking)) != cudaSuccess) return fail(e, "stream");
+    if ((e = cudaEventCreate(&s->ev0)) != cudaSuccess) return fail(e, "event");
+    if ((e = cudaEventCreate(&s->ev1)) != cudaSuccess) return fail(e, "event");
+    for (int k = 0; k < 6; k++)
+        if ((e = cudaEventCreate(&s->kev[k])) != cudaSuccess) return fail(e, "event");
+    if ((e = cudaMemsetAsync(s->slots, 0, NSLOTS * sizeof(double) + 64, s->stream)) != cudaSuccess) return fail(e, "memset");
+    for (int b = 0; b < 4; b++)
+        if ((e = cudaMemsetAsync(s->q[b], 0, MEQN * s->plane * sizeof(double), s->stream)) != cudaSuccess) return fail(e, "memset");
+    if ((e = cudaStreamSynchronize(s->stream)) != cudaSuccess) return fail(e, "sync");
+    s->t = 0.0;
+    *out = s;
+    return FIN_OK;
+}
+
+int fin_destroy(fin_solver* s)
+{
+    if (!s) return FIN_OK;
+    if (s->stream) cudaStreamSynchronize(s->stream);
+    for (int b = 0; b < 4; b++) cudaFree(s->q[b]);
+    cudaFree(s->slots);
+    cudaFree(s->d_aos);
+    cudaFree(s->d_aux);
+    cudaFree(s->d_face_x);
+    cudaFree(s->d_face_y);
+    if (s->h_slots) cudaFreeHost(s->h_slots);
+    if (s->ev0) cudaEventDestroy(s->ev0);
+    if (s->ev1) cudaEventDestroy(s->ev1);
+    for (int k = 0; k < 6; k++)
+        if (s->kev[k]) cudaEventDestroy(s->kev[k]);
+    if (s->stream) cudaStreamDestroy(s->stream);
+    delete s;
+    return FIN_OK;
+}
+
+static int ensure_aos(fin_solver* s)
+{
+    if (!s->d_aos) CK(cudaMalloc(&s->d_aos, s->aos_elems * sizeof(double)));
+    return FIN_OK;
+}
+
+static int upload(fin_solver* s, const double* q_host, int buf)
+{
+    int rc = ensure_aos(s);
+    if (rc) return rc;
+    CK(cudaMemcpyAsync(s->d_aos, q_host, s->aos_elems * sizeof(double), cudaMemcpyHostToDevice, s->stream));
+    const size_t n = size_t(s->p.mx) * s->p.my;
+    k_aos_to_planes<<<grid_blocks(n), 256, 0, s->stream>>>(s->d_aos, s->q[buf], s->p.mx, s->p.my, s->p.mbc, s->plane);
+    s->launches++;
+    CK(cudaGetLastError());
+    return FIN_OK;
+}
+
+int fin_set_state(fin_solver* s, const double* q_host, double t)
+{
+    if (!s || !q_host) return set_err(FIN_ERR_ARG, "null argument");
+    int rc = upload(s, q_host, s->cur);
+    if (rc) return rc;
+    s->t = t;
+    if ((rc = compute_alpha(s, s->cur))) return rc;
+    CK(cudaStreamSynchronize(s->stream));
+    s->alpha_valid = true;
+    return FIN_OK;
+}
+
+int fin_get_state(fin_solver* s, double* q_host, double* t)
+{
+    if (!s || !q_host) return set_err(FIN_ERR_ARG, "null argument");
+    int rc = ensure_aos(s);
+    if (rc) return rc;
+    const size_t n = s->aos_elems / MEQN;
+    k_planes_to_aos<<<grid_blocks(n), 256, 0, s->stream>>>(s->q[s->cur], s->d_aos, s->p.mx, s->p.my, s->p.mbc,
+                                                           s->plane, s->p.bc_xlow, s->p.bc_xhigh, s->p.bc_ylow,
+                                                           s->p.bc_yhigh);
+    s->launches++;
+    CK(cudaGetLastError());
+    CK(cudaMemcpyAsync(q_host, s->d_aos, s->aos_elems * sizeof(double), cudaMemcpyDeviceToHost, s->stream));
+    CK(cudaStreamSynchronize(s->stream));
+    if (t) *t = s->t;
+    return FIN_OK;
+}
+
+int fin_global_wave_spd(fin_solver* s, const double* q_host, double* alpha1, double* alpha2)
+{
+    if (!s || !q_host || !alpha1 || !alpha2) return set_err(FIN_ERR_ARG, "null argument");
+    // use the next-state buffer as scratch so the solver's state is untouched
+    const int buf = (s->cur + 3) % 4;
+    int rc = upload(s, q_host, buf);
+    if (rc) return rc;
+    if ((rc = compute_alpha(s, buf))) return rc;
+    double h[2];
+    CK(cudaMemcpyAsync(h, alpha_slot(s, buf), sizeof(h), cudaMemcpyDeviceToHost, s->stream));
+    CK(cudaStreamSynchronize(s->stream));
+    *alpha1 = h[0];
+    *alpha2 = h[1];
+    return check_status(s);
+}
+
+int fin_construct_l(fin_solver* s, const double* q_host, double* L_host, double* smax_host)
+{
+    if (!s || !q_host || !L_host) return set_err(FIN_ERR_ARG, "null argument");
+    const fin_params& p = s->p;
+    const int buf = (s->cur + 3) % 4, outb = (s->cur + 2) % 4;
+    int rc = upload(s, q_host, buf);
+    if (rc) return rc;
+    if (p.global_alpha && (rc = compute_alpha(s, buf))) return rc;
+    if (smax_host) {
+        if (!s->d_face_x) CK(cudaMalloc(&s->d_face_x, size_t(p.mx + 1) * p.my * sizeof(double)));
+        if (!s->d_face_y) CK(cudaMalloc(&s->d_face_y, size_t(p.mx) * (p.my + 1) * sizeof(double)));
+    }
+    StageArgs a = base_args(s);
+    a.qin = s->q[buf];
+    a.A = nullptr; a.B = nullptr; a.qout = s->q[outb];
+    a.a1 = 0.0; a.a2 = 0.0; a.bdt = 1.0;
+    a.alpha_in = p.global_alpha ? alpha_slot(s, buf) : nullptr;
+    a.face_alpha_x = smax_host ? s->d_face_x : nullptr;
+    a.face_alpha_y = smax_host ? s->d_face_y : nullptr;
+    if ((rc = launch_stage(s, a))) return rc;
+    // L: interior of the ghosted output, ghosts untouched (the reference
+    // leaves Lstar's ghost entries uninitialised).
+    const size_t n = size_t(p.mx) * p.my;
+    std::vector<double> hl(MEQN * n);
+    for (int m = 0; m < MEQN; m++)
+        CK(cudaMemcpyAsync(hl.data() + m * n, s->q[outb] + m * s->plane, n * sizeof(double), cudaMemcpyDeviceToHost,
+                           s->stream));
+    CK(cudaStreamSynchronize(s->stream));
+    {
+        const int sy = p.my + 2 * p.mbc;
+        for (int i = 0; i < p.mx; i++)
+            for (int j = 0; j < p.my; j++)
+                for (int m = 0; m < MEQN; m++)
+                    L_host[(size_t(i + p.mbc) * sy + (j + p.mbc)) * MEQN + m] = hl[m * n + size_t(i) * p.my + j];
+    }
+    if (smax_host) {
+        std::vector<double> fx(size_t(p.mx + 1) * p.my), fy(size_t(p.mx) * (p.my + 1));
+        CK(cudaMemcpyAsync(fx.data(), s->d_face_x, fx.size() * sizeof(double), cudaMemcpyDeviceToHost, s->stream));
+        CK(cudaMemcpyAsync(fy.data(), s->d_face_y, fy.size() * sizeof(double), cudaMemcpyDeviceToHost, s->stream));
+        CK(cudaStreamSynchronize(s->stream));
+        // smax is dTensorBC3(mx+1, my+1, 2, mbc): max-accumulate (ConstructL.cpp:173,324)
+        const int sy = p.my + 1 + 2 * p.mbc;
+        auto at = [&](int i, int j, int m) -> double& {   // 1-based i, j, m
+            return smax_host[(size_t(i + p.mbc - 1) * sy + (j + p.mbc - 1)) * 2 + (m - 1)];
+        };
+        for (int i = 1; i <= p.mx + 1; i++)
+            for (int j = 1; j <= p.my; j++) {
+                double& d = at(i, j, 1);
+                d = Max(d, fx[size_t(i - 1) * p.my + (j - 1)]);
+            }
+        for (int i = 1; i <= p.mx; i++)
+            for (int j = 1; j <= p.my + 1; j++) {
+                double& d = at(i, j, 2);
+                d = Max(d, fy[size_t(i - 1) * (p.my + 1) + (j - 1)]);
+            }
+    }
+    CK(cudaStreamSynchronize(s->stream));
+    return check_status(s);
+}
+
+int fin_step_fixed(fin_solver* s, double dt, double* cfl_out)
+{
+    if (!s) return set_err(FIN_ERR_ARG, "null solver");
+    int rc;
+    if (!s->alpha_valid && (rc = compute_alpha(s, s->cur))) return rc;
+    const int nxt = (s->cur + 3) % 4;
+    CK(cudaEventRecord(s->ev0, s->stream));
+    if ((rc = take_stages(s, dt, nxt))) return rc;
+    CK(cudaEventRecord(s->ev1, s->stream));
+    double cfl = 0.0;
+    if ((rc = get_cfl(s, dt, 1e300, &cfl))) return rc;
+    if ((rc = collect_kernel_times(s))) return rc;
+    float ms = 0.f;
+    CK(cudaEventElapsedTime(&ms, s->ev0, s->ev1));
+    s->last_ms = ms;
+    s->cur = nxt;
+    s->alpha_valid = true;
+    s->t = s->t + dt;
+    if (cfl_out) *cfl_out = cfl;
+    return FIN_OK;
+}
+
+int fin_solve(fin_solver* s, double tend, double* dtv, int* nsteps_out)
+{
+    return fin_advance(s, tend, dtv, 0x7fffffff, nsteps_out);
+}
+
+// lib/2d/FinSolveRK.cpp:13-371, stopping early after max_steps accepted steps.
+int fin_advance(fin_solver* s, double tend, double* dtv, int max_steps, int* nsteps_out)
+{
+    if (!s || !dtv) return set_err(FIN_ERR_ARG, "null argument");
+    const fin_params& p = s->p;
+    const double CFL_max = p.max_cfl, CFL_target = p.desired_cfl;
+    double t = s->t;
+    double dt = dtv[1], cfl = 0.0;
+    double t_star = s->t;   // Qstar.get_t()
+    int n_step = 0, accepted = 0, rc = FIN_OK;
+    if (!s->alpha_valid && (rc = compute_alpha(s, s->cur))) return rc;
+    double ms_total = 0.0;
+    CK(cudaEventRecord(s->ev0, s->stream));
+    s->step_ms = 0.0;
+    while (t < tend && accepted < max_steps) {
+        int m_accept = 0;
+        n_step = n_step + 1;
+        if (n_step > p.nv) { rc = set_err(FIN_ERR_NSTEPS, "Exceeded allowed # of time steps"); break; }
+        const double t_old_q = s->t;
+        while (m_accept == 0) {
+            s->t = t;
+            const double told = t;
+            if (told + dt > tend) dt = tend - told;
+            t = told + dt;
+            const int nxt = (s->cur + 3) % 4;
+            if ((rc = take_stages(s, dt, nxt))) goto done;
+            if ((rc = get_cfl(s, dt, dtv[2], &cfl))) goto done;
+            if ((rc = collect_kernel_times(s))) goto done;
+            // Qstar/Qnew time bookkeeping of UpdateSoln.cpp:27 for the 3 stages
+            t_star = 1.0 * s->t + 0.0 * t_star + 1.0 * dt;
+            t_star = 0.75 * s->t + 0.25 * t_star + 0.25 * dt;
+            const double t_new = (2.0e0 / 3.0e0) * t_star + (1.0e0 / 3.0e0) * s->t + (2.0e0 / 3.0e0) * dt;
+            if (cfl > 0.0) dt = Min(dtv[2], dt * CFL_target / cfl);
+            else dt = dtv[2];
+            if (p.verbosity)
+                printf("FinSolveRK2D ... Step%5d   CFL =%6.3f   dt =%11.3e   t =%11.3e\n", n_step, cfl, dt, t);
+            if (cfl <= CFL_max) {
+                m_accept = 1;
+                s->cur = nxt;          // accept: q^{n+1} becomes q^n (alpha slot travels with it)
+                s->t = t_new;
+            } else {
+                t = told;              // reject: q^n was never overwritten
+                s->t = t_old_q;
+                if (p.verbosity) printf("FinSolveRK2D rejecting step...CFL number too large\n");
+            }
+        }
+        accepted++;
+    }
+    dtv[1] = dt;
+done:
+    {
+        cudaError_t e1 = cudaEventRecord(s->ev1, s->stream);
+        if (e1 == cudaSuccess) e1 = cudaEventSynchronize(s->ev1);
+        float ms = 0.f;
+        if (e1 == cudaSuccess) e1 = cudaEventElapsedTime(&ms, s->ev0, s->ev1);
+        if (e1 == cudaSuccess) ms_total = ms;
+    }
+    s->last_ms = ms_total;
+    if (nsteps_out) *nsteps_out = accepted;
+    return rc;
+}
+
+int fin_fma_peak(int fp64, double* tflops)
+{
+    if (!tflops) return set_err(FIN_ERR_ARG, "null argument");
+    int dev = 0, nsm = 0;
+    CK(cudaGetDevice(&dev));
+    CK(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
+    void* out = nullptr;
+    CK(cudaMalloc(&out, 64));
+    cudaEvent_t e0, e1;
+    CK(cudaEventCreate(&e0));
+    CK(cudaEventCreate(&e1));
+    const int threads = 256, blocks = nsm * 8, iters = 1 << 14;
+    double best = 0.0;
+    for (int rep = 0; rep < 4; rep++) {
+        CK(cudaEventRecord(e0, 0));
+        if (fp64) k_fma_peak<double><<<blocks, threads>>>((double*)out, iters, 0.999999, 1e-7);
+        else k_fma_peak<float><<<blocks, threads>>>((float*)out, iters, 0.999999f, 1e-7f);
+        CK(cudaEventRecord(e1, 0));
+        CK(cudaEventSynchronize(e1));
+        float ms = 0.f;
+        CK(cudaEventElapsedTime(&ms, e0, e1));
+        const double flops = 2.0 * 8.0 * double(iters) * threads * blocks;
+        if (rep > 0) best = std::max(best, flops / (ms * 1e-3) / 1e12);
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    cudaFree(out);
+    *tflops = best;
+    return FIN_OK;
+}
+
+int fin_set_kernel_timing(fin_solver* s, int on)
+{
+    if (!s) return set_err(FIN_ERR_ARG, "null solver");
+    s->time_kernels = on != 0;
+    s->kernel_ms = 0.0;
+    s->kernel_launches = 0;
+    return FIN_OK;
+}
+
+int fin_kernel_time(fin_solver* s, double* ms, long long* launches)
+{
+    if (!s || !ms || !launches) return set_err(FIN_ERR_ARG, "null argument");
+    *ms = s->kernel_ms;
+    *launches = s->kernel_launches;
+    return FIN_OK;
+}
+
+int fin_conservation_totals(fin_solver* s, double* totals)
+{
+    if (!s || !totals) return set_err(FIN_ERR_ARG, "null argument");
+    // Host-side compensated sum over a device->host copy of the planes.
+    const size_t n = size_t(s->p.mx) * s->p.my;
+    std::vector<double> h(n);
+    for (int m = 0; m < MEQN; m++) {
+        CK(cudaMemcpyAsync(h.data(), s->q[s->cur] + m * s->plane, n * sizeof(double), cudaMemcpyDeviceToHost, s->stream));
+        CK(cudaStreamSynchronize(s->stream));
+        double sum = 0.0, comp = 0.0;
+        for (size_t k = 0; k < n; k++) {
+            const double y = s->dx * s->dy * h[k] - comp;
+            const double tt = sum + y;
+            comp = (tt - sum) - y;
+            sum = tt;
+        }
+        totals[m] = sum;
+    }
+    return FIN_OK;
+}
+
+int fin_last_kernel_ms(fin_solver* s, double* ms)
+{
+    if (!s || !ms) return set_err(FIN_ERR_ARG, "null argument");
+    *ms = s->last_ms;
+    return FIN_OK;
+}
+
+int fin_launch_count(fin_solver* s, long long* launches)
+{
+    if (!s || !launches) return set_err(FIN_ERR_ARG, "null argument");
+    *launches = s->launches;
+    return FIN_OK;
+}
+
+int fin_device_layout(fin_solver* s, size_t* plane_stride, size_t* row_stride)
+{
+    if (!s) return set_err(FIN_ERR_ARG, "null solver");
+    if (plane_stride) *plane_stride = s->plane;
+    if (row_stride) *row_stride = size_t(s->p.my);
+    return FIN_OK;
+}
+
+int fin_state_device_ptr(fin_solver* s, double** q_dev)
+{
+    if (!s || !q_dev) return set_err(FIN_ERR_ARG, "null argument");
+    *q_dev = s->q[s->cur];
+    return FIN_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,176 @@
+"""Python front end of libfinb200.so (the C ABI in include/finess_b200.h).
+
+The product is the CUDA library; this module loads it with ctypes and mirrors
+the reference's entry points with the same names and argument meaning:
+
+* ``ConstructL(q)``      -> lib/2d/ConstructL.cpp:13 (returns L and smax)
+* ``GlobalWaveSpd(q)``   -> lib/2d/GlobalWaveSpd.cpp:20
+* ``FinSolveRK(tend, dtv)`` -> lib/2d/FinSolveRK.cpp:13 (advances the device state)
+
+Arrays are numpy float64 in the reference's ghosted (i, j, m) layout.  There
+is no CPU fallback: if the library or a B200 is missing, construction raises.
+"""
+import ctypes as C
+import os
+
+import numpy as np
+
+from ._abi import FIN_OK, FinParams, ghosted_shape, smax_shape
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "_lib", "libfinb200.so")
+_dp = np.ctypeslib.ndpointer(dtype=np.float64, flags="C_CONTIGUOUS")
+_lib = None
+
+
+class FinError(RuntimeError):
+    def __init__(self, code, msg):
+        super().__init__(f"finess_b200 error {code}: {msg}")
+        self.code = code
+
+
+def load_library(path=LIB_PATH):
+    """Load libfinb200.so; raises if it has not been built."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(path):
+        raise FileNotFoundError(f"{path} is missing: build it with __graft_entry__.build()")
+    lib = C.CDLL(path)
+    P = C.POINTER(FinParams)
+    vp = C.c_void_p
+    lib.fin_params_default.argtypes = [P]
+    lib.fin_last_error.restype = C.c_char_p
+    lib.fin_abi_version.restype = C.c_int
+    lib.fin_create.argtypes = [P, C.POINTER(vp)]
+    lib.fin_destroy.argtypes = [vp]
+    lib.fin_set_state.argtypes = [vp, _dp, C.c_double]
+    lib.fin_get_state.argtypes = [vp, _dp, C.POINTER(C.c_double)]
+    lib.fin_construct_l.argtypes = [vp, _dp, _dp, C.c_void_p]
+    lib.fin_global_wave_spd.argtypes = [vp, _dp, C.POINTER(C.c_double), C.POINTER(C.c_double)]
+    lib.fin_solve.argtypes = [vp, C.c_double, _dp, C.POINTER(C.c_int)]
+    lib.fin_step_fixed.argtypes = [vp, C.c_double, C.POINTER(C.c_double)]
+    lib.fin_conservation_totals.argtypes = [vp, _dp]
+    lib.fin_last_kernel_ms.argtypes = [vp, C.POINTER(C.c_double)]
+    lib.fin_launch_count.argtypes = [vp, C.POINTER(C.c_longlong)]
+    lib.fin_device_layout.argtypes = [vp, C.POINTER(C.c_size_t), C.POINTER(C.c_size_t)]
+    lib.fin_state_device_ptr.argtypes = [vp, C.POINTER(C.c_void_p)]
+    lib.fin_advance.argtypes = [vp, C.c_double, _dp, C.c_int, C.POINTER(C.c_int)]
+    lib.fin_set_kernel_timing.argtypes = [vp, C.c_int]
+    lib.fin_kernel_time.argtypes = [vp, C.POINTER(C.c_double), C.POINTER(C.c_longlong)]
+    lib.fin_fma_peak.argtypes = [C.c_int, C.POINTER(C.c_double)]
+    for name in ("fin_create", "fin_destroy", "fin_set_state", "fin_get_state", "fin_construct_l",
+                 "fin_global_wave_spd", "fin_solve", "fin_step_fixed", "fin_conservation_totals",
+                 "fin_last_kernel_ms", "fin_launch_count", "fin_device_layout", "fin_state_device_ptr",
+                 "fin_advance", "fin_set_kernel_timing", "fin_kernel_time", "fin_fma_peak"):
+        getattr(lib, name).restype = C.c_int
+    _lib = lib
+    return lib
+
+
+def fma_peak_tflops(fp64=True):
+    lib = load_library()
+    v = C.c_double()
+    _check(lib.fin_fma_peak(1 if fp64 else 0, C.byref(v)))
+    return v.value
+
+
+def _check(rc):
+    if rc != FIN_OK:
+        raise FinError(rc, _lib.fin_last_error().decode())
+
+
+class Solver:
+    """One problem resident on the current CUDA device."""
+
+    def __init__(self, params: FinParams):
+        self.lib = load_library()
+        self.p = params.copy()
+        h = C.c_void_p()
+        _check(self.lib.fin_create(C.byref(self.p), C.byref(h)))
+        self.h = h
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.fin_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    # -- state -------------------------------------------------------------
+    def set_state(self, q, t=0.0):
+        q = np.ascontiguousarray(q, dtype=np.float64)
+        assert q.shape == ghosted_shape(self.p), (q.shape, ghosted_shape(self.p))
+        _check(self.lib.fin_set_state(self.h, q, t))
+
+    def get_state(self):
+        q = np.zeros(ghosted_shape(self.p))
+        t = C.c_double()
+        _check(self.lib.fin_get_state(self.h, q, C.byref(t)))
+        return q, t.value
+
+    # -- reference entry points -------------------------------------------
+    def ConstructL(self, q, smax=None):
+        q = np.ascontiguousarray(q, dtype=np.float64)
+        L = np.zeros(ghosted_shape(self.p))
+        sm = np.zeros(smax_shape(self.p)) if smax is None else np.ascontiguousarray(smax, dtype=np.float64).copy()
+        _check(self.lib.fin_construct_l(self.h, q, L, sm.ctypes.data_as(C.c_void_p)))
+        return L, sm
+
+    def GlobalWaveSpd(self, q):
+        a1, a2 = C.c_double(), C.c_double()
+        _check(self.lib.fin_global_wave_spd(self.h, np.ascontiguousarray(q, dtype=np.float64), C.byref(a1),
+                                            C.byref(a2)))
+        return a1.value, a2.value
+
+    def FinSolveRK(self, tend, dtv):
+        """Advance the device state to tend; dtv = [_, dt, max_dt] is updated in place."""
+        dtv = np.ascontiguousarray(dtv, dtype=np.float64)
+        n = C.c_int()
+        _check(self.lib.fin_solve(self.h, tend, dtv, C.byref(n)))
+        return dtv, n.value
+
+    def advance(self, tend, dtv, max_steps):
+        """FinSolveRK stopping after max_steps accepted steps; returns (dtv, nsteps)."""
+        dtv = np.ascontiguousarray(dtv, dtype=np.float64)
+        n = C.c_int()
+        _check(self.lib.fin_advance(self.h, tend, dtv, max_steps, C.byref(n)))
+        return dtv, n.value
+
+    def set_kernel_timing(self, on=True):
+        _check(self.lib.fin_set_kernel_timing(self.h, 1 if on else 0))
+
+    def kernel_time(self):
+        ms, n = C.c_double(), C.c_longlong()
+        _check(self.lib.fin_kernel_time(self.h, C.byref(ms), C.byref(n)))
+        return ms.value, n.value
+
+    def step_fixed(self, dt):
+        cfl = C.c_double()
+        _check(self.lib.fin_step_fixed(self.h, dt, C.byref(cfl)))
+        return cfl.value
+
+    def conservation_totals(self):
+        out = np.zeros(self.p.meqn)
+        _check(self.lib.fin_conservation_totals(self.h, out))
+        return out
+
+    def last_kernel_ms(self):
+        ms = C.c_double()
+        _check(self.lib.fin_last_kernel_ms(self.h, C.byref(ms)))
+        return ms.value
+
+    def launch_count(self):
+        n = C.c_longlong()
+        _check(self.lib.fin_launch_count(self.h, C.byref(n)))
+        return n.value

@@ -123,6 +123,11 @@ int fin_global_wave_spd(fin_solver* s, const double* q_host, double* alpha1, dou
  * nsteps_out (may be NULL) receives the number of accepted steps. */
 int fin_solve(fin_solver* s, double tend, double* dtv, int* nsteps_out);
 
+/* fin_solve that stops after max_steps accepted steps (or at tend).  The
+ * device time of the whole call, host waits included, is then available
+ * from fin_last_kernel_ms. */
+int fin_advance(fin_solver* s, double tend, double* dtv, int max_steps, int* nsteps_out);
+
 /* One time step of exactly dt with no CFL control (benchmarking and
  * per-step parity); cfl_out (may be NULL) receives GetCFL's value for it. */
 int fin_step_fixed(fin_solver* s, double dt, double* cfl_out);
@@ -131,9 +136,19 @@ int fin_step_fixed(fin_solver* s, double dt, double* cfl_out);
  * with compensated summation (lib/2d/ConSoln.cpp:52-64). totals[meqn]. */
 int fin_conservation_totals(fin_solver* s, double* totals);
 
-/* Device timing of the last fin_solve/fin_step_fixed call: milliseconds
- * spent in the stage kernels, measured with CUDA events on the solver's stream. */
+/* Device time of the last fin_solve/fin_advance/fin_step_fixed call in
+ * milliseconds (CUDA events on the solver's stream around the whole call). */
 int fin_last_kernel_ms(fin_solver* s, double* ms);
+
+/* With timing on, every stage-kernel launch is bracketed by CUDA events and
+ * its duration accumulated; fin_kernel_time returns the sum and the count
+ * since fin_set_kernel_timing was last called. */
+int fin_set_kernel_timing(fin_solver* s, int on);
+int fin_kernel_time(fin_solver* s, double* ms, long long* launches);
+
+/* Measured FMA throughput of the current device in TFLOP/s (FMA = 2 flops),
+ * FP64 (fp64 != 0) or FP32: the denominators of pipe-utilisation figures. */
+int fin_fma_peak(int fp64, double* tflops);
 
 /* Counts of kernel launches issued by this solver since creation. */
 int fin_launch_count(fin_solver* s, long long* launches);

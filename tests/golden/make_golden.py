@@ -1,0 +1,78 @@
+"""Generates the golden fixtures in this directory by running the reference's
+own sources (oracle/_ref/libfinref.so, built by ``make -C oracle ref`` from
+the reference checkout) on small seeded inputs.
+
+The reference repository stores no golden vectors for this path, so these
+files pin its behaviour: each .npz holds the inputs (ghosted q after the BC
+remap, parameters) and the reference's outputs.  Re-run with
+``python tests/golden/make_golden.py`` after ``make -C oracle ref``.
+"""
+import json
+import os
+import sys
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(os.path.dirname(HERE))
+sys.path.insert(0, ROOT)
+sys.path.insert(0, os.path.join(ROOT, "oracle"))
+
+from oracle import RefLib  # noqa: E402
+from finess_b200 import problems as P  # noqa: E402
+from finess_b200._abi import (FIN_BC_TRANSMISSIVE, FIN_TS_RK, FIN_WENO_FD, FIN_WENO_JS,  # noqa: E402
+                              FIN_WENO_Z)
+
+
+def params_json(p):
+    return json.dumps(p.as_dict())
+
+
+def construct_l_cases():
+    rng = np.random.default_rng(20261203)
+    cases = []
+    for weno, wname in ((FIN_WENO_JS, "js"), (FIN_WENO_Z, "z"), (FIN_WENO_FD, "fd")):
+        p = P.vortex_params(n=20, weno=weno)
+        p.my = 14
+        cases.append((f"constructl_{wname}_smooth_periodic", p, P.random_smooth_state(p, rng)))
+        p = P.riemann_params(n=18, weno=weno)
+        p.my = 22
+        cases.append((f"constructl_{wname}_riemann_transmissive", p, P.random_riemann_state(p, rng)))
+    # mixed boundaries and the local (non-global) LLF alpha
+    p = P.shock_entropy_params(nx=24, ny=12, weno=FIN_WENO_JS)
+    cases.append(("constructl_js_shock_entropy_mixed", p, P.shock_entropy_init(p)))
+    p = P.riemann_params(n=16, weno=FIN_WENO_Z, global_alpha=0)
+    cases.append(("constructl_z_riemann_local_alpha", p, P.riemann_init(p)))
+    return cases
+
+
+def main():
+    ref = RefLib()
+    for name, p, q in construct_l_cases():
+        q = ref.set_bnd(p, q)
+        L, smax = ref.construct_l(p, q)
+        a1, a2 = ref.global_wave_spd(p, q)
+        np.savez_compressed(os.path.join(HERE, name + ".npz"), params=params_json(p), q=q, L=L, smax=smax,
+                            alpha=np.array([a1, a2]))
+        print("wrote", name)
+
+    # Whole FinSolveRK frames (adaptive dt, accept/reject) on small grids.
+    runs = []
+    p = P.vortex_params(n=24, weno=FIN_WENO_JS)
+    runs.append(("finsolverk_js_vortex24", p, P.vortex_exact(p), 0.0, 0.5, 0.05))
+    p = P.riemann_params(n=32, weno=FIN_WENO_Z)
+    runs.append(("finsolverk_z_riemann32", p, P.riemann_init(p), 0.0, 0.05, 1e-3))
+    # a large initial dt forces step rejections (FinSolveRK.cpp:343-357)
+    p = P.riemann_params(n=20, weno=FIN_WENO_JS)
+    runs.append(("finsolverk_js_riemann20_reject", p, P.riemann_init(p), 0.0, 0.03, 0.05))
+    for name, p, q0, t0, tend, dt in runs:
+        q0 = ref.set_bnd(p, q0)
+        rc, q1, t1, dt1 = ref.finsolve(p, q0, t0, tend, dt)
+        assert rc == 0
+        np.savez_compressed(os.path.join(HERE, name + ".npz"), params=params_json(p), q0=q0, q1=q1,
+                            t0=t0, t1=t1, tend=tend, dt0=dt, dt1=dt1)
+        print("wrote", name, t1, dt1)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,166 @@
+"""CUDA path (through the C ABI) against the oracle and the reference's golden
+fixtures.  Tolerances, all relative L-infinity (max|a-b| / max|b|):
+
+* plain FP64 form: 1e-12 per ConstructL and per time step (the bar for the
+  plain method); FinSolveRK frames, whose adaptive dt follows the CFL of
+  every step, to 1e-11;
+* FP32-bulk form: stated per test against the FP64 result.
+"""
+import numpy as np
+import pytest
+
+from conftest import golden_cases, interior, load_golden, rel_linf
+from finess_b200 import problems as P
+from finess_b200._abi import (FIN_BC_PERIODIC, FIN_PREC_FP32, FIN_PREC_FP64, FIN_WENO_FD, FIN_WENO_JS,
+                              FIN_WENO_Z)
+
+pytestmark = pytest.mark.gpu
+
+TOL_STEP = 1e-12
+TOL_FRAME = 1e-11
+
+
+@pytest.fixture(scope="module")
+def Solver():
+    from finess_b200.solver import Solver as S
+    return S
+
+
+@pytest.mark.parametrize("path", golden_cases("constructl_"))
+def test_construct_l_golden(Solver, path):
+    g = load_golden(path)
+    p = g["p"]
+    with Solver(p) as s:
+        L, smax = s.ConstructL(g["q"])
+        a1, a2 = s.GlobalWaveSpd(g["q"])
+    assert rel_linf(interior(p, L), interior(p, g["L"])) <= TOL_STEP
+    assert rel_linf(smax, g["smax"]) <= 1e-14
+    assert abs(a1 - g["alpha"][0]) <= 1e-15 * g["alpha"][0]
+    assert abs(a2 - g["alpha"][1]) <= 1e-15 * g["alpha"][1]
+
+
+@pytest.mark.parametrize("path", golden_cases("finsolverk_"))
+def test_finsolve_rk_golden(Solver, path):
+    g = load_golden(path)
+    p = g["p"]
+    with Solver(p) as s:
+        s.set_state(g["q0"], float(g["t0"]))
+        dtv, n = s.FinSolveRK(float(g["tend"]), [0.0, float(g["dt0"]), p.max_dt])
+        q1, t1 = s.get_state()
+    assert rel_linf(interior(p, q1), interior(p, g["q1"])) <= TOL_FRAME
+    assert abs(t1 - float(g["t1"])) <= 1e-14 * abs(float(g["t1"]))
+    assert abs(dtv[1] - float(g["dt1"])) <= 1e-10 * float(g["dt1"])
+
+
+@pytest.mark.parametrize("weno", [FIN_WENO_JS, FIN_WENO_Z, FIN_WENO_FD])
+@pytest.mark.parametrize("kind", ["riemann", "smooth", "shock_entropy"])
+def test_step_vs_oracle(Solver, oracle, weno, kind):
+    """Three RK3 steps of fixed dt on ragged grids (sizes not multiples of the tile)."""
+    rng = np.random.default_rng(11)
+    if kind == "riemann":
+        p = P.riemann_params(n=45, weno=weno)
+        p.my = 37
+        q = P.random_riemann_state(p, rng)
+    elif kind == "smooth":
+        p = P.vortex_params(n=33, weno=weno)
+        p.my = 50
+        q = P.random_smooth_state(p, rng)
+    else:
+        p = P.shock_entropy_params(nx=70, ny=17, weno=weno)
+        q = P.shock_entropy_init(p)
+    q = oracle.set_bnd(p, q)
+    dt = 0.2 * min((p.xhigh - p.xlow) / p.mx, (p.yhigh - p.ylow) / p.my) / 4.0
+    with Solver(p) as s:
+        s.set_state(q)
+        qo = q
+        for _ in range(3):
+            cfl_g = s.step_fixed(dt)
+            qo, cfl_o = oracle.step_fixed(p, qo, dt)
+            qg, _ = s.get_state()
+            assert rel_linf(interior(p, qg), interior(p, qo)) <= TOL_STEP
+            assert abs(cfl_g - cfl_o) <= 1e-14 * cfl_o
+
+
+def test_local_alpha_and_power(Solver, oracle):
+    """global_alpha off (pure local LLF) and a non-default WENO power."""
+    rng = np.random.default_rng(3)
+    p = P.riemann_params(n=30, weno=FIN_WENO_JS, global_alpha=0, power_param=1.5)
+    q = oracle.set_bnd(p, P.random_riemann_state(p, rng))
+    with Solver(p) as s:
+        L, smax = s.ConstructL(q)
+    Lo, so = oracle.construct_l(p, q)
+    assert rel_linf(interior(p, L), interior(p, Lo)) <= TOL_STEP
+    assert rel_linf(smax, so) <= 1e-14
+
+
+def test_tiny_and_single_row_grids(Solver, oracle):
+    """Edge sizes: grids smaller than one tile, a single row (transmissive)."""
+    rng = np.random.default_rng(5)
+    for mx, my in ((3, 3), (1, 9), (9, 1), (17, 2)):
+        p = P.riemann_params(n=mx, weno=FIN_WENO_Z)
+        p.my = my
+        q = oracle.set_bnd(p, P.random_riemann_state(p, rng))
+        with Solver(p) as s:
+            L, smax = s.ConstructL(q)
+        Lo, so = oracle.construct_l(p, q)
+        assert rel_linf(interior(p, L), interior(p, Lo)) <= TOL_STEP, (mx, my)
+        assert rel_linf(smax, so) <= 1e-14
+
+
+def test_parity_256_riemann_frame(Solver, oracle):
+    """A whole adaptive-dt frame at 128x128 against the oracle."""
+    p = P.riemann_params(n=128, weno=FIN_WENO_Z)
+    q = oracle.set_bnd(p, P.riemann_init(p))
+    rc, qo, to, dto, n = oracle.finsolve(p, q, 0.0, 0.02, 1e-3)
+    with Solver(p) as s:
+        s.set_state(q)
+        dtv, ng = s.FinSolveRK(0.02, [0.0, 1e-3, p.max_dt])
+        qg, tg = s.get_state()
+    assert ng == n
+    assert rel_linf(interior(p, qg), interior(p, qo)) <= TOL_FRAME
+
+
+def test_periodic_conservation_and_shift(Solver):
+    """Size-independent properties at 1024^2: periodic totals conserved to
+    round-off, and a periodic shift of the data shifts the result exactly."""
+    p = P.vortex_params(n=1024)
+    q0 = P.vortex_exact(p)
+    dt = 0.002
+    with Solver(p) as s:
+        s.set_state(q0)
+        t0 = s.conservation_totals()
+        for _ in range(3):
+            s.step_fixed(dt)
+        t1 = s.conservation_totals()
+        qa, _ = s.get_state()
+    assert np.all(np.abs(t1 - t0) <= 1e-12 * np.maximum(1.0, np.abs(t0)))
+    mb = p.mbc
+    qs = q0.copy()
+    qs[mb:mb + p.mx, mb:mb + p.my] = np.roll(interior(p, q0), (37, -101), axis=(0, 1))
+    with Solver(p) as s:
+        s.set_state(qs)
+        for _ in range(3):
+            s.step_fixed(dt)
+        qb, _ = s.get_state()
+    assert np.array_equal(interior(p, qb), np.roll(interior(p, qa), (37, -101), axis=(0, 1)))
+
+
+@pytest.mark.parametrize("weno", [FIN_WENO_JS, FIN_WENO_Z])
+def test_fp32_bulk_vs_fp64(Solver, weno):
+    """FP32 reconstruction/splitting/projection with FP64 state: per-step
+    relative L-infinity against the FP64 form below 1e-5."""
+    p64 = P.riemann_params(n=96, weno=weno)
+    q = P.riemann_init(p64)
+    p32 = p64.copy()
+    p32.precision = FIN_PREC_FP32
+    dt = 2e-4
+    with Solver(p64) as a, Solver(p32) as b:
+        a.set_state(q)
+        b.set_state(q)
+        for _ in range(5):
+            a.step_fixed(dt)
+            b.step_fixed(dt)
+        qa, _ = a.get_state()
+        qb, _ = b.get_state()
+    err = rel_linf(interior(p64, qb), interior(p64, qa))
+    assert err <= 1e-5, err
