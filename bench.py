@@ -229,7 +229,12 @@ def main():
     s = Solver(p)
     s.set_state(q0, 0.0)
     tend = 0.8
-    dtv = np.array([0.0, p.initial_dt, p.max_dt])
+    # initial_dt of parameters.ini chosen for this grid: desired CFL at the
+    # initial maximum wave speed
+    a1, a2 = s.GlobalWaveSpd(q0)
+    dt0 = p.desired_cfl * min((p.xhigh - p.xlow) / p.mx, (p.yhigh - p.ylow) / p.my) / max(a1, a2)
+    s.set_state(q0, 0.0)
+    dtv = np.array([0.0, dt0, p.max_dt])
     dtv, _ = s.advance(tend, dtv, args.warmup)
 
     # ---- timed region: K steps, device-resident state ----
@@ -288,7 +293,7 @@ def main():
         barrier()
         t0 = time.perf_counter()
         s.set_state(qh, 0.0)
-        dtv2, n2 = s.advance(tend, np.array([0.0, dtv[1], p.max_dt]), args.steps)
+        dtv2, n2 = s.advance(tend, np.array([0.0, dt0, p.max_dt]), args.steps)
         qout, _ = s.get_state()
         barrier()
         e2e_s = time.perf_counter() - t0

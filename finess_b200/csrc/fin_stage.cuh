@@ -188,14 +188,16 @@ __global__ void __launch_bounds__(Cfg::NT, 1) k_stage(const StageArgs a)
 #pragma unroll
             for (int m = 0; m < MEQN; m++) Fh[m * (TI + 1) * TJ + fi * TJ + fj] = o[m];
             const int gfi = i0 + fi, gj = j0 + fj;
-            if (gfi < mx && gj < my) smax_x = Max(smax_x, alpha);
+            // GetCFL's Max skips NaN entries (Max(NaN, c) = c), so only
+            // finite face speeds enter the CFL maximum.
+            if (gfi < mx && gj < my && alpha <= R(1e30)) smax_x = Max(smax_x, alpha);
             if (a.face_alpha_x && gfi <= mx && gj < my) a.face_alpha_x[size_t(gfi) * my + gj] = double(alpha);
         } else {
             const R o[MEQN] = {fh[0], fh[2], fh[1], fh[3], fh[4]};
 #pragma unroll
             for (int m = 0; m < MEQN; m++) Gh[m * TI * (TJ + 1) + fi * (TJ + 1) + fj] = o[m];
             const int gi = i0 + fi, gfj = j0 + fj;
-            if (gi < mx && gfj < my) smax_y = Max(smax_y, alpha);
+            if (gi < mx && gfj < my && alpha <= R(1e30)) smax_y = Max(smax_y, alpha);
             if (a.face_alpha_y && gi < mx && gfj <= my) a.face_alpha_y[size_t(gi) * (my + 1) + gfj] = double(alpha);
         }
     }
@@ -230,8 +232,8 @@ __global__ void __launch_bounds__(Cfg::NT, 1) k_stage(const StageArgs a)
             const double sx = Euler::cell_speed(Euler::cell(gam, qn));
             const double sy = Euler::cell_speed(Euler::cell(gam, qy));
             if (!(sx <= 1e300) || !(sy <= 1e300)) nonfinite = true;
-            cs_x = Max(cs_x, sx);
-            cs_y = Max(cs_y, sy);
+            if (sx <= 1e300) cs_x = Max(cs_x, sx);
+            if (sy <= 1e300) cs_y = Max(cs_y, sy);
         }
     }
 

@@ -41,7 +41,9 @@ int set_err(int code, const std::string& msg)
 using Cfg = TileCfg<16, 16, 288>;
 
 // Reduction slots (doubles) in one device block, reset by one memset per step.
-enum { SLOT_SMAX = 0, SLOT_ALPHA = 2, NSLOTS = 2 + 2 * 4 };
+// The status word (bit 0: non-finite speed or state, bit 1: negative p or rho)
+// sits in slot STATUS so one copy returns it with the maxima.
+enum { SLOT_SMAX = 0, SLOT_ALPHA = 2, SLOT_STATUS = 10, NSLOTS = 11 };
 
 }  // namespace
 
@@ -92,8 +94,8 @@ __global__ void k_wave_spd_max(const double* q, int mx, int my, size_t plane, do
         const double sx = Euler::cell_speed(Euler::cell(gamma, Q));
         const double sy = Euler::cell_speed(Euler::cell(gamma, Qy));
         if (!(sx <= 1e300) || !(sy <= 1e300)) nonfinite = true;
-        ax = Max(ax, sx);
-        ay = Max(ay, sy);
+        if (sx <= 1e300) ax = Max(ax, sx);
+        if (sy <= 1e300) ay = Max(ay, sy);
     }
     if (!(ax <= 1e300)) ax = 0.0;
     if (!(ay <= 1e300)) ay = 0.0;
@@ -306,8 +308,10 @@ int take_stages(fin_solver* s, double dt, int nxt)
     for (int b = 0; b < 4 && k < 2; b++)
         if (b != qn && b != nxt) reg[k++] = b;
     const int q1 = reg[0], q2 = reg[1];
-    // reset smax and the alpha slots of the three buffers written this step
+    // reset smax, the status word and the alpha slots of the three buffers
+    // written this step
     CK(cudaMemsetAsync(s->slots + SLOT_SMAX, 0, 2 * sizeof(double), s->stream));
+    CK(cudaMemsetAsync(s->slots + SLOT_STATUS, 0, sizeof(double), s->stream));
     CK(cudaMemsetAsync(alpha_slot(s, q1), 0, 2 * sizeof(double), s->stream));
     CK(cudaMemsetAsync(alpha_slot(s, q2), 0, 2 * sizeof(double), s->stream));
     CK(cudaMemsetAsync(alpha_slot(s, nxt), 0, 2 * sizeof(double), s->stream));
@@ -339,11 +343,16 @@ int take_stages(fin_solver* s, double dt, int nxt)
 // GetCFL (lib/2d/GetCFL.cpp:31-73) from the step's face-speed maxima: the
 // maximum of dt*smax/dx over faces equals dt*max(smax)/dx because the
 // rounded product and quotient are monotone in smax.
-int get_cfl(fin_solver* s, double dt, double dtmax, double* cfl)
+// *nonfinite reports NaN/Inf met during the step: like the reference, such a
+// step is judged by the CFL of its finite face speeds (a rejected step is
+// simply retried); the caller refuses to accept it.
+int get_cfl(fin_solver* s, double dt, double dtmax, double* cfl, bool* nonfinite)
 {
     CK(cudaMemcpyAsync(s->h_slots, s->slots, NSLOTS * sizeof(double), cudaMemcpyDeviceToHost, s->stream));
-    int rc = check_status(s);   // synchronizes the stream
-    if (rc) return rc;
+    CK(cudaStreamSynchronize(s->stream));
+    unsigned int st;
+    memcpy(&st, s->h_slots + SLOT_STATUS, sizeof(st));
+    *nonfinite = (st & 1u) != 0;
     if (dt > dtmax) return set_err(FIN_ERR_DT_BOUNDS, "dt is out of bounds");
     double c = -100.0;
     c = Max(dt * s->h_slots[SLOT_SMAX] / s->dx, c);
@@ -441,15 +450,15 @@ int fin_create(const fin_params* p, fin_solver** out)
     cudaError_t e;
     for (int b = 0; b < 4; b++)
         if ((e = cudaMalloc(&s->q[b], MEQN * s->plane * sizeof(double))) != cudaSuccess) return fail(e, "cudaMalloc state");
-    if ((e = cudaMalloc(&s->slots, NSLOTS * sizeof(double) + 64)) != cudaSuccess) return fail(e, "cudaMalloc slots");
-    s->status = reinterpret_cast<unsigned int*>(s->slots + NSLOTS);
+    if ((e = cudaMalloc(&s->slots, NSLOTS * sizeof(double))) != cudaSuccess) return fail(e, "cudaMalloc slots");
+    s->status = reinterpret_cast<unsigned int*>(s->slots + SLOT_STATUS);
     if ((e = cudaMallocHost(&s->h_slots, NSLOTS * sizeof(double))) != cudaSuccess) return fail(e, "cudaMallocHost");
     if ((e = cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking)) != cudaSuccess) return fail(e, "stream");
     if ((e = cudaEventCreate(&s->ev0)) != cudaSuccess) return fail(e, "event");
     if ((e = cudaEventCreate(&s->ev1)) != cudaSuccess) return fail(e, "event");
     for (int k = 0; k < 6; k++)
         if ((e = cudaEventCreate(&s->kev[k])) != cudaSuccess) return fail(e, "event");
-    if ((e = cudaMemsetAsync(s->slots, 0, NSLOTS * sizeof(double) + 64, s->stream)) != cudaSuccess) return fail(e, "memset");
+    if ((e = cudaMemsetAsync(s->slots, 0, NSLOTS * sizeof(double), s->stream)) != cudaSuccess) return fail(e, "memset");
     for (int b = 0; b < 4; b++)
         if ((e = cudaMemsetAsync(s->q[b], 0, MEQN * s->plane * sizeof(double), s->stream)) != cudaSuccess) return fail(e, "memset");
     if ((e = cudaStreamSynchronize(s->stream)) != cudaSuccess) return fail(e, "sync");
@@ -488,6 +497,7 @@ static int upload(fin_solver* s, const double* q_host, int buf)
 {
     int rc = ensure_aos(s);
     if (rc) return rc;
+    CK(cudaMemsetAsync(s->slots + SLOT_STATUS, 0, sizeof(double), s->stream));
     CK(cudaMemcpyAsync(s->d_aos, q_host, s->aos_elems * sizeof(double), cudaMemcpyHostToDevice, s->stream));
     const size_t n = size_t(s->p.mx) * s->p.my;
     k_aos_to_planes<<<grid_blocks(n), 256, 0, s->stream>>>(s->d_aos, s->q[buf], s->p.mx, s->p.my, s->p.mbc, s->plane);
@@ -502,10 +512,10 @@ int fin_set_state(fin_solver* s, const double* q_host, double t)
     int rc = upload(s, q_host, s->cur);
     if (rc) return rc;
     s->t = t;
+    CK(cudaMemsetAsync(s->slots + SLOT_STATUS, 0, sizeof(double), s->stream));
     if ((rc = compute_alpha(s, s->cur))) return rc;
-    CK(cudaStreamSynchronize(s->stream));
     s->alpha_valid = true;
-    return FIN_OK;
+    return check_status(s);
 }
 
 int fin_get_state(fin_solver* s, double* q_host, double* t)
@@ -611,8 +621,10 @@ int fin_step_fixed(fin_solver* s, double dt, double* cfl_out)
     if ((rc = take_stages(s, dt, nxt))) return rc;
     CK(cudaEventRecord(s->ev1, s->stream));
     double cfl = 0.0;
-    if ((rc = get_cfl(s, dt, 1e300, &cfl))) return rc;
+    bool nonfinite = false;
+    if ((rc = get_cfl(s, dt, 1e300, &cfl, &nonfinite))) return rc;
     if ((rc = collect_kernel_times(s))) return rc;
+    if (nonfinite) return set_err(FIN_ERR_NONFINITE, "non-finite wave speed or state");
     float ms = 0.f;
     CK(cudaEventElapsedTime(&ms, s->ev0, s->ev1));
     s->last_ms = ms;
@@ -654,7 +666,8 @@ int fin_advance(fin_solver* s, double tend, double* dtv, int max_steps, int* nst
             t = told + dt;
             const int nxt = (s->cur + 3) % 4;
             if ((rc = take_stages(s, dt, nxt))) goto done;
-            if ((rc = get_cfl(s, dt, dtv[2], &cfl))) goto done;
+            bool nonfinite = false;
+            if ((rc = get_cfl(s, dt, dtv[2], &cfl, &nonfinite))) goto done;
             if ((rc = collect_kernel_times(s))) goto done;
             // Qstar/Qnew time bookkeeping of UpdateSoln.cpp:27 for the 3 stages
             t_star = 1.0 * s->t + 0.0 * t_star + 1.0 * dt;
@@ -664,6 +677,10 @@ int fin_advance(fin_solver* s, double tend, double* dtv, int max_steps, int* nst
             else dt = dtv[2];
             if (p.verbosity)
                 printf("FinSolveRK2D ... Step%5d   CFL =%6.3f   dt =%11.3e   t =%11.3e\n", n_step, cfl, dt, t);
+            if (cfl <= CFL_max && nonfinite) {
+                rc = set_err(FIN_ERR_NONFINITE, "non-finite wave speed or state in an accepted step");
+                goto done;
+            }
             if (cfl <= CFL_max) {
                 m_accept = 1;
                 s->cur = nxt;          // accept: q^{n+1} becomes q^n (alpha slot travels with it)

@@ -70,12 +70,21 @@ def test_step_vs_oracle(Solver, oracle, weno, kind):
         q = P.shock_entropy_init(p)
     q = oracle.set_bnd(p, q)
     dt = 0.2 * min((p.xhigh - p.xlow) / p.mx, (p.yhigh - p.ylow) / p.my) / 4.0
+    from finess_b200.solver import FinError
     with Solver(p) as s:
         s.set_state(q)
         qo = q
         for _ in range(3):
-            cfl_g = s.step_fixed(dt)
             qo, cfl_o = oracle.step_fixed(p, qo, dt)
+            if not np.all(np.isfinite(interior(p, qo))):
+                # FD5 (linear weights, no limiting) at a jump goes negative and
+                # NaN in the reference too; the C ABI reports it as an error.
+                with pytest.raises(FinError) as ei:
+                    s.step_fixed(dt)
+                assert ei.value.code == 7
+                assert weno == FIN_WENO_FD
+                return
+            cfl_g = s.step_fixed(dt)
             qg, _ = s.get_state()
             assert rel_linf(interior(p, qg), interior(p, qo)) <= TOL_STEP
             assert abs(cfl_g - cfl_o) <= 1e-14 * cfl_o
@@ -107,7 +116,7 @@ def test_tiny_and_single_row_grids(Solver, oracle):
         assert rel_linf(smax, so) <= 1e-14
 
 
-def test_parity_256_riemann_frame(Solver, oracle):
+def test_parity_128_riemann_frame(Solver, oracle):
     """A whole adaptive-dt frame at 128x128 against the oracle."""
     p = P.riemann_params(n=128, weno=FIN_WENO_Z)
     q = oracle.set_bnd(p, P.riemann_init(p))
@@ -164,3 +173,32 @@ def test_fp32_bulk_vs_fp64(Solver, weno):
         qb, _ = b.get_state()
     err = rel_linf(interior(p64, qb), interior(p64, qa))
     assert err <= 1e-5, err
+
+
+def test_oversized_first_dt_is_rejected_and_retried(Solver, oracle):
+    """initial_dt above the CFL limit: the first attempt is rejected
+    (FinSolveRK.cpp:343-357) and retried with dt*desired_cfl/cfl."""
+    p = P.riemann_params(n=64, weno=FIN_WENO_Z)
+    q = oracle.set_bnd(p, P.riemann_init(p))
+    rc, qo, to, dto, n = oracle.finsolve(p, q, 0.0, 0.01, 0.004)   # first CFL ~0.6 > max_cfl 0.45
+    with Solver(p) as s:
+        s.set_state(q)
+        dtv, ng = s.FinSolveRK(0.01, [0.0, 0.004, p.max_dt])
+        qg, tg = s.get_state()
+    assert rc == 0 and ng == n
+    assert rel_linf(interior(p, qg), interior(p, qo)) <= TOL_FRAME
+    assert abs(dtv[1] - dto) <= 1e-10 * dto
+
+
+def test_nan_producing_attempt_is_rejected_not_fatal(Solver):
+    """A first dt so large that the attempt produces NaNs (CFL ~80): the
+    reference's GetCFL skips NaN faces, rejects the step and retries; so does
+    the C ABI, which only reports an error if such a step would be accepted."""
+    p = P.riemann_params(n=64, weno=FIN_WENO_Z)
+    q = P.riemann_init(p)
+    with Solver(p) as s:
+        s.set_state(q)
+        dtv, ng = s.FinSolveRK(0.01, [0.0, 0.5, p.max_dt])
+        qg, tg = s.get_state()
+    assert ng > 0 and abs(tg - 0.01) < 1e-12
+    assert np.all(np.isfinite(interior(p, qg)))
