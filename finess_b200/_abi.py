@@ -39,6 +39,8 @@ class FinParams(C.Structure):
         ("bc_xlow", C.c_int), ("bc_xhigh", C.c_int), ("bc_ylow", C.c_int), ("bc_yhigh", C.c_int),
         ("physics", C.c_int),
         ("precision", C.c_int),
+        ("tfinal", C.c_double),
+        ("nout", C.c_int),
     ]
 
     def copy(self):
@@ -68,6 +70,7 @@ def default_params(**overrides):
     p.bc_xlow = p.bc_xhigh = p.bc_ylow = p.bc_yhigh = FIN_BC_PERIODIC
     p.physics = FIN_PHYS_EULER
     p.precision = FIN_PREC_FP64
+    p.tfinal, p.nout = 0.0, 1
     for k, v in overrides.items():
         if not hasattr(p, k):
             raise AttributeError(f"fin_params has no field {k!r}")

@@ -415,6 +415,8 @@ void fin_params_default(fin_params* p)
     p->bc_xlow = p->bc_xhigh = p->bc_ylow = p->bc_yhigh = FIN_BC_PERIODIC;
     p->physics = FIN_PHYS_EULER;
     p->precision = FIN_PREC_FP64;
+    p->tfinal = 0.0;
+    p->nout = 1;
 }
 
 const char* fin_last_error(void) { return g_err.c_str(); }

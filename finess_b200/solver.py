@@ -59,6 +59,9 @@ def load_library(path=LIB_PATH):
     lib.fin_set_kernel_timing.argtypes = [vp, C.c_int]
     lib.fin_kernel_time.argtypes = [vp, C.POINTER(C.c_double), C.POINTER(C.c_longlong)]
     lib.fin_fma_peak.argtypes = [C.c_int, C.POINTER(C.c_double)]
+    lib.fin_params_from_ini.argtypes = [C.c_char_p, P]
+    lib.fin_params_from_ini.restype = C.c_int
+    lib.fin_ini_last_error.restype = C.c_char_p
     for name in ("fin_create", "fin_destroy", "fin_set_state", "fin_get_state", "fin_construct_l",
                  "fin_global_wave_spd", "fin_solve", "fin_step_fixed", "fin_conservation_totals",
                  "fin_last_kernel_ms", "fin_launch_count", "fin_device_layout", "fin_state_device_ptr",
@@ -66,6 +69,16 @@ def load_library(path=LIB_PATH):
         getattr(lib, name).restype = C.c_int
     _lib = lib
     return lib
+
+
+def params_from_ini(path):
+    """parameters.ini -> FinParams through the library's reader."""
+    lib = load_library()
+    p = FinParams()
+    rc = lib.fin_params_from_ini(os.fsencode(path), C.byref(p))
+    if rc != FIN_OK:
+        raise FinError(rc, lib.fin_ini_last_error().decode())
+    return p
 
 
 def fma_peak_tflops(fp64=True):

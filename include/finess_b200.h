@@ -76,10 +76,24 @@ typedef struct fin_params {
     /* this library */
     int physics;                   /* enum fin_physics */
     int precision;                 /* enum fin_precision */
+    /* frame loop of RunFinpack (lib/2d/RunFinpack.cpp:95-130) */
+    double tfinal;
+    int nout;
 } fin_params;
 
 /* Defaults of python/finess/params/finess.py, weno.py and euler.py. */
 void fin_params_default(fin_params* p);
+
+/* Reads an application's parameters.ini (sections [finess], [grid], [weno],
+ * [euler] with the keys, defaults and checks of the reference's parameter
+ * specs, python/finess/params/{finess,dim2,weno,euler}.py, which its build
+ * compiles into IniParams, python/finess/params/params.py:358-497), plus an
+ * optional [finess_b200] section: bc_xlow/bc_xhigh/bc_ylow/bc_yhigh =
+ * periodic|transmissive and precision = fp64|fp32|hybrid.  Returns
+ * FIN_ERR_ARG with fin_ini_last_error() set when a check fails, where the
+ * reference's terminate() would throw (lib/sys/util.h:38-43). */
+int fin_params_from_ini(const char* path, fin_params* p);
+const char* fin_ini_last_error(void);
 
 /* Last error message of the calling thread (never NULL). */
 const char* fin_last_error(void);
