@@ -21,6 +21,8 @@ def _newest_source():
     newest = 0.0
     for d in (CSRC, os.path.join(ROOT, "include")):
         for dirpath, _, files in os.walk(d):
+            if os.path.basename(dirpath) == "shim":   # compiled into applications, not this library
+                continue
             for f in files:
                 if f.endswith((".cu", ".cuh", ".h", ".cpp")):
                     newest = max(newest, os.path.getmtime(os.path.join(dirpath, f)))

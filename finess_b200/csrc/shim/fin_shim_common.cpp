@@ -1,0 +1,120 @@
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <string>
+#include "IniParams.h"
+#include "fin_shim.h"
+
+void SetBndValues(StateVars& Q);   // the application's own (app_defined.h:10)
+
+namespace {
+
+fin_solver* g_solver = nullptr;
+fin_params g_key;   // parameters g_solver was created with (before the BC probe)
+
+// Reads the boundary condition of one side off the application's
+// SetBndValues: the probe's interior cell (i, j) holds the value
+// i*(my+2mbc)+j, so every ghost shows which interior cell it copied.
+// Periodic and zeroth-order extrapolation are the two remaps built.
+int classify(const dTensorBC3& q, int side, int mx, int my, int mbc)
+{
+    const double sy = my + 2 * mbc;
+    int periodic = 1, transmissive = 1;
+    for (int g = 1; g <= mbc; g++) {
+        const int n = (side < 2) ? my : mx;
+        for (int k = 1; k <= n; k++) {
+            int i, j, pi, pj, ti, tj;
+            if (side == 0) { i = 1 - g; j = k; pi = i + mx; pj = j; ti = 1; tj = j; }
+            else if (side == 1) { i = mx + g; j = k; pi = i - mx; pj = j; ti = mx; tj = j; }
+            else if (side == 2) { i = k; j = 1 - g; pi = i; pj = j + my; ti = i; tj = 1; }
+            else { i = k; j = my + g; pi = i; pj = j - my; ti = i; tj = my; }
+            const double v = q.get(i, j, 1);
+            if (v != pi * sy + pj) periodic = 0;
+            if (v != ti * sy + tj) transmissive = 0;
+        }
+    }
+    if (periodic) return FIN_BC_PERIODIC;
+    if (transmissive) return FIN_BC_TRANSMISSIVE;
+    return -1;
+}
+
+}  // namespace
+
+void fin_shim_check(int rc, const char* where)
+{
+    if (rc == FIN_OK) return;
+    printf(" Error in %s: %s (finess_b200 status %d)\n", where, fin_last_error(), rc);
+    exit(1);
+}
+
+fin_solver* fin_shim_solver()
+{
+    const IniParams& g = global_ini_params;
+    fin_params p;
+    fin_params_default(&p);
+    p.meqn = g.get_meqn(); p.maux = g.get_maux();
+    p.space_order = g.get_space_order(); p.time_order = g.get_time_order();
+    p.time_stepping_method = FIN_TS_RK;
+    p.global_alpha = g.get_global_alpha() ? 1 : 0;
+    p.source_term = g.get_source_term() ? 1 : 0;
+    p.nv = g.get_nv(); p.verbosity = g.get_verbosity();
+    p.initial_dt = g.get_initial_dt(); p.max_dt = g.get_max_dt();
+    p.max_cfl = g.get_max_cfl(); p.desired_cfl = g.get_desired_cfl();
+    p.mx = g.get_mx(); p.my = g.get_my(); p.mbc = g.get_mbc();
+    p.xlow = g.get_xlow(); p.xhigh = g.get_xhigh(); p.ylow = g.get_ylow(); p.yhigh = g.get_yhigh();
+    if (g.get_weno_version() == IniParams::WenoVersion::JS) p.weno_version = FIN_WENO_JS;
+    else if (g.get_weno_version() == IniParams::WenoVersion::Z) p.weno_version = FIN_WENO_Z;
+    else p.weno_version = FIN_WENO_FD;
+    p.epsilon = g.get_epsilon(); p.power_param = g.get_power_param(); p.alpha_scaling = g.get_alpha_scaling();
+    p.gamma = g.get_gamma();
+    // The solver is kept while the grid and method stay the same.
+    if (g_solver && memcmp(&p, &g_key, sizeof(p)) == 0) return g_solver;
+    g_key = p;
+    // Probe the application's SetBndValues.
+    {
+        StateVars probe(0.0, p.mx, p.my, p.meqn, (p.maux > 0 ? p.maux : 1), p.mbc);
+        dTensorBC3& q = probe.ref_q();
+        const double sy = p.my + 2 * p.mbc;
+        for (int i = 1; i <= p.mx; i++)
+            for (int j = 1; j <= p.my; j++)
+                for (int m = 1; m <= p.meqn; m++) q.set(i, j, m, i * sy + j);
+        SetBndValues(probe);
+        int* bc[4] = {&p.bc_xlow, &p.bc_xhigh, &p.bc_ylow, &p.bc_yhigh};
+        for (int side = 0; side < 4; side++) {
+            const int k = classify(q, side, p.mx, p.my, p.mbc);
+            if (k < 0) {
+                printf(" Error: SetBndValues side %d is neither periodic nor zeroth-order extrapolation;"
+                       " this library remaps only those two\n", side);
+                exit(1);
+            }
+            *bc[side] = k;
+        }
+    }
+    if (g_solver) fin_destroy(g_solver);
+    g_solver = nullptr;
+    fin_shim_check(fin_create(&p, &g_solver), "fin_create");
+    return g_solver;
+}
+
+void fin_shim_pack(const dTensorBC3& t, std::vector<double>& buf)
+{
+    const int n = t.numel();
+    buf.resize(n);
+    for (int k = 0; k < n; k++) buf[k] = t.vget(k);
+}
+
+void fin_shim_unpack_all(const std::vector<double>& buf, dTensorBC3& t)
+{
+    const int n = t.numel();
+    for (int k = 0; k < n; k++) t.vset(k, buf[k]);
+}
+
+void fin_shim_unpack_interior(const std::vector<double>& buf, dTensorBC3& t)
+{
+    const int mx = t.getsize(1), my = t.getsize(2), meqn = t.getsize(3), mbc = t.getmbc();
+    const int sy = my + 2 * mbc;
+    for (int i = 1; i <= mx; i++)
+        for (int j = 1; j <= my; j++)
+            for (int m = 1; m <= meqn; m++)
+                t.set(i, j, m, buf[((size_t)(i + mbc - 1) * sy + (j + mbc - 1)) * meqn + (m - 1)]);
+}

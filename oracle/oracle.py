@@ -27,6 +27,8 @@ from finess_b200._abi import FinParams, ghosted_shape, smax_shape  # noqa: E402
 _dp = np.ctypeslib.ndpointer(dtype=np.float64, flags="C_CONTIGUOUS")
 ORACLE_SO = os.path.join(HERE, "liboracle.so")
 REF_SO = os.path.join(HERE, "_ref", "libfinref.so")
+# the same reference objects relinked against libfinb200.so through the shim
+REF_SHIM_SO = os.path.join(HERE, "_ref", "libfinref_shim.so")
 
 
 def build_oracle():
@@ -128,11 +130,11 @@ class RefLib:
     """The reference's own compiled sources; available where oracle/_ref was built."""
 
     @staticmethod
-    def available():
-        return os.path.exists(REF_SO)
+    def available(path=REF_SO):
+        return os.path.exists(path)
 
-    def __init__(self):
-        lib = C.CDLL(REF_SO)
+    def __init__(self, path=REF_SO):
+        lib = C.CDLL(path)
         P = C.POINTER(FinParams)
         lib.ref_setup.argtypes = [P]
         lib.ref_set_bnd.argtypes = [_dp]
