@@ -174,6 +174,26 @@ int fin_device_layout(fin_solver* s, size_t* plane_stride, size_t* row_stride);
 /* Device pointer to the solver's current state planes (FP64). */
 int fin_state_device_ptr(fin_solver* s, double** q_dev);
 
+/* ---- for callers that cannot allocate device memory ------------------- */
+/* No counterpart in the reference.  For callers that must not call
+ * cudaMalloc (an application whose own allocator owns the device, or a loop
+ * that may not allocate once running): ConstructL, as fin_construct_l, but on
+ * device pointers in the reference's ghosted layout (q_dev read, L_dev's
+ * interior written, its ghosts untouched), enqueued on `stream` (a
+ * cudaStream_t; NULL = default stream) and returning without waiting.  All
+ * scratch lives in a static device array of this library (about 21 MB,
+ * held on every GPU that loads it until exit): no allocation of any kind.
+ *   - FP64 plain form only; mx*my must not exceed 262144 cells, larger
+ *     grids return FIN_ERR_SIZE.
+ *   - The first call on each device looks up the array's device address and
+ *     sets the kernels' shared-memory limit; make that first call before any
+ *     stream capture.
+ *   - Calls share the one array: calls that overlap on the GPU (other
+ *     streams, other threads) race; serialise them.
+ *   - Errors are reported by the return code only (fin_last_error does not
+ *     describe them); non-finite speeds are not reported. */
+int fin_construct_l_noalloc(const fin_params* p, const double* q_dev, double* L_dev, void* stream);
+
 #ifdef __cplusplus
 }
 #endif
