@@ -45,7 +45,35 @@ __device__ __forceinline__ void atomic_max_nonneg(double* addr, double v)
 template <class R> __host__ __device__ __forceinline__ R Max(R a, R b) { return a > b ? a : b; }
 template <class R> __host__ __device__ __forceinline__ R Min(R a, R b) { return a < b ? a : b; }
 
-template <class R> __device__ __forceinline__ R rcp(R x) { return R(1) / x; }
+// Reciprocal by Newton-Raphson refinement of the hardware approximation
+// (PTX rcp.approx.ftz): r <- r + r(1 - x r), which squares the relative error
+// per step.  Two steps bring the FP64 approximation to within an ulp or two
+// (the plain form's parity bar is 1e-12, four orders above); FP32 uses the
+// approximation alone (~1 ulp).  x = 0 gives NaN instead of Inf; every use
+// here divides by a density, pressure or WENO weight sum, where 0 is already
+// a failed state that the non-finite check reports.
+__device__ __forceinline__ double rcp(double x)
+{
+    double r;
+    asm("rcp.approx.ftz.f64 %0, %1;" : "=d"(r) : "d"(x));
+    double e = fma(-x, r, 1.0);
+    r = fma(r, e, r);
+    e = fma(-x, r, 1.0);
+    return fma(r, e, r);
+}
+__device__ __forceinline__ float rcp(float x)
+{
+    float r;
+    asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
+    return r;
+}
+__device__ __forceinline__ double fsqrt(double x) { return sqrt(x); }
+__device__ __forceinline__ float fsqrt(float x)
+{
+    float r;
+    asm("sqrt.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
+    return r;
+}
 
 // ---------------------------------------------------------------------------
 // Euler callbacks (apps/2d/euler/lib).  Component order inside a face is the
@@ -102,7 +130,7 @@ struct Euler {
         // Right projection uses sqrt(fabs()) (ProjectRightEig.cpp:42), the
         // left one plain sqrt (ProjectLeftEig.cpp:43): identical unless the
         // pressure is negative, where the left one is NaN.
-        e.c = sqrt(fabs(c2));
+        e.c = fsqrt(fabs(c2));
         e.cl = c2 < R(0) ? R(NAN) : e.c;
         e.H = (energy + press) * ir;
         e.hu2 = e.umag2 / R(2);
@@ -110,6 +138,52 @@ struct Euler {
         e.inv_cd = rcp(e.cl * d);
         e.inv_d2 = R(2) * rcp(d);
         return e;
+    }
+
+    // Per-face coefficients of the three full rows of the left projection
+    // (ProjectLeftEig.cpp:49-65): W0 = (a0 v1 + b0 v0 + c tail) inv_cd,
+    // W4 = (a4 v1 + b4 v0 + c tail) inv_cd, W1 = (e1 v0 + u1 v1 + u2 v2 + u3 v3 - v4) inv_d2,
+    // with tail = v4 - u2 v2 - u3 v3; rows 2 and 3 are v2 - u2 v0, v3 - u3 v0.
+    template <class R>
+    struct Rows { R a0, b0, a4, b4, e1; };
+
+    template <class R>
+    __device__ __forceinline__ static Rows<R> rows(const Eig<R>& e)
+    {
+        Rows<R> r;
+        const R c = e.cl;
+        r.a0 = e.hu2 - e.H - e.u1 * c;
+        r.b0 = e.hu2 * (c - e.u1) + e.H * e.u1;
+        r.a4 = e.H - e.hu2 - e.u1 * c;
+        r.b4 = e.hu2 * (c + e.u1) - e.H * e.u1;
+        r.e1 = e.H - e.umag2;
+        return r;
+    }
+
+    // Rows 0 and 4 of the left projection of one vector (normal frame).
+    template <class R>
+    __device__ __forceinline__ static void left04(const Eig<R>& e, const Rows<R>& r, const R* v, R& w0, R& w4)
+    {
+        const R ct = e.cl * (v[4] - e.u2 * v[2] - e.u3 * v[3]);
+        w0 = (r.a0 * v[1] + r.b0 * v[0] + ct) * e.inv_cd;
+        w4 = (r.a4 * v[1] + r.b4 * v[0] + ct) * e.inv_cd;
+    }
+    // Row 1 of the left projection of one vector (normal frame).
+    template <class R>
+    __device__ __forceinline__ static R left1(const Eig<R>& e, const Rows<R>& r, const R* v)
+    {
+        return (r.e1 * v[0] + e.u1 * v[1] + e.u2 * v[2] + e.u3 * v[3] - v[4]) * e.inv_d2;
+    }
+
+    // Rows 0, 1 and 4 of the left projection of one vector (normal frame).
+    template <class R>
+    __device__ __forceinline__ static void left014(const Eig<R>& e, const Rows<R>& r, const R* v, R& w0, R& w1, R& w4)
+    {
+        const R tail = v[4] - e.u2 * v[2] - e.u3 * v[3];
+        const R ct = e.cl * tail;
+        w0 = (r.a0 * v[1] + r.b0 * v[0] + ct) * e.inv_cd;
+        w4 = (r.a4 * v[1] + r.b4 * v[0] + ct) * e.inv_cd;
+        w1 = (r.e1 * v[0] + e.u1 * v[1] + e.u2 * v[2] + e.u3 * v[3] - v[4]) * e.inv_d2;
     }
 
     // ProjectLeftEig.cpp:47-66 for one point (normal frame in and out).
@@ -151,7 +225,7 @@ struct Euler {
         const R u1 = Qn[1] * ir, u2 = Qn[2] * ir, u3 = Qn[3] * ir;
         s.un = u1;
         s.p = (gamma - R(1)) * (Qn[4] - R(0.5) * s.rho * (u1 * u1 + u2 * u2 + u3 * u3));
-        s.c = sqrt(fabs(gamma * s.p * ir));
+        s.c = fsqrt(fabs(gamma * s.p * ir));
         return s;
     }
 
@@ -165,7 +239,7 @@ struct Euler {
         const R rho = R(0.5) * (l.rho + r.rho);
         const R un = R(0.5) * (l.un + r.un);
         const R press = R(0.5) * (l.p + r.p);
-        const R c = sqrt(fabs(gamma * press / rho));
+        const R c = fsqrt(fabs(gamma * press * rcp(rho)));
         if (press < R(0) || rho < R(0)) *neg = true;
         const R s1 = Min(l.un - l.c, un - c);
         const R s2 = Max(r.un + r.c, un + c);
@@ -245,7 +319,7 @@ __device__ __forceinline__ R weno5(const R* u, R eps, R pw)
             w2 = R(0.3) * (R(1) + pow(tau / (eps + b2), pw));
         }
     }
-    return (w0 * c0 + w1 * c1 + w2 * c2) / (w0 + w1 + w2);
+    return (w0 * c0 + w1 * c1 + w2 * c2) * rcp(w0 + w1 + w2);
 }
 
 }  // namespace fin

@@ -26,7 +26,7 @@ namespace {
 using namespace fin;
 // A type of this file's own, so the stage-kernel instantiations below are
 // distinct (internal-linkage) kernels, not a second copy of the main ones.
-struct NaCfg : TileCfg<16, 16, 288> {};
+struct NaCfg : TileCfg<15, 16, 256> {};
 
 constexpr size_t NA_MAX_CELLS = size_t(1) << 18;   // 262,144 interior cells (e.g. 512 x 512)
 constexpr size_t NA_SLOTS = 8;                      // [0..1] alpha x/y, [2..3] smax x/y, [4] status
@@ -189,6 +189,10 @@ extern "C" int fin_construct_l_noalloc(const fin_params* p, const double* q_dev,
     a.eps = p->epsilon;
     a.pw = p->power_param;
     a.alpha_scaling = p->alpha_scaling;
+    a.gamma_f = float(a.gamma);
+    a.eps_f = float(a.eps);
+    a.pw_f = float(a.pw);
+    a.alpha_scaling_f = float(a.alpha_scaling);
     a.alpha_in = p->global_alpha ? slots : nullptr;
     a.status = reinterpret_cast<unsigned int*>(slots + 4);
     a.bc[0] = p->bc_xlow; a.bc[1] = p->bc_xhigh; a.bc[2] = p->bc_ylow; a.bc[3] = p->bc_yhigh;

@@ -42,6 +42,7 @@ struct StageArgs {
     size_t plane;          // elements per component plane (>= mx*my)
     double rdx, rdy;       // 1/dx, 1/dy
     double gamma, eps, pw, alpha_scaling;
+    float gamma_f, eps_f, pw_f, alpha_scaling_f;   // the same in FP32 (set by the launcher)
     const double* alpha_in;   // [2] global alpha of q_in (x, y); nullptr = local LLF
     double* alpha_out;        // [2] max cell speed of q_out; nullptr = skip
     double* smax_out;         // [2] max face speed over GetCFL's faces; nullptr = skip
@@ -56,37 +57,114 @@ struct TileCfg {
     static constexpr int TI = TI_, TJ = TJ_, NT = NT_, H = 3;
     static constexpr int RI = TI + 2 * H, RJ = TJ + 2 * H;
     static constexpr int NFX = (TI + 1) * TJ, NFY = TI * (TJ + 1);
-    // byte offset of the reduction scratch (after the five arrays, 16-B aligned)
+    static constexpr int NPRIM = 4;   // per-cell u, v, p, c of the cross region
+    // byte offset of the reduction scratch (after the arrays, 16-B aligned)
     template <class R>
     __host__ __device__ static constexpr size_t red_offset()
     {
-        return (sizeof(R) * MEQN * (size_t(RI) * RJ + size_t(RI) * TJ + size_t(TI) * RJ +
-                                    size_t(TI + 1) * TJ + size_t(TI) * (TJ + 1)) + 15) / 16 * 16;
+        return (sizeof(R) * (size_t(MEQN) * (size_t(RI) * RJ + size_t(RI) * TJ + size_t(TI) * RJ +
+                                             size_t(TI + 1) * TJ + size_t(TI) * (TJ + 1)) +
+                             size_t(NPRIM) * RI * RJ) + 15) / 16 * 16;
     }
     template <class R>
     __host__ __device__ static constexpr size_t smem_bytes() { return red_offset<R>() + 4 * (NT / 32) * sizeof(double); }
 };
 
+// Resident blocks per SM the register budget is sized for: FP64 faces need
+// about 110 registers a thread, FP32 about 70.
+// Measured on B200 at 4096^2 (stage-kernel ms, FP64 / FP32): one block per
+// SM 5.81 / 2.71; two FP64 blocks (128 registers, ~200 B spilled to L1) and
+// three FP32 blocks 4.07 / 2.44.  More resident warps beat the spills.
+#ifndef FIN_MINB_F64
+#define FIN_MINB_F64 2
+#endif
+#ifndef FIN_MINB_F32
+#define FIN_MINB_F32 3
+#endif
+template <class R> struct MinBlocks { static constexpr int value = FIN_MINB_F64; };
+template <> struct MinBlocks<float> { static constexpr int value = FIN_MINB_F32; };
+
+// Scalar parameters read from kernel-parameter space where they are used
+// (keeps them out of the register budget of the face loop).
+template <class R> struct Par;
+template <> struct Par<double> {
+    __device__ static double gamma(const StageArgs& a) { return a.gamma; }
+    __device__ static double eps(const StageArgs& a) { return a.eps; }
+    __device__ static double pw(const StageArgs& a) { return a.pw; }
+    __device__ static double ascale(const StageArgs& a) { return a.alpha_scaling; }
+};
+template <> struct Par<float> {
+    __device__ static float gamma(const StageArgs& a) { return a.gamma_f; }
+    __device__ static float eps(const StageArgs& a) { return a.eps_f; }
+    __device__ static float pw(const StageArgs& a) { return a.pw_f; }
+    __device__ static float ascale(const StageArgs& a) { return a.alpha_scaling_f; }
+};
+
+// Scheduling fences: an empty volatile asm that reads and writes x.  Volatile
+// asm statements keep their order, so fencing the inputs and result of each
+// pair of WENO reconstructions stops the scheduler from evaluating all ten of
+// a face at once (which wants ~230 registers in FP64).
+__device__ __forceinline__ void fence(double& x) { asm volatile("" : "+d"(x)); }
+__device__ __forceinline__ void fence(float& x) { asm volatile("" : "+f"(x)); }
+template <class R>
+__device__ __forceinline__ void fence5(R* u)
+{
+#pragma unroll
+    for (int k = 0; k < 5; k++) fence(u[k]);
+}
+
+// gp and gm reconstructions of one characteristic field, fenced as a unit.
+template <class R, int VER, bool P2>
+__device__ __forceinline__ R weno_pair(R* up, R* um, R eps, R pw)
+{
+    fence5(up);
+    fence5(um);
+    R g = weno5<R, VER, P2>(up, eps, pw) + weno5<R, VER, P2>(um, eps, pw);
+    fence(g);
+    return g;
+}
+
+// Right projection (ProjectRightEig.cpp:46-62) of one characteristic field k
+// with amplitude gk, added into the face flux f[0..4] (normal frame).  The
+// projection is linear, so the face flux is accumulated field by field.
+template <class R>
+__device__ __forceinline__ void right_add(const typename Euler::Eig<R>& e, int k, R gk, R* f)
+{
+    if (k == 0) {
+        f[0] += gk; f[1] += (e.u1 - e.c) * gk; f[2] += e.u2 * gk; f[3] += e.u3 * gk; f[4] += (e.H - e.u1 * e.c) * gk;
+    } else if (k == 4) {
+        f[0] += gk; f[1] += (e.u1 + e.c) * gk; f[2] += e.u2 * gk; f[3] += e.u3 * gk; f[4] += (e.H + e.u1 * e.c) * gk;
+    } else if (k == 1) {
+        f[0] += gk; f[1] += e.u1 * gk; f[2] += e.u2 * gk; f[3] += e.u3 * gk; f[4] += e.hu2 * gk;
+    } else if (k == 2) {
+        f[2] += gk; f[4] += e.u2 * gk;
+    } else {
+        f[3] += gk; f[4] += e.u3 * gk;
+    }
+}
+
 template <class R, int VER, bool P2, class Cfg>
-__global__ void __launch_bounds__(Cfg::NT, 1) k_stage(const StageArgs a)
+__global__ void __launch_bounds__(Cfg::NT, MinBlocks<R>::value) k_stage(const StageArgs a)
 {
     constexpr int TI = Cfg::TI, TJ = Cfg::TJ, NT = Cfg::NT, H = Cfg::H;
     constexpr int RI = Cfg::RI, RJ = Cfg::RJ;
+    constexpr int PQ = RI * RJ;                    // plane size of qs and prim
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    R* qs = reinterpret_cast<R*>(smem_raw);
-    R* fs = qs + MEQN * RI * RJ;
-    R* gs = fs + MEQN * RI * TJ;
-    R* Fh = gs + MEQN * TI * RJ;
-    R* Gh = Fh + MEQN * (TI + 1) * TJ;
+    R* qs = reinterpret_cast<R*>(smem_raw);        // [M][RI][RJ]
+    R* fs = qs + MEQN * PQ;                        // [M][RI][TJ]   0.5 * f
+    R* gs = fs + MEQN * RI * TJ;                   // [M][TI][RJ]   0.5 * g
+    R* Fh = gs + MEQN * TI * RJ;                   // [M][TI+1][TJ]
+    R* Gh = Fh + MEQN * (TI + 1) * TJ;             // [M][TI][TJ+1]
+    R* prim = Gh + MEQN * TI * (TJ + 1);           // [4][RI][RJ]   u, v, p, c
     double* red = reinterpret_cast<double*>(smem_raw + Cfg::template red_offset<R>());
 
     const int tid = threadIdx.x;
     const int i0 = blockIdx.y * TI, j0 = blockIdx.x * TJ;
     const int mx = a.mx, my = a.my;
-    const R gamma = R(a.gamma);
+#define gamma (Par<R>::gamma(a))
 
     // ---- phase 0: load the tile + halo, boundary conditions by remap ----
-    for (int e = tid; e < RI * RJ; e += NT) {
+    for (int e = tid; e < PQ; e += NT) {
         const int ii = e / RJ, jj = e - ii * RJ;
         const bool xin = ii >= H && ii < H + TI, yin = jj >= H && jj < H + TJ;
         if (!xin && !yin) continue;
@@ -94,36 +172,53 @@ __global__ void __launch_bounds__(Cfg::NT, 1) k_stage(const StageArgs a)
         const int gj = bc_remap(j0 + jj - H, my, a.bc[2], a.bc[3]);
         const size_t g = size_t(gi) * my + gj;
 #pragma unroll
-        for (int m = 0; m < MEQN; m++) qs[m * RI * RJ + e] = R(__ldg(a.qin + m * a.plane + g));
+        for (int m = 0; m < MEQN; m++) qs[m * PQ + e] = R(__ldg(a.qin + m * a.plane + g));
     }
     __syncthreads();
 
-    // ---- phase 1: FluxFunc once per cell of the cross-shaped stencil region ----
-    for (int e = tid; e < RI * RJ; e += NT) {
+    // ---- phase 1: per cell of the cross region: FluxFunc (FluxFunc.cpp:19-42,
+    // once per cell instead of once per stencil point of every face), halved
+    // for the LLF split, and the cell's u, v, p, c for SetWaveSpd.cpp:24-50 ----
+    for (int e = tid; e < PQ; e += NT) {
         const int ii = e / RJ, jj = e - ii * RJ;
         const bool xin = ii >= H && ii < H + TI, yin = jj >= H && jj < H + TJ;
         if (!xin && !yin) continue;
-        R Q[MEQN], f[MEQN], g[MEQN];
-#pragma unroll
-        for (int m = 0; m < MEQN; m++) Q[m] = qs[m * RI * RJ + e];
-        Euler::flux(gamma, Q, f, g);
+        const R rho = qs[e], m1 = qs[PQ + e], m2 = qs[2 * PQ + e], m3 = qs[3 * PQ + e], en = qs[4 * PQ + e];
+        const R ir = rcp(rho);
+        const R u1 = m1 * ir, u2 = m2 * ir, u3 = m3 * ir;
+        const R press = (gamma - R(1)) * (en - R(0.5) * rho * (u1 * u1 + u2 * u2 + u3 * u3));
+        prim[e] = u1;
+        prim[PQ + e] = u2;
+        prim[2 * PQ + e] = press;
+        prim[3 * PQ + e] = fsqrt(fabs(gamma * press * ir));
+        const R hr = R(0.5) * rho, hep = R(0.5) * (en + press);
         if (yin) {
-#pragma unroll
-            for (int m = 0; m < MEQN; m++) fs[m * RI * TJ + ii * TJ + (jj - H)] = f[m];
+            const int o = ii * TJ + (jj - H);
+            fs[o] = hr * u1;
+            fs[RI * TJ + o] = hr * u1 * u1 + R(0.5) * press;
+            fs[2 * RI * TJ + o] = hr * u1 * u2;
+            fs[3 * RI * TJ + o] = hr * u1 * u3;
+            fs[4 * RI * TJ + o] = u1 * hep;
         }
         if (xin) {
-#pragma unroll
-            for (int m = 0; m < MEQN; m++) gs[m * TI * RJ + (ii - H) * RJ + jj] = g[m];
+            const int o = (ii - H) * RJ + jj;
+            gs[o] = hr * u2;
+            gs[TI * RJ + o] = hr * u2 * u1;
+            gs[2 * TI * RJ + o] = hr * u2 * u2 + R(0.5) * press;
+            gs[3 * TI * RJ + o] = hr * u2 * u3;
+            gs[4 * TI * RJ + o] = u2 * hep;
         }
     }
     __syncthreads();
 
     // ---- phase 2: one thread per face (x faces then y faces) ----
-    const R eps = R(a.eps), pw = R(a.pw), ascale = R(a.alpha_scaling);
+#define eps (Par<R>::eps(a))
+#define pw (Par<R>::pw(a))
     const R ag1 = a.alpha_in ? R(a.alpha_in[0]) : R(0);
     const R ag2 = a.alpha_in ? R(a.alpha_in[1]) : R(0);
     R smax_x = R(0), smax_y = R(0);
     bool neg = false, nonfinite = false;
+#pragma unroll 1
     for (int w = tid; w < Cfg::NFX + Cfg::NFY; w += NT) {
         const bool isx = w < Cfg::NFX;
         int fi, fj, qbase, qstr, fbase, fstr, fplane;
@@ -139,49 +234,128 @@ __global__ void __launch_bounds__(Cfg::NT, 1) k_stage(const StageArgs a)
             fl = gs; fbase = fi * RJ + (H + fj); fstr = 1; fplane = TI * RJ;
         }
         const int cn = isx ? 1 : 2, ct = isx ? 2 : 1;   // normal / tangential momentum
+        const int ql = qbase - qstr;
         // Face average (ConstructL.cpp:72-77) in the normal frame.
-        R Ql[MEQN], Qr[MEQN], Qa[MEQN];
-        {
-            const int ml[MEQN] = {0, cn, ct, 3, 4};
-#pragma unroll
-            for (int m = 0; m < MEQN; m++) {
-                Qr[m] = qs[ml[m] * RI * RJ + qbase];
-                Ql[m] = qs[ml[m] * RI * RJ + qbase - qstr];
-                Qa[m] = R(0.5) * (Qr[m] + Ql[m]);
-            }
-        }
-        // Local wave speed (SetWaveSpd.cpp) and LLF alpha (ConstructL.cpp:172-174).
-        const typename Euler::Cell<R> cl = Euler::cell(gamma, Ql), cr = Euler::cell(gamma, Qr);
-        const R sloc = Euler::speed(gamma, cl, cr, &neg);
-        const R alpha = Max(isx ? ag1 : ag2, sloc);
-        if (!(alpha <= R(1e30))) nonfinite = true;
-        const R la = ascale * alpha;
+        R Qa[MEQN];
+        Qa[0] = R(0.5) * (qs[qbase] + qs[ql]);
+        Qa[1] = R(0.5) * (qs[cn * PQ + qbase] + qs[cn * PQ + ql]);
+        Qa[2] = R(0.5) * (qs[ct * PQ + qbase] + qs[ct * PQ + ql]);
+        Qa[3] = R(0.5) * (qs[3 * PQ + qbase] + qs[3 * PQ + ql]);
+        Qa[4] = R(0.5) * (qs[4 * PQ + qbase] + qs[4 * PQ + ql]);
         const typename Euler::Eig<R> ev = Euler::eig(gamma, Qa);
-        // Project the 6-point stencil (ConstructL.cpp:140-141) and split
-        // (:179-185): gp_k(s) uses points s = 0..4, gm_k(s) points 5-s.
-        R gp[MEQN][5], gm[MEQN][5];
+        // SetWaveSpd.cpp:39-68 from the two cells' u_n, p, c (nmag = 1) and
+        // the LLF alpha of ConstructL.cpp:172-174.
+        R alpha;
+        {
+            const int un = isx ? 0 : 1;
+            const R unl = prim[un * PQ + ql], unr = prim[un * PQ + qbase];
+            const R pl = prim[2 * PQ + ql], pr = prim[2 * PQ + qbase];
+            const R cl = prim[3 * PQ + ql], cr = prim[3 * PQ + qbase];
+            const R rho = Qa[0];
+            const R ua = R(0.5) * (unl + unr);
+            const R pa = R(0.5) * (pl + pr);
+            const R ca = fsqrt(fabs(gamma * pa * rcp(rho)));
+            if (pa < R(0) || rho < R(0)) neg = true;
+            const R s1 = Min(unl - cl, ua - ca);
+            const R s2 = Max(unr + cr, ua + ca);
+            alpha = Max(isx ? ag1 : ag2, Max(fabs(s1), fabs(s2)));
+        }
+        if (!(alpha <= R(1e30))) nonfinite = true;
+        // gp = 0.5 (L f + l_alpha L q) = L (0.5 f + 0.5 l_alpha q), points
+        // 0..4; gm the same with -l_alpha, points 5..1 (ConstructL.cpp:179-185).
+        const R lah = R(0.5) * Par<R>::ascale(a) * alpha;
+        const typename Euler::Rows<R> rw = Euler::rows(ev);
+        R fh[MEQN] = {R(0), R(0), R(0), R(0), R(0)};
+        {
+            // pass 1: characteristic fields 0 and 4 (acoustic rows, shared tail)
+            R p0[5], p4[5], m0[5], m4[5];
 #pragma unroll
-        for (int s = 0; s < 6; s++) {
-            R Q[MEQN], F[MEQN], W[MEQN], G[MEQN];
-            const int ml[MEQN] = {0, cn, ct, 3, 4};
-#pragma unroll
-            for (int m = 0; m < MEQN; m++) {
-                Q[m] = qs[ml[m] * RI * RJ + qbase + (s - 3) * qstr];
-                F[m] = fl[ml[m] * fplane + fbase + (s - 3) * fstr];
+            for (int s = 0; s < 6; s++) {
+                // keep the compiler from hoisting every stencil point's loads
+                // ahead of the arithmetic (that would hold ~60 values live)
+                asm volatile("" ::: "memory");
+                const int oq = qbase + (s - 3) * qstr, of = fbase + (s - 3) * fstr;
+                const R q0 = qs[oq], qn = qs[cn * PQ + oq], qt = qs[ct * PQ + oq], qw = qs[3 * PQ + oq], qe = qs[4 * PQ + oq];
+                const R f0 = fl[of], fn = fl[cn * fplane + of], ft = fl[ct * fplane + of], fw = fl[3 * fplane + of],
+                        fe = fl[4 * fplane + of];
+                if (s < 5) {
+                    const R v[MEQN] = {f0 + lah * q0, fn + lah * qn, ft + lah * qt, fw + lah * qw, fe + lah * qe};
+                    Euler::left04(ev, rw, v, p0[s], p4[s]);
+                }
+                if (s > 0) {
+                    const R v[MEQN] = {f0 - lah * q0, fn - lah * qn, ft - lah * qt, fw - lah * qw, fe - lah * qe};
+                    Euler::left04(ev, rw, v, m0[5 - s], m4[5 - s]);
+                }
             }
-            Euler::left(ev, Q, W);
-            Euler::left(ev, F, G);
+            // one reconstruction pair per iteration; the loop is not unrolled,
+            // which keeps the scheduler from overlapping the two pairs
+#pragma unroll 1
+            for (int k = 0; k < 2; k++) {
+                R up[5], um[5];
 #pragma unroll
-            for (int k = 0; k < MEQN; k++) {
-                if (s < 5) gp[k][s] = R(0.5) * (G[k] + la * W[k]);
-                if (s > 0) gm[k][5 - s] = R(0.5) * (G[k] - la * W[k]);
+                for (int t = 0; t < 5; t++) {
+                    up[t] = k == 0 ? p0[t] : p4[t];
+                    um[t] = k == 0 ? m0[t] : m4[t];
+                }
+                right_add<R>(ev, k == 0 ? 0 : 4, weno_pair<R, VER, P2>(up, um, eps, pw), fh);
             }
         }
-        R gh[MEQN], fh[MEQN];
+        {
+            // pass 2: characteristic field 1 (the entropy-like row)
+            R p1[5], m1[5];
 #pragma unroll
-        for (int k = 0; k < MEQN; k++)
-            gh[k] = weno5<R, VER, P2>(gp[k], eps, pw) + weno5<R, VER, P2>(gm[k], eps, pw);
-        Euler::right(ev, gh, fh);
+            for (int s = 0; s < 6; s++) {
+                // keep the compiler from hoisting every stencil point's loads
+                // ahead of the arithmetic (that would hold ~60 values live)
+                asm volatile("" ::: "memory");
+                const int oq = qbase + (s - 3) * qstr, of = fbase + (s - 3) * fstr;
+                const R q0 = qs[oq], qn = qs[cn * PQ + oq], qt = qs[ct * PQ + oq], qw = qs[3 * PQ + oq], qe = qs[4 * PQ + oq];
+                const R f0 = fl[of], fn = fl[cn * fplane + of], ft = fl[ct * fplane + of], fw = fl[3 * fplane + of],
+                        fe = fl[4 * fplane + of];
+                if (s < 5) {
+                    const R v[MEQN] = {f0 + lah * q0, fn + lah * qn, ft + lah * qt, fw + lah * qw, fe + lah * qe};
+                    p1[s] = Euler::left1(ev, rw, v);
+                }
+                if (s > 0) {
+                    const R v[MEQN] = {f0 - lah * q0, fn - lah * qn, ft - lah * qt, fw - lah * qw, fe - lah * qe};
+                    m1[5 - s] = Euler::left1(ev, rw, v);
+                }
+            }
+            right_add<R>(ev, 1, weno_pair<R, VER, P2>(p1, m1, eps, pw), fh);
+        }
+        {
+            // pass 3: fields 2 and 3 (rows v_t - u2 v0 and v_w - u3 v0)
+            R p2[5], p3[5], m2[5], m3[5];
+#pragma unroll
+            for (int s = 0; s < 6; s++) {
+                // keep the compiler from hoisting every stencil point's loads
+                // ahead of the arithmetic (that would hold ~60 values live)
+                asm volatile("" ::: "memory");
+                const int oq = qbase + (s - 3) * qstr, of = fbase + (s - 3) * fstr;
+                const R q0 = qs[oq], qt = qs[ct * PQ + oq], qw = qs[3 * PQ + oq];
+                const R f0 = fl[of], ft = fl[ct * fplane + of], fw = fl[3 * fplane + of];
+                if (s < 5) {
+                    const R v0 = f0 + lah * q0;
+                    p2[s] = (ft + lah * qt) - ev.u2 * v0;
+                    p3[s] = (fw + lah * qw) - ev.u3 * v0;
+                }
+                if (s > 0) {
+                    const R v0 = f0 - lah * q0;
+                    m2[5 - s] = (ft - lah * qt) - ev.u2 * v0;
+                    m3[5 - s] = (fw - lah * qw) - ev.u3 * v0;
+                }
+            }
+#pragma unroll 1
+            for (int k = 0; k < 2; k++) {
+                R up[5], um[5];
+#pragma unroll
+                for (int t = 0; t < 5; t++) {
+                    up[t] = k == 0 ? p2[t] : p3[t];
+                    um[t] = k == 0 ? m2[t] : m3[t];
+                }
+                right_add<R>(ev, k == 0 ? 2 : 3, weno_pair<R, VER, P2>(up, um, eps, pw), fh);
+            }
+        }
         // Back to (rho, rho u, rho v, rho w, E) and store.
         if (isx) {
             const R o[MEQN] = {fh[0], fh[1], fh[2], fh[3], fh[4]};
@@ -202,6 +376,9 @@ __global__ void __launch_bounds__(Cfg::NT, 1) k_stage(const StageArgs a)
         }
     }
     __syncthreads();
+#undef gamma
+#undef eps
+#undef pw
 
     // ---- phase 3: flux difference, stage update, next-stage wave speed ----
     double cs_x = 0.0, cs_y = 0.0;

@@ -38,7 +38,12 @@ int set_err(int code, const std::string& msg)
 
 // Tile shape of the stage kernel: 16 x 16 cells, 544 faces over 288 threads
 // (two rounds of the face loop, the second 89% full).
-using Cfg = TileCfg<16, 16, 288>;
+#ifndef FIN_TILE_TI
+#define FIN_TILE_TI 15
+#define FIN_TILE_TJ 16
+#define FIN_TILE_NT 256
+#endif
+using Cfg = TileCfg<FIN_TILE_TI, FIN_TILE_TJ, FIN_TILE_NT>;
 
 // Reduction slots (doubles) in one device block, reset by one memset per step.
 // The status word (bit 0: non-finite speed or state, bit 1: negative p or rho)
@@ -254,6 +259,10 @@ StageArgs base_args(fin_solver* s)
     a.eps = s->p.epsilon;
     a.pw = s->p.power_param;
     a.alpha_scaling = s->p.alpha_scaling;
+    a.gamma_f = float(a.gamma);
+    a.eps_f = float(a.eps);
+    a.pw_f = float(a.pw);
+    a.alpha_scaling_f = float(a.alpha_scaling);
     a.status = s->status;
     a.bc[0] = s->p.bc_xlow; a.bc[1] = s->p.bc_xhigh;
     a.bc[2] = s->p.bc_ylow; a.bc[3] = s->p.bc_yhigh;

@@ -153,6 +153,81 @@ static void euler_wave_spd(double gamma, double n1, double n2, const double* Ql,
     *s2 = Max(unr + cr, un + c);
 }
 
+/* Directional derivatives of the Euler flux component d (0: f, 1: g) at Q.
+ * The reference tabulates the Jacobian and Hessian entry by entry
+ * (apps/2d/euler/lib/DFluxFunc.cpp:30-105, D2FluxFunc.cpp:44-300); for every
+ * 2D state (rho w = 0) its Jacobian entries are the exact derivatives, and its
+ * Hessian entries are exact except the energy-flux E cross terms (see
+ * euler_d2flux_dir).  These closed forms produce them:
+ *   du_k[a] = (a_k - u_k a_0)/rho,  dp[a] = (g-1)(a_4 - u.a_m + |u|^2 a_0/2),
+ *   f_0 = m_n, f_k = m_n u_k + delta_kn p, f_4 = (E+p) u_n  (n = 1+d),
+ *   d2u_k[a,b] = -(du_k[a] b_0 + du_k[b] a_0)/rho,
+ *   d2p[a,b] = -(g-1) rho du[a].du[b]. */
+static void euler_dflux_dir(double gamma, const double* Q, int d, const double* a, double* out)
+{
+    const int n = 1 + d;
+    const double rho = Q[0], u[3] = {Q[1] / rho, Q[2] / rho, Q[3] / rho}, E = Q[4];
+    const double uu = u[0] * u[0] + u[1] * u[1] + u[2] * u[2];
+    const double p = (gamma - 1.0) * (E - 0.5 * rho * uu);
+    double du[3];
+    for (int k = 0; k < 3; k++) du[k] = (a[k + 1] - u[k] * a[0]) / rho;
+    const double dp = (gamma - 1.0) * (a[4] - (u[0] * a[1] + u[1] * a[2] + u[2] * a[3]) + 0.5 * uu * a[0]);
+    out[0] = a[n];
+    for (int k = 0; k < 3; k++) out[k + 1] = a[n] * u[k] + Q[n] * du[k] + (k + 1 == n ? dp : 0.0);
+    out[4] = (a[4] + dp) * u[n - 1] + (E + p) * du[n - 1];
+}
+
+static void euler_d2flux_dir(double gamma, const double* Q, int d, const double* a, const double* b, double* out)
+{
+    const int n = 1 + d;
+    const double rho = Q[0], u[3] = {Q[1] / rho, Q[2] / rho, Q[3] / rho}, E = Q[4];
+    const double uu = u[0] * u[0] + u[1] * u[1] + u[2] * u[2];
+    const double p = (gamma - 1.0) * (E - 0.5 * rho * uu);
+    double dua[3], dub[3], d2u[3];
+    for (int k = 0; k < 3; k++) {
+        dua[k] = (a[k + 1] - u[k] * a[0]) / rho;
+        dub[k] = (b[k + 1] - u[k] * b[0]) / rho;
+        d2u[k] = -(dua[k] * b[0] + dub[k] * a[0]) / rho;
+    }
+    const double dpa = (gamma - 1.0) * (a[4] - (u[0] * a[1] + u[1] * a[2] + u[2] * a[3]) + 0.5 * uu * a[0]);
+    const double dpb = (gamma - 1.0) * (b[4] - (u[0] * b[1] + u[1] * b[2] + u[2] * b[3]) + 0.5 * uu * b[0]);
+    const double d2p = -(gamma - 1.0) * rho * (dua[0] * dub[0] + dua[1] * dub[1] + dua[2] * dub[2]);
+    out[0] = 0.0;
+    for (int k = 0; k < 3; k++)
+        out[k + 1] = a[n] * dub[k] + b[n] * dua[k] + Q[n] * d2u[k] + (k + 1 == n ? d2p : 0.0);
+    /* The reference's energy-flux Hessian (D2FluxFunc.cpp, entries
+     * D2flux(i,5,1,5,.), (i,5,2,5,.), (i,5,3,5,.) and their transposes) omits
+     * the pressure's dependence on E in the E cross terms: its d2f5/dE dq_k is
+     * d u_n/dq_k where the exact value is gamma d u_n/dq_k.  Reproduced here:
+     * the E component of dp is left out of the two cross terms. */
+    const double dpa_noE = dpa - (gamma - 1.0) * a[4];
+    const double dpb_noE = dpb - (gamma - 1.0) * b[4];
+    out[4] = (a[4] + dpa_noE) * dub[n - 1] + (b[4] + dpb_noE) * dua[n - 1] + d2p * u[n - 1] + (E + p) * d2u[n - 1];
+}
+
+void oracle_flux_derivs(double gamma, const double* Q, double* A, double* H);
+
+/* Jacobian A[d][m][k] = d f^d_m / d q_k and Hessian H[d][m][k1][k2]
+ * (DFluxFunc / D2FluxFunc's Dflux(1,m,k,d), D2flux(1,m,k1,k2,d)). */
+static void euler_jac_hess(double gamma, const double* Q, double A[2][5][5], double H[2][5][5][5], int want_h)
+{
+    double e[5][5] = {{0}};
+    for (int k = 0; k < 5; k++) e[k][k] = 1.0;
+    for (int d = 0; d < 2; d++) {
+        double col[5];
+        for (int k = 0; k < 5; k++) {
+            euler_dflux_dir(gamma, Q, d, e[k], col);
+            for (int m = 0; m < 5; m++) A[d][m][k] = col[m];
+        }
+        if (!want_h) continue;
+        for (int k1 = 0; k1 < 5; k1++)
+            for (int k2 = 0; k2 < 5; k2++) {
+                euler_d2flux_dir(gamma, Q, d, e[k1], e[k2], col);
+                for (int m = 0; m < 5; m++) H[d][m][k1][k2] = col[m];
+            }
+    }
+}
+
 /* ---------------------------------------------------------------------- */
 /* WENO reconstructions (lib/WenoReconstruct.cpp)                          */
 /* ---------------------------------------------------------------------- */
@@ -409,6 +484,9 @@ static int get_cfl(const fin_params* p, double dt, double dtmax, const double* s
     return FIN_OK;
 }
 
+static int construct_integrated_r2(const fin_params* p, double dt, double a1, double b1, const double* q1,
+                                   double a2, double b2, const double* q2, double* F, double* G);
+
 typedef struct {
     grid_t g, gS;
     size_t n, nS;
@@ -461,6 +539,49 @@ static int take_stages(const fin_params* p, work_t* w, double* q, double* tnew, 
         if ((rc = oracle_construct_l(p, w->qstar, w->L, w->smax))) return rc;
         update_soln(g, a1[2], a2[2], bt[2], dt, w->qstar, w->L, q);
         *tnew = a1[2] * *tstar + a2[2] * *tnew + bt[2] * dt;
+        return FIN_OK;
+    }
+    if (p->time_stepping_method == FIN_TS_MD) {
+        /* FinSolveMD.cpp:116-170 (time_order 4) */
+        if (p->time_order != 4) return FIN_ERR_UNSUPPORTED;
+        memcpy(w->qold, q, w->n * sizeof(double));   /* Qold: the step's starting state */
+        oracle_set_bnd(p, q);
+        if ((rc = oracle_construct_integrated_r(p, 0.5 * dt, q, w->F, w->G))) return rc;
+        if ((rc = oracle_construct_lxwl(p, q, w->F, w->G, w->L, w->smax))) return rc;
+        for (int i = 1; i <= g->mx; i++)
+            for (int j = 1; j <= g->my; j++)
+                for (int m = 1; m <= g->meqn; m++) {
+                    const size_t k = IDX(g, i, j, m);
+                    w->qstar[k] = q[k] + 0.5 * dt * w->L[k];
+                }
+        *tstar = *tnew + 0.5 * dt;
+        oracle_set_bnd(p, q);
+        oracle_set_bnd(p, w->qstar);
+        if ((rc = construct_integrated_r2(p, dt, 1.0, (1.0 / 6.0), q, 0.0, (1.0 / 3.0), w->qstar, w->F, w->G)))
+            return rc;
+        if ((rc = oracle_construct_lxwl(p, w->qstar, w->F, w->G, w->L, w->smax))) return rc;
+        /* q^{n+1} = q_old + dt L; q here still holds q_old (the stages never wrote it) */
+        for (int i = 1; i <= g->mx; i++)
+            for (int j = 1; j <= g->my; j++)
+                for (int m = 1; m <= g->meqn; m++) {
+                    const size_t k = IDX(g, i, j, m);
+                    q[k] = w->qold[k] + dt * w->L[k];
+                }
+        *tnew = *tnew + dt;   /* Qold.get_t() + dt, Qold.t == Qnew.t at step start */
+        return FIN_OK;
+    }
+    if (p->time_stepping_method == FIN_TS_LXW) {
+        /* FinSolveLxW.cpp:120-176 (no MPP limiter) */
+        oracle_set_bnd(p, q);
+        if ((rc = oracle_construct_integrated_r(p, dt, q, w->F, w->G))) return rc;
+        if ((rc = oracle_construct_lxwl(p, q, w->F, w->G, w->L, w->smax))) return rc;
+        for (int i = 1; i <= g->mx; i++)
+            for (int j = 1; j <= g->my; j++)
+                for (int m = 1; m <= g->meqn; m++) {
+                    const size_t k = IDX(g, i, j, m);
+                    q[k] = q[k] + dt * w->L[k];
+                }
+        *tnew = *tnew + dt;
         return FIN_OK;
     }
     return FIN_ERR_UNSUPPORTED;
@@ -523,10 +644,195 @@ done:
     return rc;
 }
 
+/* Flat copies of the Jacobian and Hessian at one state (for tests). */
+void oracle_flux_derivs(double gamma, const double* Q, double* Aout, double* Hout)
+{
+    double A[2][5][5], H[2][5][5][5];
+    euler_jac_hess(gamma, Q, A, H, 1);
+    memcpy(Aout, A, sizeof(A));
+    memcpy(Hout, H, sizeof(H));
+}
+
+/* Diff1 / Diff2 of lib/WenoReconstruct.cpp:702-716 and :791-806 (5 points). */
+static double diff1(double dx, const double* f)
+{
+    double tmp = (f[0] - f[4]) * (1.0 / 12.0);
+    tmp += (-f[1] + f[3]) * (2.0 / 3.0);
+    return tmp / dx;
+}
+static double diff2(double dx, const double* f)
+{
+    double tmp = (-f[0] - f[4]) * (1.0 / 12.0);
+    tmp += (f[1] + f[3]) * (4.0 / 3.0);
+    tmp += (-f[2]) * (5.0 / 2.0);
+    return tmp / (dx * dx);
+}
+
+/* R = FluxFunc sampled over the whole ghosted grid (SampleFunction,
+ * lib/2d/SampleFunction.cpp:62-125): Rf, Rg ghosted (mx,my,meqn). */
+static void sample_flux(const fin_params* p, const double* q, double* Rf, double* Rg)
+{
+    const grid_t g = grid_of(p, p->mx, p->my);
+    for (int i = 1 - g.mbc; i <= g.mx + g.mbc; i++)
+        for (int j = 1 - g.mbc; j <= g.my + g.mbc; j++)
+            euler_flux(p->gamma, q + IDX(&g, i, j, 1), Rf + IDX(&g, i, j, 1), Rg + IDX(&g, i, j, 1));
+}
+
+/* f_t, g_t (and with nterms > 2, f_tt, g_tt) at one cell:
+ * ConstructIntegratedR.cpp:106-284 (1-state, 2nd-order mixed derivatives,
+ * mixed4 = 0) and LocalIntegrate :298-523 (4th-order mixed stencil, mixed4 = 1). */
+static void local_time_derivs(const fin_params* p, const grid_t* g, int i, int j, const double* q,
+                              const double* Rf, const double* Rg, int nterms, int mixed4,
+                              double* f_t, double* g_t, double* f_tt, double* g_tt)
+{
+    const double dx = get_dx(p), dy = get_dy(p);
+    const int meqn = 5;
+    double fx[5], gy[5], qx[5], qy[5];
+    for (int m = 0; m < meqn; m++) {
+        double Fv[5], Gv[5], qxv[5], qyv[5];
+        for (int r = 0; r < 5; r++) {
+            const int s = r - 2;
+            Fv[r] = Rf[IDX(g, i + s, j, m + 1)];
+            Gv[r] = Rg[IDX(g, i, j + s, m + 1)];
+            qxv[r] = q[IDX(g, i + s, j, m + 1)];
+            qyv[r] = q[IDX(g, i, j + s, m + 1)];
+        }
+        fx[m] = diff1(dx, Fv);
+        qx[m] = diff1(dx, qxv);
+        gy[m] = diff1(dy, Gv);
+        qy[m] = diff1(dy, qyv);
+    }
+    double A[2][5][5], H[2][5][5][5];
+    euler_jac_hess(p->gamma, q + IDX(g, i, j, 1), A, H, nterms > 2);
+    for (int m1 = 0; m1 < meqn; m1++) {
+        double tmp1 = 0., tmp2 = 0.;
+        for (int m2 = 0; m2 < meqn; m2++) {
+            tmp1 += -(A[0][m1][m2]) * (fx[m2] + gy[m2]);
+            tmp2 += -(A[1][m1][m2]) * (fx[m2] + gy[m2]);
+        }
+        f_t[m1] = tmp1;
+        g_t[m1] = tmp2;
+    }
+    for (int m = 0; m < meqn; m++) f_tt[m] = g_tt[m] = 0.0;
+    if (nterms <= 2) return;
+    double w[5], fxx[5], gyy[5], fxy[5], gxy[5], fpg_t[5];
+    for (int m = 0; m < meqn; m++) {
+        w[m] = fx[m] + gy[m];
+        double Fv[5], Gv[5];
+        for (int r = 0; r < 5; r++) {
+            Fv[r] = Rf[IDX(g, i + r - 2, j, m + 1)];
+            Gv[r] = Rg[IDX(g, i, j + r - 2, m + 1)];
+        }
+        fxx[m] = diff2(dx, Fv);
+        gyy[m] = diff2(dy, Gv);
+    }
+    for (int m = 0; m < meqn; m++) {
+        for (int d = 0; d < 2; d++) {
+            const double* R = d == 0 ? Rf : Rg;
+#define RR(a, b) R[IDX(g, i + (a), j + (b), m + 1)]
+            double tmp;
+            if (!mixed4) {
+                tmp = 0.5 * (RR(1, 1) - RR(-1, 1)) / dx;
+                tmp -= 0.5 * (RR(1, -1) - RR(-1, -1)) / dx;
+                tmp *= 0.5 / dy;
+            } else {
+                tmp = 0.25 * (RR(1, 1) - RR(-1, 1) - RR(1, -1) + RR(-1, -1));
+                tmp -= (1. / 24.) * (RR(2, 1) + RR(-2, -1) - RR(2, -1) - RR(-2, 1) -
+                                     RR(1, 2) - RR(-1, -2) + RR(1, -2) + RR(-1, 2));
+                tmp *= (1. / (dx * dy));
+            }
+#undef RR
+            if (d == 0) fxy[m] = tmp; else gxy[m] = tmp;
+        }
+    }
+    for (int m = 0; m < meqn; m++) {
+        double tmp = 0.;
+        for (int m1 = 0; m1 < meqn; m1++)
+            for (int m2 = 0; m2 < meqn; m2++) {
+                tmp += H[0][m][m1][m2] * qx[m1] * w[m2];
+                tmp += H[1][m][m1][m2] * qy[m1] * w[m2];
+            }
+        for (int m1 = 0; m1 < meqn; m1++) {
+            tmp += A[0][m][m1] * (fxx[m1] + gxy[m1]);
+            tmp += A[1][m][m1] * (fxy[m1] + gyy[m1]);
+        }
+        fpg_t[m] = tmp;
+    }
+    for (int m1 = 0; m1 < meqn; m1++) {
+        double tmp1 = 0., tmp2 = 0.;
+        for (int m2 = 0; m2 < meqn; m2++) {
+            tmp1 += A[0][m1][m2] * fpg_t[m2];
+            tmp2 += A[1][m1][m2] * fpg_t[m2];
+        }
+        f_tt[m1] = tmp1;
+        g_tt[m1] = tmp2;
+    }
+    for (int m = 0; m < meqn; m++) {
+        double tmp1 = 0., tmp2 = 0.;
+        for (int m1 = 0; m1 < meqn; m1++)
+            for (int m2 = 0; m2 < meqn; m2++) {
+                tmp1 += H[0][m][m1][m2] * w[m1] * w[m2];
+                tmp2 += H[1][m][m1][m2] * w[m1] * w[m2];
+            }
+        f_tt[m] = f_tt[m] + tmp1;
+        g_tt[m] = g_tt[m] + tmp2;
+    }
+}
+
+/* ConstructIntegratedR, 1-state (lib/2d/ConstructIntegratedR.cpp:59-296):
+ * F = R + dt/2 (f_t + dt/3 f_tt) on [1-3, mx+3] x [1-3, my+3]; the Hessian
+ * terms are present when time_order > 2 (:171). */
 int oracle_construct_integrated_r(const fin_params* p, double dt, const double* q, double* F, double* G)
 {
-    (void)p; (void)dt; (void)q; (void)F; (void)G;
-    return FIN_ERR_UNSUPPORTED;
+    if (p->meqn != 5 || p->mbc < 5) return FIN_ERR_ARG;
+    const grid_t g = grid_of(p, p->mx, p->my);
+    const size_t n = numel(&g);
+    double* Rf = (double*)malloc(n * sizeof(double));
+    double* Rg = (double*)malloc(n * sizeof(double));
+    sample_flux(p, q, Rf, Rg);
+    const int nterms = p->time_order > 2 ? 3 : 2;
+    for (int i = 1 - 3; i <= g.mx + 3; i++)
+        for (int j = 1 - 3; j <= g.my + 3; j++) {
+            double f_t[5], g_t[5], f_tt[5], g_tt[5];
+            local_time_derivs(p, &g, i, j, q, Rf, Rg, nterms, 0, f_t, g_t, f_tt, g_tt);
+            for (int m = 1; m <= 5; m++) {
+                const size_t k = IDX(&g, i, j, m);
+                F[k] = Rf[k] + 0.5 * dt * (f_t[m - 1] + dt / 3.0 * f_tt[m - 1]);
+                G[k] = Rg[k] + 0.5 * dt * (g_t[m - 1] + dt / 3.0 * g_tt[m - 1]);
+            }
+        }
+    free(Rf);
+    free(Rg);
+    return FIN_OK;
+}
+
+/* ConstructIntegratedR, 2-state (lib/2d/ConstructIntegratedR.cpp:525-606):
+ * F = a1 R1 + dt (b1 f1_t) + a2 R2 + dt (b2 f2_t), LocalIntegrate with nterms 2. */
+static int construct_integrated_r2(const fin_params* p, double dt, double a1, double b1, const double* q1,
+                                   double a2, double b2, const double* q2, double* F, double* G)
+{
+    if (p->meqn != 5 || (p->mbc + 1) / 2 != 3) return FIN_ERR_ARG;
+    const grid_t g = grid_of(p, p->mx, p->my);
+    const size_t n = numel(&g);
+    double* R1f = (double*)malloc(n * sizeof(double));
+    double* R1g = (double*)malloc(n * sizeof(double));
+    double* R2f = (double*)malloc(n * sizeof(double));
+    double* R2g = (double*)malloc(n * sizeof(double));
+    sample_flux(p, q1, R1f, R1g);
+    sample_flux(p, q2, R2f, R2g);
+    for (int i = 1 - 3; i <= g.mx + 3; i++)
+        for (int j = 1 - 3; j <= g.my + 3; j++) {
+            double f1t[5], g1t[5], f2t[5], g2t[5], z1[5], z2[5];
+            local_time_derivs(p, &g, i, j, q1, R1f, R1g, 2, 1, f1t, g1t, z1, z2);
+            local_time_derivs(p, &g, i, j, q2, R2f, R2g, 2, 1, f2t, g2t, z1, z2);
+            for (int m = 1; m <= 5; m++) {
+                const size_t k = IDX(&g, i, j, m);
+                F[k] = a1 * R1f[k] + dt * (b1 * f1t[m - 1]) + a2 * R2f[k] + dt * (b2 * f2t[m - 1]);
+                G[k] = a1 * R1g[k] + dt * (b1 * g1t[m - 1]) + a2 * R2g[k] + dt * (b2 * g2t[m - 1]);
+            }
+        }
+    free(R1f); free(R1g); free(R2f); free(R2g);
+    return FIN_OK;
 }
 
 /* lib/2d/ConSoln.cpp:52-64 */

@@ -38,6 +38,9 @@ void ConstructIntegratedR(double dt, double alpha1, double beta1, const StateVar
 void ConstructLxWL(const StateVars& Q, const dTensorBC3& F, const dTensorBC3& G,
     dTensorBC3& Lstar, dTensorBC3& smax);
 
+void DFluxFunc(const dTensor2&, const dTensor2&, const dTensor2&, dTensor4&);
+void D2FluxFunc(const dTensor2&, const dTensor2&, const dTensor2&, dTensor5&);
+
 static int g_bc[4] = {FIN_BC_PERIODIC, FIN_BC_PERIODIC, FIN_BC_PERIODIC, FIN_BC_PERIODIC};
 
 static int remap(int k, int n, int bc_lo, int bc_hi)
@@ -186,6 +189,27 @@ int ref_finsolve(int method, double* q, double* t, double tend, double* dtv)
     *t = Q->get_t();
     delete Q;
     return rc;
+}
+
+// Jacobian and Hessian of the application's flux at one state (DFluxFunc,
+// D2FluxFunc): A[(d*5+m)*5+k], H[((d*5+m)*5+k1)*5+k2], d = 0 (f) or 1 (g).
+int ref_flux_derivs(const double* Q, double* A, double* H)
+{
+    dTensor2 xp(1, 2), q(1, 5), aux(1, 1);
+    xp.setall(0.); aux.setall(0.);
+    for (int m = 1; m <= 5; m++) q.set(1, m, Q[m - 1]);
+    dTensor4 D(1, 5, 5, 2);
+    dTensor5 D2(1, 5, 5, 5, 2);
+    DFluxFunc(xp, q, aux, D);
+    D2FluxFunc(xp, q, aux, D2);
+    for (int d = 0; d < 2; d++)
+        for (int m = 0; m < 5; m++)
+            for (int k = 0; k < 5; k++) {
+                A[(d * 5 + m) * 5 + k] = D.get(1, m + 1, k + 1, d + 1);
+                for (int k2 = 0; k2 < 5; k2++)
+                    H[((d * 5 + m) * 5 + k) * 5 + k2] = D2.get(1, m + 1, k + 1, k2 + 1, d + 1);
+            }
+    return 0;
 }
 
 }  // extern "C"

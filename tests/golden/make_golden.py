@@ -20,8 +20,8 @@ sys.path.insert(0, os.path.join(ROOT, "oracle"))
 
 from oracle import RefLib  # noqa: E402
 from finess_b200 import problems as P  # noqa: E402
-from finess_b200._abi import (FIN_BC_TRANSMISSIVE, FIN_TS_RK, FIN_WENO_FD, FIN_WENO_JS,  # noqa: E402
-                              FIN_WENO_Z)
+from finess_b200._abi import (FIN_BC_TRANSMISSIVE, FIN_TS_LXW, FIN_TS_MD, FIN_TS_RK, FIN_WENO_FD,  # noqa: E402
+                              FIN_WENO_JS, FIN_WENO_Z)
 
 
 def params_json(p):
@@ -48,6 +48,23 @@ def construct_l_cases():
 
 def main():
     ref = RefLib()
+    # ConstructIntegratedR, 1-state, with (time_order 4) and without
+    # (time_order 2) the Hessian terms.
+    rng = np.random.default_rng(99)
+    for to, kind in ((4, "riemann"), (2, "riemann"), (4, "smooth")):
+        p = P.riemann_params(n=16, weno=FIN_WENO_Z, method=FIN_TS_MD, time_order=to)
+        p.my = 13
+        if kind == "smooth":
+            from finess_b200._abi import FIN_BC_PERIODIC
+            p.bc_xlow = p.bc_xhigh = p.bc_ylow = p.bc_yhigh = FIN_BC_PERIODIC
+            q = P.random_smooth_state(p, rng)
+        else:
+            q = P.random_riemann_state(p, rng)
+        q = ref.set_bnd(p, q)
+        F, G = ref.construct_integrated_r(p, 0.004, q)
+        name = f"intr_t{to}_{kind}"
+        np.savez_compressed(os.path.join(HERE, name + ".npz"), params=params_json(p), q=q, F=F, G=G, dt=0.004)
+        print("wrote", name)
     for name, p, q in construct_l_cases():
         q = ref.set_bnd(p, q)
         L, smax = ref.construct_l(p, q)
@@ -65,6 +82,16 @@ def main():
     # a large initial dt forces step rejections (FinSolveRK.cpp:343-357)
     p = P.riemann_params(n=20, weno=FIN_WENO_JS)
     runs.append(("finsolverk_js_riemann20_reject", p, P.riemann_init(p), 0.0, 0.03, 0.05))
+    # Two-stage multiderivative (FinSolveMD, time_order 4) and single-stage
+    # Lax-Wendroff (FinSolveLxW) frames; both need mbc = 5.
+    p = P.riemann_params(n=24, weno=FIN_WENO_Z, method=FIN_TS_MD)
+    p.my = 20
+    runs.append(("finsolvemd_z_riemann24", p, P.riemann_init(p), 0.0, 0.02, 1e-3))
+    p = P.vortex_params(n=20, weno=FIN_WENO_JS, mbc=5, time_stepping_method=FIN_TS_MD, time_order=4)
+    runs.append(("finsolvemd_js_vortex20", p, P.vortex_exact(p), 0.0, 0.3, 0.05))
+    p = P.riemann_params(n=22, weno=FIN_WENO_JS, method=FIN_TS_MD, time_stepping_method=FIN_TS_LXW,
+                         time_order=3)
+    runs.append(("finsolvelxw_js_riemann22", p, P.riemann_init(p), 0.0, 0.02, 1e-3))
     for name, p, q0, t0, tend, dt in runs:
         q0 = ref.set_bnd(p, q0)
         rc, q1, t1, dt1 = ref.finsolve(p, q0, t0, tend, dt)

@@ -66,3 +66,51 @@ def test_conservation_periodic(oracle):
     t1v = oracle.conservation_totals(p, q1)
     assert rc == 0 and n > 0
     assert np.all(np.abs(t1v - t0) <= 1e-12 * np.maximum(1.0, np.abs(t0)))
+
+
+# The multiderivative path's Jacobian/Hessian are closed forms here and
+# tabulated entries in the reference, so these agree to rounding, not bits.
+TOL_MD = 1e-13
+
+
+@pytest.mark.parametrize("path", golden_cases("intr_"))
+def test_integrated_flux_matches_golden(oracle, path):
+    g = load_golden(path)
+    p = g["p"]
+    F, G = oracle.construct_integrated_r(p, float(g["dt"]), g["q"])
+    mb = p.mbc
+    E = (slice(mb - 3, mb + p.mx + 3), slice(mb - 3, mb + p.my + 3))   # [1-3, mx+3] x [1-3, my+3]
+    for a, b in ((F, g["F"]), (G, g["G"])):
+        assert np.max(np.abs(a[E] - b[E])) <= TOL_MD * np.max(np.abs(b[E]))
+
+
+@pytest.mark.parametrize("path", golden_cases("finsolvemd_") + golden_cases("finsolvelxw_"))
+def test_finsolve_md_lxw_matches_golden(oracle, path):
+    g = load_golden(path)
+    p = g["p"]
+    rc, q1, t1, dt1, n = oracle.finsolve(p, g["q0"], float(g["t0"]), float(g["tend"]), float(g["dt0"]))
+    assert rc == 0
+    a, b = interior(p, q1), interior(p, g["q1"])
+    assert np.max(np.abs(a - b)) <= TOL_MD * np.max(np.abs(b))
+    assert abs(t1 - float(g["t1"])) <= 1e-15 and abs(dt1 - float(g["dt1"])) <= 1e-12 * float(g["dt1"])
+
+
+def test_reference_hessian_convention(reflib):
+    """The reference's energy-flux Hessian omits the pressure's E dependence in
+    its E cross terms (D2FluxFunc.cpp: D2flux(i,5,2,5,1) = 1/q1 where the exact
+    value is gamma/q1); the oracle reproduces the reference, not the exact one."""
+    import ctypes as C
+    from oracle import ORACLE_SO, REF_SO
+    dp = np.ctypeslib.ndpointer(np.float64, flags="C")
+    ref = C.CDLL(REF_SO)
+    orc = C.CDLL(ORACLE_SO)
+    ref.ref_flux_derivs.argtypes = [dp, dp, dp]
+    orc.oracle_flux_derivs.argtypes = [C.c_double, dp, dp, dp]
+    from finess_b200._abi import default_params
+    reflib.setup(default_params(gamma=1.4))
+    Q = np.array([1.3, 0.4, -0.7, 0.0, 2.9])
+    A1, H1, A2, H2 = np.zeros(50), np.zeros(250), np.zeros(50), np.zeros(250)
+    ref.ref_flux_derivs(Q, A1, H1)
+    orc.oracle_flux_derivs(1.4, Q, A2, H2)
+    assert np.max(np.abs(A1 - A2)) < 1e-14 and np.max(np.abs(H1 - H2)) < 1e-13
+    assert abs(H1.reshape(2, 5, 5, 5)[0, 4, 1, 4] - 1.0 / Q[0]) < 1e-15
