@@ -209,6 +209,7 @@ def main():
     ap.add_argument("--form", default="fp64", choices=["fp64", "fp32"])
     ap.add_argument("--n", type=int, default=N_CELLS)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-md", action="store_true")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     if args.impl == "reference":
@@ -308,6 +309,25 @@ def main():
            "h2d_bytes_per_step": state_bytes / args.steps, "d2h_bytes_per_step": state_bytes / args.steps,
            "api": "fin_set_state + fin_advance(K steps) + fin_get_state on host arrays (one FinSolveRK frame)"}
 
+    # ---- the same problem with the two-stage multiderivative (Lax-Wendroff /
+    # PIF) stepper, FP64 (device-resident, same K) ----
+    md = None
+    if args.form == "fp64" and not args.no_md:
+        from finess_b200._abi import FIN_TS_MD
+        pm = p.copy()
+        pm.time_stepping_method, pm.time_order, pm.mbc = FIN_TS_MD, 4, 5
+        from finess_b200 import problems as P
+        qm = P.riemann_init(pm)
+        sm = Solver(pm)
+        sm.set_state(qm, 0.0)
+        dtvm, _ = sm.advance(tend, np.array([0.0, dt0, pm.max_dt]), args.warmup)
+        barrier()
+        dtvm, nm = sm.advance(tend, dtvm, args.steps)
+        md_ms = sm.last_kernel_ms()
+        sm.close()
+        md = {"value": cells * nm / (md_ms * 1e-3), "unit": UNIT, "ms_per_step": md_ms / nm,
+              "stepper": "FinSolveMD time_order 4 (two-stage Lax-Wendroff/PIF)"}
+
     cpu = None
     if rank == 0 and ws == 1 and not args.no_cpu_baseline:
         try:
@@ -325,7 +345,7 @@ def main():
             "config": {"workload": "euler2d_riemann4q_wenoz_rk3", "grid": f"{p.mx}x{p.my}", "form": args.form,
                        "weno": "Z", "time": "SSP-RK3", "cfl": 0.4, "parallelism": f"replicas{ws}",
                        "l2": "inputs larger than L2 (673 MB per state array)"},
-            "roofline": roofline, "pipe": pipe, "cpu_baseline": cpu, "e2e": e2e,
+            "roofline": roofline, "pipe": pipe, "cpu_baseline": cpu, "e2e": e2e, "md_stepper": md,
             "clocks": clocks, "gpu_launches": launches,
         }
         print(json.dumps(line), flush=True)

@@ -50,6 +50,12 @@ struct StageArgs {
     double* face_alpha_y;     // optional per-face alpha, mx*(my+1)
     unsigned int* status;     // bit 0: non-finite speed, bit 1: negative p or rho
     int bc[4];                // xlow, xhigh, ylow, yhigh
+    // Lax-Wendroff / multiderivative stages (ConstructLxWL): the split fluxes
+    // are the time-integrated F, G (ghosted (mx+6) x (my+6) planes) instead of
+    // FluxFunc of q_in (lib/2d/ConstructLxWL.cpp:150-155).
+    const double* Fg;
+    const double* Gg;
+    size_t gplane;
 };
 
 template <int TI_, int TJ_, int NT_>
@@ -143,7 +149,7 @@ __device__ __forceinline__ void right_add(const typename Euler::Eig<R>& e, int k
     }
 }
 
-template <class R, int VER, bool P2, class Cfg>
+template <class R, int VER, bool P2, class Cfg, bool FG = false>
 __global__ void __launch_bounds__(Cfg::NT, MinBlocks<R>::value) k_stage(const StageArgs a)
 {
     constexpr int TI = Cfg::TI, TJ = Cfg::TJ, NT = Cfg::NT, H = Cfg::H;
@@ -191,6 +197,26 @@ __global__ void __launch_bounds__(Cfg::NT, MinBlocks<R>::value) k_stage(const St
         prim[PQ + e] = u2;
         prim[2 * PQ + e] = press;
         prim[3 * PQ + e] = fsqrt(fabs(gamma * press * ir));
+        if (FG) {
+            // 0.5 * F, 0.5 * G of the integrated-flux kernel, unremapped: it
+            // covers the 3-cell ghost frame; cells of a partial tile beyond it
+            // only feed discarded faces, so their index is clamped.
+            int ci = i0 + ii - H, cj = j0 + jj - H;
+            ci = ci < -3 ? -3 : (ci > mx + 2 ? mx + 2 : ci);
+            cj = cj < -3 ? -3 : (cj > my + 2 ? my + 2 : cj);
+            const size_t o = size_t(ci + 3) * (my + 6) + (cj + 3);
+            if (yin) {
+                const int d = ii * TJ + (jj - H);
+#pragma unroll
+                for (int m = 0; m < MEQN; m++) fs[m * RI * TJ + d] = R(0.5 * __ldg(a.Fg + m * a.gplane + o));
+            }
+            if (xin) {
+                const int d = (ii - H) * RJ + jj;
+#pragma unroll
+                for (int m = 0; m < MEQN; m++) gs[m * TI * RJ + d] = R(0.5 * __ldg(a.Gg + m * a.gplane + o));
+            }
+            continue;
+        }
         const R hr = R(0.5) * rho, hep = R(0.5) * (en + press);
         if (yin) {
             const int o = ii * TJ + (jj - H);

@@ -16,6 +16,7 @@
 #include <algorithm>
 #include "finess_b200.h"
 #include "fin_stage.cuh"
+#include "fin_intflux.cuh"
 
 using namespace fin;
 
@@ -64,6 +65,9 @@ struct fin_solver {
     double* d_aos;          // staging buffer for the reference ghosted layout
     size_t aos_elems;
     double* d_aux;          // second staging / L output buffer (planes)
+    double* Fg;             // integrated fluxes F, G (Lax-Wendroff / multiderivative)
+    double* Gg;
+    size_t gplane;          // their ghosted plane stride
     double* d_face_x;       // per-face alpha buffers (only for fin_construct_l)
     double* d_face_y;
     cudaStream_t stream;
@@ -187,11 +191,11 @@ __global__ void k_fma_peak(R* out, int iters, R a, R b)
 // ---------------------------------------------------------------------------
 namespace {
 
-template <class R, int VER, bool P2>
+template <class R, int VER, bool P2, bool FG = false>
 int launch_stage_t(fin_solver* s, const StageArgs& a)
 {
     const size_t smem = Cfg::smem_bytes<R>();
-    auto kern = k_stage<R, VER, P2, Cfg>;
+    auto kern = k_stage<R, VER, P2, Cfg, FG>;
     static bool configured = false;   // per instantiation; attribute is per device function
     if (!configured) {
         CK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
@@ -216,8 +220,25 @@ int launch_stage_r(fin_solver* s, const StageArgs& a)
     return set_err(FIN_ERR_ARG, "weno_version");
 }
 
+// Stages that split the time-integrated fluxes (ConstructLxWL): FP64 only.
+int launch_stage_fg(fin_solver* s, const StageArgs& a)
+{
+    const bool p2 = s->p.power_param == 2.0;
+    switch (s->p.weno_version) {
+    case FIN_WENO_JS:
+        return p2 ? launch_stage_t<double, FIN_WENO_JS, true, true>(s, a)
+                  : launch_stage_t<double, FIN_WENO_JS, false, true>(s, a);
+    case FIN_WENO_Z:
+        return p2 ? launch_stage_t<double, FIN_WENO_Z, true, true>(s, a)
+                  : launch_stage_t<double, FIN_WENO_Z, false, true>(s, a);
+    case FIN_WENO_FD: return launch_stage_t<double, FIN_WENO_FD, true, true>(s, a);
+    }
+    return set_err(FIN_ERR_ARG, "weno_version");
+}
+
 int launch_stage(fin_solver* s, const StageArgs& a)
 {
+    if (a.Fg) return launch_stage_fg(s, a);
     if (s->p.precision == FIN_PREC_FP64) return launch_stage_r<double>(s, a);
     if (s->p.precision == FIN_PREC_FP32) return launch_stage_r<float>(s, a);
     return set_err(FIN_ERR_UNSUPPORTED, "precision form not built");
@@ -237,7 +258,8 @@ int launch_stage_timed(fin_solver* s, const StageArgs& a, int k)
 int collect_kernel_times(fin_solver* s)
 {
     if (!s->time_kernels) return FIN_OK;
-    for (int k = 0; k < 3; k++) {
+    const int nst = s->p.time_stepping_method == FIN_TS_RK ? 3 : (s->p.time_stepping_method == FIN_TS_MD ? 2 : 1);
+    for (int k = 0; k < nst; k++) {
         float ms = 0.f;
         CK(cudaEventElapsedTime(&ms, s->kev[2 * k], s->kev[2 * k + 1]));
         s->kernel_ms += ms;
@@ -304,13 +326,88 @@ int check_status(fin_solver* s)
     return FIN_OK;
 }
 
+// ConstructIntegratedR into s->Fg, s->Gg: mode 0/1 = 1-state without/with
+// the f_tt terms, 2 = 2-state.
+constexpr int IF_TI = 16, IF_TJ = 16;
+int launch_intflux(fin_solver* s, int mode, const double* q1, const double* q2, double dt, double a1,
+                   double b1, double a2, double b2)
+{
+    IntFluxArgs f;
+    memset(&f, 0, sizeof(f));
+    f.q1 = q1; f.q2 = q2; f.F = s->Fg; f.G = s->Gg;
+    f.plane = s->plane; f.gplane = s->gplane;
+    f.mx = s->p.mx; f.my = s->p.my;
+    f.dx = s->dx; f.dy = s->dy; f.gamma = s->p.gamma; f.dt = dt;
+    f.a1 = a1; f.b1 = b1; f.a2 = a2; f.b2 = b2;
+    f.bc[0] = s->p.bc_xlow; f.bc[1] = s->p.bc_xhigh; f.bc[2] = s->p.bc_ylow; f.bc[3] = s->p.bc_yhigh;
+    constexpr size_t smem = 3 * MEQN * (IF_TI + 4) * (IF_TJ + 4) * sizeof(double);
+    dim3 grid((s->p.my + 6 + IF_TJ - 1) / IF_TJ, (s->p.mx + 6 + IF_TI - 1) / IF_TI);
+    if (mode == 0) k_intflux<0, IF_TI, IF_TJ><<<grid, IF_TI * IF_TJ, smem, s->stream>>>(f);
+    else if (mode == 1) k_intflux<1, IF_TI, IF_TJ><<<grid, IF_TI * IF_TJ, smem, s->stream>>>(f);
+    else k_intflux<2, IF_TI, IF_TJ><<<grid, IF_TI * IF_TJ, smem, s->stream>>>(f);
+    s->launches++;
+    CK(cudaGetLastError());
+    return FIN_OK;
+}
+
+int take_stages_rk(fin_solver* s, double dt, int nxt);
+
+// Lax-Wendroff (FinSolveLxW.cpp:120-176) and two-stage multiderivative
+// (FinSolveMD.cpp:116-170, time_order 4) steps from q[cur] into q[nxt].
+int take_stages_lw(fin_solver* s, double dt, int nxt)
+{
+    const fin_params& p = s->p;
+    const int qn = s->cur;
+    int q1 = 0;
+    while (q1 == qn || q1 == nxt) q1++;
+    CK(cudaMemsetAsync(s->slots + SLOT_SMAX, 0, 2 * sizeof(double), s->stream));
+    CK(cudaMemsetAsync(s->slots + SLOT_STATUS, 0, sizeof(double), s->stream));
+    CK(cudaMemsetAsync(alpha_slot(s, q1), 0, 2 * sizeof(double), s->stream));
+    CK(cudaMemsetAsync(alpha_slot(s, nxt), 0, 2 * sizeof(double), s->stream));
+    const bool ga = p.global_alpha != 0;
+    int rc;
+    StageArgs a = base_args(s);
+    a.smax_out = s->slots + SLOT_SMAX;
+    a.Fg = s->Fg; a.Gg = s->Gg; a.gplane = s->gplane;
+    if (p.time_stepping_method == FIN_TS_LXW) {
+        // F = ConstructIntegratedR(dt, q); q^{n+1} = q + dt L
+        if ((rc = launch_intflux(s, p.time_order > 2 ? 1 : 0, s->q[qn], nullptr, dt, 0, 0, 0, 0))) return rc;
+        a.qin = s->q[qn]; a.A = s->q[qn]; a.B = nullptr; a.qout = s->q[nxt];
+        a.a1 = 1.0; a.a2 = 0.0; a.bdt = dt;
+        a.alpha_in = ga ? alpha_slot(s, qn) : nullptr;
+        a.alpha_out = alpha_slot(s, nxt);
+        return launch_stage_timed(s, a, 0);
+    }
+    // stage 1: F = ConstructIntegratedR(dt/2, q^n) (f_tt included: time_order 4 > 2);
+    //          q* = q^n + (dt/2) L
+    if ((rc = launch_intflux(s, 1, s->q[qn], nullptr, 0.5 * dt, 0, 0, 0, 0))) return rc;
+    a.qin = s->q[qn]; a.A = s->q[qn]; a.B = nullptr; a.qout = s->q[q1];
+    a.a1 = 1.0; a.a2 = 0.0; a.bdt = 0.5 * dt;
+    a.alpha_in = ga ? alpha_slot(s, qn) : nullptr;
+    a.alpha_out = alpha_slot(s, q1);
+    if ((rc = launch_stage_timed(s, a, 0))) return rc;
+    // stage 2: F = ConstructIntegratedR(dt, 1, 1/6, q^n, 0, 1/3, q*); q^{n+1} = q^n + dt L(q*)
+    if ((rc = launch_intflux(s, 2, s->q[qn], s->q[q1], dt, 1.0, (1.0 / 6.0), 0.0, (1.0 / 3.0)))) return rc;
+    a.qin = s->q[q1]; a.A = s->q[qn]; a.B = nullptr; a.qout = s->q[nxt];
+    a.a1 = 1.0; a.a2 = 0.0; a.bdt = dt;
+    a.alpha_in = ga ? alpha_slot(s, q1) : nullptr;
+    a.alpha_out = alpha_slot(s, nxt);
+    return launch_stage_timed(s, a, 1);
+}
+
+int take_stages(fin_solver* s, double dt, int nxt)
+{
+    if (s->p.time_stepping_method == FIN_TS_RK) return take_stages_rk(s, dt, nxt);
+    return take_stages_lw(s, dt, nxt);
+}
+
 // The stages of one step of size dt from q[cur] into q[nxt] (RK3:
 // FinSolveRK.cpp:158-211 with SetRKinfo.cpp:50-64).  Leaves the face-speed
 // maxima of the step in slots SMAX and alpha(q[nxt]) in its slot.
-int take_stages(fin_solver* s, double dt, int nxt)
+int take_stages_rk(fin_solver* s, double dt, int nxt)
 {
     const fin_params& p = s->p;
-    if (p.time_stepping_method != FIN_TS_RK || p.time_order != 3)
+    if (p.time_order != 3)
         return set_err(FIN_ERR_UNSUPPORTED, "only SSP-RK3 (time_order 3) is built");
     const int qn = s->cur;
     int reg[2], k = 0;
@@ -380,6 +477,19 @@ int validate(const fin_params* p)
         return set_err(FIN_ERR_ARG, "Requested WENO Reconstruction not implemented.");
     if (p->mx < 1 || p->my < 1) return set_err(FIN_ERR_ARG, "mx, my must be positive");
     if (p->mbc < 3) return set_err(FIN_ERR_ARG, "mbc must be >= 3 for WENO5");
+    if (p->time_stepping_method == FIN_TS_RK && p->time_order != 3)
+        return set_err(FIN_ERR_UNSUPPORTED, "Runge-Kutta: only SSP-RK3 (time_order 3) is built");
+    if (p->time_stepping_method == FIN_TS_MD && p->time_order != 4)
+        return set_err(FIN_ERR_UNSUPPORTED, "Multiderivative: only time_order 4 (two-stage) is built");
+    if (p->time_stepping_method != FIN_TS_RK && p->time_stepping_method != FIN_TS_MD &&
+        p->time_stepping_method != FIN_TS_LXW)
+        return set_err(FIN_ERR_ARG, "time_stepping_method");
+    if (p->time_stepping_method != FIN_TS_RK) {
+        // the integrated fluxes reach 5 cells out (ConstructIntegratedR.cpp:565 asserts it)
+        if (p->mbc < 5) return set_err(FIN_ERR_ARG, "Lax-Wendroff / multiderivative stepping needs mbc >= 5");
+        if (p->precision != FIN_PREC_FP64)
+            return set_err(FIN_ERR_UNSUPPORTED, "Lax-Wendroff / multiderivative stepping is built in FP64 only");
+    }
     if (p->source_term) return set_err(FIN_ERR_UNSUPPORTED, "source terms are not built");
     if (!(p->xhigh > p->xlow) || !(p->yhigh > p->ylow)) return set_err(FIN_ERR_ARG, "empty domain");
     for (int b : {p->bc_xlow, p->bc_xhigh, p->bc_ylow, p->bc_yhigh})
@@ -461,6 +571,11 @@ int fin_create(const fin_params* p, fin_solver** out)
     cudaError_t e;
     for (int b = 0; b < 4; b++)
         if ((e = cudaMalloc(&s->q[b], MEQN * s->plane * sizeof(double))) != cudaSuccess) return fail(e, "cudaMalloc state");
+    if (p->time_stepping_method != FIN_TS_RK) {
+        s->gplane = (size_t(p->mx + 6) * (p->my + 6) + 31) / 32 * 32;
+        if ((e = cudaMalloc(&s->Fg, MEQN * s->gplane * sizeof(double))) != cudaSuccess) return fail(e, "cudaMalloc F");
+        if ((e = cudaMalloc(&s->Gg, MEQN * s->gplane * sizeof(double))) != cudaSuccess) return fail(e, "cudaMalloc G");
+    }
     if ((e = cudaMalloc(&s->slots, NSLOTS * sizeof(double))) != cudaSuccess) return fail(e, "cudaMalloc slots");
     s->status = reinterpret_cast<unsigned int*>(s->slots + SLOT_STATUS);
     if ((e = cudaMallocHost(&s->h_slots, NSLOTS * sizeof(double))) != cudaSuccess) return fail(e, "cudaMallocHost");
@@ -486,6 +601,8 @@ int fin_destroy(fin_solver* s)
     cudaFree(s->slots);
     cudaFree(s->d_aos);
     cudaFree(s->d_aux);
+    cudaFree(s->Fg);
+    cudaFree(s->Gg);
     cudaFree(s->d_face_x);
     cudaFree(s->d_face_y);
     if (s->h_slots) cudaFreeHost(s->h_slots);
@@ -622,6 +739,32 @@ int fin_construct_l(fin_solver* s, const double* q_host, double* L_host, double*
     return check_status(s);
 }
 
+// ConstructIntegratedR, 1-state (lib/2d/ConstructIntegratedR.cpp:59-296).
+int fin_construct_integrated_r(fin_solver* s, double dt, const double* q_host, double* F_host, double* G_host)
+{
+    if (!s || !q_host || !F_host || !G_host) return set_err(FIN_ERR_ARG, "null argument");
+    if (!s->Fg) return set_err(FIN_ERR_ARG, "the solver was created for Runge-Kutta stepping (no F, G buffers)");
+    const fin_params& p = s->p;
+    const int buf = (s->cur + 3) % 4;
+    int rc = upload(s, q_host, buf);
+    if (rc) return rc;
+    if ((rc = launch_intflux(s, p.time_order > 2 ? 1 : 0, s->q[buf], nullptr, dt, 0, 0, 0, 0))) return rc;
+    std::vector<double> hf(MEQN * s->gplane), hg(MEQN * s->gplane);
+    CK(cudaMemcpyAsync(hf.data(), s->Fg, hf.size() * sizeof(double), cudaMemcpyDeviceToHost, s->stream));
+    CK(cudaMemcpyAsync(hg.data(), s->Gg, hg.size() * sizeof(double), cudaMemcpyDeviceToHost, s->stream));
+    CK(cudaStreamSynchronize(s->stream));
+    const int sy = p.my + 2 * p.mbc;
+    for (int i = -3; i < p.mx + 3; i++)
+        for (int j = -3; j < p.my + 3; j++)
+            for (int m = 0; m < MEQN; m++) {
+                const size_t dst = (size_t(i + p.mbc) * sy + (j + p.mbc)) * MEQN + m;
+                const size_t src = m * s->gplane + size_t(i + 3) * (p.my + 6) + (j + 3);
+                F_host[dst] = hf[src];
+                G_host[dst] = hg[src];
+            }
+    return FIN_OK;
+}
+
 int fin_step_fixed(fin_solver* s, double dt, double* cfl_out)
 {
     if (!s) return set_err(FIN_ERR_ARG, "null solver");
@@ -680,14 +823,24 @@ int fin_advance(fin_solver* s, double tend, double* dtv, int max_steps, int* nst
             bool nonfinite = false;
             if ((rc = get_cfl(s, dt, dtv[2], &cfl, &nonfinite))) goto done;
             if ((rc = collect_kernel_times(s))) goto done;
-            // Qstar/Qnew time bookkeeping of UpdateSoln.cpp:27 for the 3 stages
-            t_star = 1.0 * s->t + 0.0 * t_star + 1.0 * dt;
-            t_star = 0.75 * s->t + 0.25 * t_star + 0.25 * dt;
-            const double t_new = (2.0e0 / 3.0e0) * t_star + (1.0e0 / 3.0e0) * s->t + (2.0e0 / 3.0e0) * dt;
+            // Qnew's time after the step: RK3 keeps UpdateSoln.cpp:27's
+            // bookkeeping over its stages; FinSolveMD.cpp:162 and
+            // FinSolveLxW.cpp:175 set Qold.t + dt (= told + dt here).
+            double t_new;
+            if (p.time_stepping_method == FIN_TS_RK) {
+                t_star = 1.0 * s->t + 0.0 * t_star + 1.0 * dt;
+                t_star = 0.75 * s->t + 0.25 * t_star + 0.25 * dt;
+                t_new = (2.0e0 / 3.0e0) * t_star + (1.0e0 / 3.0e0) * s->t + (2.0e0 / 3.0e0) * dt;
+            } else {
+                t_new = s->t + dt;
+            }
             if (cfl > 0.0) dt = Min(dtv[2], dt * CFL_target / cfl);
             else dt = dtv[2];
             if (p.verbosity)
-                printf("FinSolveRK2D ... Step%5d   CFL =%6.3f   dt =%11.3e   t =%11.3e\n", n_step, cfl, dt, t);
+                printf("%s ... Step%5d   CFL =%6.3f   dt =%11.3e   t =%11.3e\n",
+                       p.time_stepping_method == FIN_TS_RK ? "FinSolveRK2D"
+                                                           : (p.time_stepping_method == FIN_TS_MD ? "FinSolveMD2D" : "FinSolveLxW2D"),
+                       n_step, cfl, dt, t);
             if (cfl <= CFL_max && nonfinite) {
                 rc = set_err(FIN_ERR_NONFINITE, "non-finite wave speed or state in an accepted step");
                 goto done;

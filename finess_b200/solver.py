@@ -59,6 +59,8 @@ def load_library(path=LIB_PATH):
     lib.fin_set_kernel_timing.argtypes = [vp, C.c_int]
     lib.fin_kernel_time.argtypes = [vp, C.POINTER(C.c_double), C.POINTER(C.c_longlong)]
     lib.fin_fma_peak.argtypes = [C.c_int, C.POINTER(C.c_double)]
+    lib.fin_construct_integrated_r.argtypes = [vp, C.c_double, _dp, _dp, _dp]
+    lib.fin_construct_integrated_r.restype = C.c_int
     lib.fin_params_from_ini.argtypes = [C.c_char_p, P]
     lib.fin_params_from_ini.restype = C.c_int
     lib.fin_ini_last_error.restype = C.c_char_p
@@ -152,6 +154,18 @@ class Solver:
         n = C.c_int()
         _check(self.lib.fin_solve(self.h, tend, dtv, C.byref(n)))
         return dtv, n.value
+
+    # FinSolveMD (lib/2d/FinSolveMD.cpp:21) and FinSolveLxW (FinSolveLxW.cpp:16)
+    # run through the same driver; the solver's time_stepping_method picks the steps.
+    FinSolveMD = FinSolveRK
+    FinSolveLxW = FinSolveRK
+
+    def ConstructIntegratedR(self, dt, q):
+        """1-state ConstructIntegratedR; returns ghosted F, G (interior + 3 ghost layers set)."""
+        F = np.zeros(ghosted_shape(self.p))
+        G = np.zeros(ghosted_shape(self.p))
+        _check(self.lib.fin_construct_integrated_r(self.h, dt, np.ascontiguousarray(q, dtype=np.float64), F, G))
+        return F, G
 
     def advance(self, tend, dtv, max_steps):
         """FinSolveRK stopping after max_steps accepted steps; returns (dtv, nsteps)."""

@@ -142,6 +142,13 @@ int fin_solve(fin_solver* s, double tend, double* dtv, int* nsteps_out);
  * from fin_last_kernel_ms. */
 int fin_advance(fin_solver* s, double tend, double* dtv, int max_steps, int* nsteps_out);
 
+/* ConstructIntegratedR, 1-state form (lib/2d/ConstructIntegratedR.cpp:59-296):
+ * the time-integrated fluxes F = f + dt/2 (f_t + dt/3 f_tt) (f_tt when
+ * time_order > 2) on the interior and the 3-cell ghost frame, written into
+ * ghosted host arrays F_host, G_host (other ghost entries untouched).  Needs a
+ * solver created with Lax-Wendroff or multiderivative stepping (mbc >= 5). */
+int fin_construct_integrated_r(fin_solver* s, double dt, const double* q_host, double* F_host, double* G_host);
+
 /* One time step of exactly dt with no CFL control (benchmarking and
  * per-step parity); cfl_out (may be NULL) receives GetCFL's value for it. */
 int fin_step_fixed(fin_solver* s, double dt, double* cfl_out);

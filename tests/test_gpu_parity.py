@@ -202,3 +202,60 @@ def test_nan_producing_attempt_is_rejected_not_fatal(Solver):
         qg, tg = s.get_state()
     assert ng > 0 and abs(tg - 0.01) < 1e-12
     assert np.all(np.isfinite(interior(p, qg)))
+
+
+# ---------------------------------------------------------------------------
+# Lax-Wendroff / two-stage multiderivative path
+# ---------------------------------------------------------------------------
+@pytest.mark.parametrize("path", golden_cases("intr_"))
+def test_integrated_flux_golden(Solver, path):
+    g = load_golden(path)
+    p = g["p"]
+    with Solver(p) as s:
+        F, G = s.ConstructIntegratedR(float(g["dt"]), g["q"])
+    mb = p.mbc
+    E = (slice(mb - 3, mb + p.mx + 3), slice(mb - 3, mb + p.my + 3))
+    assert rel_linf(F[E], g["F"][E]) <= TOL_STEP
+    assert rel_linf(G[E], g["G"][E]) <= TOL_STEP
+
+
+@pytest.mark.parametrize("path", golden_cases("finsolvemd_") + golden_cases("finsolvelxw_"))
+def test_finsolve_md_lxw_golden(Solver, path):
+    g = load_golden(path)
+    p = g["p"]
+    with Solver(p) as s:
+        s.set_state(g["q0"], float(g["t0"]))
+        dtv, n = s.FinSolveMD(float(g["tend"]), [0.0, float(g["dt0"]), p.max_dt])
+        q1, t1 = s.get_state()
+    assert rel_linf(interior(p, q1), interior(p, g["q1"])) <= TOL_FRAME
+    assert abs(t1 - float(g["t1"])) <= 1e-14 * abs(float(g["t1"]))
+    assert abs(dtv[1] - float(g["dt1"])) <= 1e-10 * float(g["dt1"])
+
+
+@pytest.mark.parametrize("method", ["md", "lxw"])
+@pytest.mark.parametrize("kind", ["riemann", "smooth"])
+def test_md_lxw_steps_vs_oracle(Solver, oracle, method, kind):
+    """Two fixed-dt steps on ragged grids, against the oracle, per step."""
+    from finess_b200._abi import FIN_BC_PERIODIC, FIN_TS_LXW, FIN_TS_MD
+    rng = np.random.default_rng(21)
+    p = P.riemann_params(n=41, weno=FIN_WENO_Z, method=FIN_TS_MD)
+    p.my = 35
+    if method == "lxw":
+        p.time_stepping_method = FIN_TS_LXW
+        p.time_order = 3
+    if kind == "smooth":
+        p.bc_xlow = p.bc_xhigh = p.bc_ylow = p.bc_yhigh = FIN_BC_PERIODIC
+        q = P.random_smooth_state(p, rng)
+    else:
+        q = P.random_riemann_state(p, rng)
+    q = oracle.set_bnd(p, q)
+    dt = 0.15 / 41 / 3.0
+    with Solver(p) as s:
+        s.set_state(q)
+        qo = q
+        for _ in range(2):
+            cg = s.step_fixed(dt)
+            qo, co = oracle.step_fixed(p, qo, dt)
+            qg, _ = s.get_state()
+            assert rel_linf(interior(p, qg), interior(p, qo)) <= TOL_STEP
+            assert abs(cg - co) <= 1e-14 * co
