@@ -181,6 +181,32 @@ int fin_device_layout(fin_solver* s, size_t* plane_stride, size_t* row_stride);
 /* Device pointer to the solver's current state planes (FP64). */
 int fin_state_device_ptr(fin_solver* s, double** q_dev);
 
+/* ---- troubled-cell indicator network ---------------------------------- */
+/* No counterpart in the reference (its WENO weights are the labels the
+ * network learns, lib/WenoReconstruct.cpp:131-134 against :104).  A
+ * 20 -> 32 -> 32 -> 1 GELU network with BF16 weights and activations and FP32
+ * accumulation, run and trained on tcgen05 tensor cores.  Parameters (FP32,
+ * fin_mlp_nparam() values): W1[32][20], b1[32], W2[32][32], b2[32], w3[32], b3. */
+typedef struct fin_mlp fin_mlp;
+int fin_mlp_nparam(void);
+const char* fin_mlp_last_error(void);
+/* params == NULL: He-uniform initialisation from seed. */
+int fin_mlp_create(const float* params, unsigned long long seed, fin_mlp** out);
+int fin_mlp_destroy(fin_mlp* m);
+int fin_mlp_get_params(fin_mlp* m, float* out);
+int fin_mlp_set_params(fin_mlp* m, const float* in);
+int fin_mlp_device_params(fin_mlp* m, const float** P);
+/* Logits z[n] of the n x 20 feature rows X (host arrays). */
+int fin_mlp_forward(fin_mlp* m, const float* X_host, long long n, float* z_host);
+/* Gradient of the weighted binary cross-entropy (mean over the n rows; label
+ * rows weigh pos_weight when y = 1) with respect to the parameters. */
+int fin_mlp_gradients(fin_mlp* m, const float* X_host, const unsigned char* y_host, long long n, float pos_weight,
+                      float* grad_host, float* loss);
+/* Adam training: epochs over the n rows in shuffled batches; epoch_loss
+ * (may be NULL) receives the mean loss of each epoch. */
+int fin_mlp_train(fin_mlp* m, const float* X_host, const unsigned char* y_host, long long n, int epochs, int batch,
+                  float lr, float pos_weight, unsigned long long seed, float* epoch_loss);
+
 /* ---- for callers that cannot allocate device memory ------------------- */
 /* No counterpart in the reference.  For callers that must not call
  * cudaMalloc (an application whose own allocator owns the device, or a loop
