@@ -56,6 +56,11 @@ struct StageArgs {
     const double* Fg;
     const double* Gg;
     size_t gplane;
+    // Hybrid form: troubled-face flags of the step (x faces then y faces, as
+    // written by the indicator).  A face takes full WENO when any flag in the
+    // 3 x 3 window of same-direction faces around it is set, else the linear
+    // FD5 weights (lib/WenoReconstruct.cpp:580-616).
+    const unsigned char* flags;
 };
 
 template <int TI_, int TJ_, int NT_>
@@ -149,7 +154,7 @@ __device__ __forceinline__ void right_add(const typename Euler::Eig<R>& e, int k
     }
 }
 
-template <class R, int VER, bool P2, class Cfg, bool FG = false>
+template <class R, int VER, bool P2, class Cfg, bool FG = false, bool HYB = false>
 __global__ void __launch_bounds__(Cfg::NT, MinBlocks<R>::value) k_stage(const StageArgs a)
 {
     constexpr int TI = Cfg::TI, TJ = Cfg::TJ, NT = Cfg::NT, H = Cfg::H;
@@ -287,6 +292,27 @@ __global__ void __launch_bounds__(Cfg::NT, MinBlocks<R>::value) k_stage(const St
             alpha = Max(isx ? ag1 : ag2, Max(fabs(s1), fabs(s2)));
         }
         if (!(alpha <= R(1e30))) nonfinite = true;
+        bool trb = true;
+        if (HYB) {
+            trb = false;
+            const long long nxf = (long long)(mx + 1) * my;
+            if (isx) {
+                const int gfi = i0 + fi, gj = j0 + fj;
+                for (int di = -1; di <= 1; di++)
+                    for (int dj = -1; dj <= 1; dj++) {
+                        const int a1 = gfi + di, b1 = gj + dj;
+                        if (a1 >= 0 && a1 <= mx && b1 >= 0 && b1 < my) trb |= a.flags[(long long)a1 * my + b1] != 0;
+                    }
+            } else {
+                const int gi = i0 + fi, gfj = j0 + fj;
+                for (int di = -1; di <= 1; di++)
+                    for (int dj = -1; dj <= 1; dj++) {
+                        const int a1 = gi + di, b1 = gfj + dj;
+                        if (a1 >= 0 && a1 < mx && b1 >= 0 && b1 <= my)
+                            trb |= a.flags[nxf + (long long)a1 * (my + 1) + b1] != 0;
+                    }
+            }
+        }
         // gp = 0.5 (L f + l_alpha L q) = L (0.5 f + 0.5 l_alpha q), points
         // 0..4; gm the same with -l_alpha, points 5..1 (ConstructL.cpp:179-185).
         const R lah = R(0.5) * Par<R>::ascale(a) * alpha;
@@ -323,7 +349,7 @@ __global__ void __launch_bounds__(Cfg::NT, MinBlocks<R>::value) k_stage(const St
                     up[t] = k == 0 ? p0[t] : p4[t];
                     um[t] = k == 0 ? m0[t] : m4[t];
                 }
-                right_add<R>(ev, k == 0 ? 0 : 4, weno_pair<R, VER, P2>(up, um, eps, pw), fh);
+                right_add<R>(ev, k == 0 ? 0 : 4, (trb ? weno_pair<R, VER, P2>(up, um, eps, pw) : weno_pair<R, FIN_WENO_FD, true>(up, um, eps, pw)), fh);
             }
         }
         {
@@ -347,7 +373,7 @@ __global__ void __launch_bounds__(Cfg::NT, MinBlocks<R>::value) k_stage(const St
                     m1[5 - s] = Euler::left1(ev, rw, v);
                 }
             }
-            right_add<R>(ev, 1, weno_pair<R, VER, P2>(p1, m1, eps, pw), fh);
+            right_add<R>(ev, 1, (trb ? weno_pair<R, VER, P2>(p1, m1, eps, pw) : weno_pair<R, FIN_WENO_FD, true>(p1, m1, eps, pw)), fh);
         }
         {
             // pass 3: fields 2 and 3 (rows v_t - u2 v0 and v_w - u3 v0)
@@ -379,7 +405,7 @@ __global__ void __launch_bounds__(Cfg::NT, MinBlocks<R>::value) k_stage(const St
                     up[t] = k == 0 ? p2[t] : p3[t];
                     um[t] = k == 0 ? m2[t] : m3[t];
                 }
-                right_add<R>(ev, k == 0 ? 2 : 3, weno_pair<R, VER, P2>(up, um, eps, pw), fh);
+                right_add<R>(ev, k == 0 ? 2 : 3, (trb ? weno_pair<R, VER, P2>(up, um, eps, pw) : weno_pair<R, FIN_WENO_FD, true>(up, um, eps, pw)), fh);
             }
         }
         // Back to (rho, rho u, rho v, rho w, E) and store.

@@ -17,6 +17,7 @@
 #include "finess_b200.h"
 #include "fin_stage.cuh"
 #include "fin_intflux.cuh"
+#include "fin_hybrid.cuh"
 
 using namespace fin;
 
@@ -47,9 +48,13 @@ int set_err(int code, const std::string& msg)
 using Cfg = TileCfg<FIN_TILE_TI, FIN_TILE_TJ, FIN_TILE_NT>;
 
 // Reduction slots (doubles) in one device block, reset by one memset per step.
-// The status word (bit 0: non-finite speed or state, bit 1: negative p or rho)
-// sits in slot STATUS so one copy returns it with the maxima.
-enum { SLOT_SMAX = 0, SLOT_ALPHA = 2, SLOT_STATUS = 10, NSLOTS = 11 };
+// The status word (bit 0: non-finite speed or state, bit 1: negative p or rho,
+// bit 2: a tensor-core wait ran out) sits in slot STATUS so one copy returns it
+// with the maxima.  SMAX_ALT keeps the face-speed maxima of the hybrid attempt
+// while a judge step recomputes with full WENO; DIFF receives the judge's
+// max |q_hybrid - q_full| and max |q_full|.
+enum { NBUF = 5, SLOT_SMAX = 0, SLOT_ALPHA = 2, SLOT_STATUS = SLOT_ALPHA + 2 * NBUF, SLOT_SMAX_ALT = SLOT_STATUS + 1,
+       SLOT_DIFF = SLOT_SMAX_ALT + 2, NSLOTS = SLOT_DIFF + 2 };
 
 }  // namespace
 
@@ -57,7 +62,7 @@ struct fin_solver {
     fin_params p;
     double dx, dy;
     size_t plane;           // elements per component plane
-    double* q[4];           // state buffers (planes); q[cur] holds q^n
+    double* q[NBUF];        // state buffers (planes); q[cur] holds q^n; q[4] only in the hybrid form
     int cur;                // index of q^n
     double* slots;          // NSLOTS doubles (+ status word after them)
     unsigned int* status;
@@ -78,6 +83,16 @@ struct fin_solver {
     long long kernel_launches;
     double t;               // Qnew.get_t()
     double step_ms;
+    // hybrid form
+    float* mlpP;            // network parameters on the device
+    unsigned char* flags;   // troubled-face flags of the current step
+    unsigned long long* ind_count;
+    float zthr;
+    int judge_every;
+    double judge_tol;
+    long long hstep, judges, reverts, troubled_last, faces;
+    int hyb_off;            // steps left with the indicator switched off after a revert
+    bool judge_pending;     // the last take_stages ran a judge (results in q[nxt] and q[4])
     bool alpha_valid;       // slots hold alpha of q[cur]
     double last_ms;
     long long launches;
@@ -191,11 +206,11 @@ __global__ void k_fma_peak(R* out, int iters, R a, R b)
 // ---------------------------------------------------------------------------
 namespace {
 
-template <class R, int VER, bool P2, bool FG = false>
+template <class R, int VER, bool P2, bool FG = false, bool HYB = false>
 int launch_stage_t(fin_solver* s, const StageArgs& a)
 {
     const size_t smem = Cfg::smem_bytes<R>();
-    auto kern = k_stage<R, VER, P2, Cfg, FG>;
+    auto kern = k_stage<R, VER, P2, Cfg, FG, HYB>;
     static bool configured = false;   // per instantiation; attribute is per device function
     if (!configured) {
         CK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
@@ -236,9 +251,27 @@ int launch_stage_fg(fin_solver* s, const StageArgs& a)
     return set_err(FIN_ERR_ARG, "weno_version");
 }
 
+// Hybrid stages: FP32 with per-face choice between full WENO and FD5.
+int launch_stage_hyb(fin_solver* s, const StageArgs& a)
+{
+    const bool p2 = s->p.power_param == 2.0;
+    switch (s->p.weno_version) {
+    case FIN_WENO_JS:
+        return p2 ? launch_stage_t<float, FIN_WENO_JS, true, false, true>(s, a)
+                  : launch_stage_t<float, FIN_WENO_JS, false, false, true>(s, a);
+    case FIN_WENO_Z:
+        return p2 ? launch_stage_t<float, FIN_WENO_Z, true, false, true>(s, a)
+                  : launch_stage_t<float, FIN_WENO_Z, false, false, true>(s, a);
+    case FIN_WENO_FD: return launch_stage_t<float, FIN_WENO_FD, true, false, false>(s, a);
+    }
+    return set_err(FIN_ERR_ARG, "weno_version");
+}
+
 int launch_stage(fin_solver* s, const StageArgs& a)
 {
     if (a.Fg) return launch_stage_fg(s, a);
+    if (a.flags) return launch_stage_hyb(s, a);
+    if (s->p.precision == FIN_PREC_HYBRID) return launch_stage_r<float>(s, a);
     if (s->p.precision == FIN_PREC_FP64) return launch_stage_r<double>(s, a);
     if (s->p.precision == FIN_PREC_FP32) return launch_stage_r<float>(s, a);
     return set_err(FIN_ERR_UNSUPPORTED, "precision form not built");
@@ -350,7 +383,40 @@ int launch_intflux(fin_solver* s, int mode, const double* q1, const double* q2, 
     return FIN_OK;
 }
 
-int take_stages_rk(fin_solver* s, double dt, int nxt);
+int take_stages_rk(fin_solver* s, double dt, int nxt, const unsigned char* flags, int q1, int q2);
+
+// Troubled-face flags of q[buf] (fin_hybrid.cuh).
+int launch_indicator(fin_solver* s, int buf)
+{
+    IndicatorArgs ia;
+    memset(&ia, 0, sizeof(ia));
+    ia.q = s->q[buf];
+    ia.plane = s->plane;
+    ia.mx = s->p.mx;
+    ia.my = s->p.my;
+    ia.bc[0] = s->p.bc_xlow; ia.bc[1] = s->p.bc_xhigh; ia.bc[2] = s->p.bc_ylow; ia.bc[3] = s->p.bc_yhigh;
+    ia.gamma = float(s->p.gamma);
+    ia.P = s->mlpP;
+    ia.zthr = s->zthr;
+    ia.flags = s->flags;
+    ia.status = s->status;
+    ia.count = s->ind_count;
+    static bool configured = false;
+    const size_t smem = std::max(sizeof(IndSmem), size_t(29 * 1024));   // <= 8 CTAs per SM: TMEM never waits
+    if (!configured) {
+        CK(cudaFuncSetAttribute(k_indicator, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
+        configured = true;
+    }
+    CK(cudaMemsetAsync(s->ind_count, 0, sizeof(unsigned long long), s->stream));
+    const long long nf = (long long)(s->p.mx + 1) * s->p.my + (long long)s->p.mx * (s->p.my + 1);
+    const long long tiles = (nf + mlp::TILE - 1) / mlp::TILE;
+    const int grid = int(std::min<long long>(tiles, 148 * 8));
+    k_indicator<<<grid, mlp::TILE, smem, s->stream>>>(ia);
+    s->launches++;
+    s->faces = nf;
+    CK(cudaGetLastError());
+    return FIN_OK;
+}
 
 // Lax-Wendroff (FinSolveLxW.cpp:120-176) and two-stage multiderivative
 // (FinSolveMD.cpp:116-170, time_order 4) steps from q[cur] into q[nxt].
@@ -395,25 +461,90 @@ int take_stages_lw(fin_solver* s, double dt, int nxt)
     return launch_stage_timed(s, a, 1);
 }
 
+int launch_indicator(fin_solver* s, int buf);
+
+// The two stage registers of a step from q[cur] into q[nxt]: the first two
+// buffers that are neither (buffer 4 is reserved for the judge step).
+void stage_registers(fin_solver* s, int nxt, int* q1, int* q2)
+{
+    int reg[2], k = 0;
+    for (int b = 0; b < 4 && k < 2; b++)
+        if (b != s->cur && b != nxt) reg[k++] = b;
+    *q1 = reg[0];
+    *q2 = reg[1];
+}
+
 int take_stages(fin_solver* s, double dt, int nxt)
 {
-    if (s->p.time_stepping_method == FIN_TS_RK) return take_stages_rk(s, dt, nxt);
-    return take_stages_lw(s, dt, nxt);
+    s->judge_pending = false;
+    if (s->p.time_stepping_method != FIN_TS_RK) return take_stages_lw(s, dt, nxt);
+    int q1, q2, rc;
+    stage_registers(s, nxt, &q1, &q2);
+    if (s->p.precision != FIN_PREC_HYBRID || !s->mlpP) return take_stages_rk(s, dt, nxt, nullptr, q1, q2);
+    // Hybrid form: flags from the indicator on q^n, FP32 stages with the
+    // per-face choice; every judge_every-th step also a full-WENO FP32 step
+    // from the same q^n into q[4], compared on the device.
+    const bool active = s->hyb_off == 0;
+    if (!active) {
+        s->hyb_off--;
+        return take_stages_rk(s, dt, nxt, nullptr, q1, q2);
+    }
+    if ((rc = launch_indicator(s, s->cur))) return rc;
+    if ((rc = take_stages_rk(s, dt, nxt, s->flags, q1, q2))) return rc;
+    s->hstep++;
+    if (s->judge_every > 0 && s->hstep % s->judge_every == 0) {
+        CK(cudaMemcpyAsync(s->slots + SLOT_SMAX_ALT, s->slots + SLOT_SMAX, 2 * sizeof(double), cudaMemcpyDeviceToDevice,
+                           s->stream));
+        if ((rc = take_stages_rk(s, dt, 4, nullptr, q1, q2))) return rc;
+        CK(cudaMemsetAsync(s->slots + SLOT_DIFF, 0, 2 * sizeof(double), s->stream));
+        const size_t n = size_t(s->p.mx) * s->p.my;
+        k_max_diff<<<grid_blocks(n), 256, 0, s->stream>>>(s->q[nxt], s->q[4], s->plane, n, s->slots + SLOT_DIFF);
+        s->launches++;
+        CK(cudaGetLastError());
+        s->judge_pending = true;
+    }
+    return FIN_OK;
+}
+
+// After get_cfl brought the slots to the host: settle a judge step.  Keeps
+// the hybrid result (and its face-speed maxima) unless it differs from the
+// full-WENO result by more than judge_tol (relative L-infinity); then the
+// full result is taken (moved into q[nxt]), its maxima give the CFL, and the
+// indicator stays off for judge_every steps.
+void settle_judge(fin_solver* s, int nxt, double dt, double* cfl)
+{
+    if (!s->judge_pending) return;
+    s->judges++;
+    const double d = s->h_slots[SLOT_DIFF], m = s->h_slots[SLOT_DIFF + 1];
+    const bool revert = !(d <= s->judge_tol * (m > 0 ? m : 1.0));
+    double sx, sy;
+    if (revert) {
+        // q[nxt] <- the full-WENO result (pointer swap), with its alpha slot
+        s->reverts++;
+        s->hyb_off = s->judge_every;
+        std::swap(s->q[4], s->q[nxt]);
+        cudaMemcpyAsync(alpha_slot(s, nxt), alpha_slot(s, 4), 2 * sizeof(double), cudaMemcpyDeviceToDevice, s->stream);
+        sx = s->h_slots[SLOT_SMAX];
+        sy = s->h_slots[SLOT_SMAX + 1];
+    } else {
+        sx = s->h_slots[SLOT_SMAX_ALT];
+        sy = s->h_slots[SLOT_SMAX_ALT + 1];
+    }
+    double c = -100.0;
+    c = Max(dt * sx / s->dx, c);
+    c = Max(dt * sy / s->dy, c);
+    *cfl = c;
 }
 
 // The stages of one step of size dt from q[cur] into q[nxt] (RK3:
 // FinSolveRK.cpp:158-211 with SetRKinfo.cpp:50-64).  Leaves the face-speed
 // maxima of the step in slots SMAX and alpha(q[nxt]) in its slot.
-int take_stages_rk(fin_solver* s, double dt, int nxt)
+int take_stages_rk(fin_solver* s, double dt, int nxt, const unsigned char* flags, int q1, int q2)
 {
     const fin_params& p = s->p;
     if (p.time_order != 3)
         return set_err(FIN_ERR_UNSUPPORTED, "only SSP-RK3 (time_order 3) is built");
     const int qn = s->cur;
-    int reg[2], k = 0;
-    for (int b = 0; b < 4 && k < 2; b++)
-        if (b != qn && b != nxt) reg[k++] = b;
-    const int q1 = reg[0], q2 = reg[1];
     // reset smax, the status word and the alpha slots of the three buffers
     // written this step
     CK(cudaMemsetAsync(s->slots + SLOT_SMAX, 0, 2 * sizeof(double), s->stream));
@@ -425,6 +556,7 @@ int take_stages_rk(fin_solver* s, double dt, int nxt)
     int rc;
     StageArgs a = base_args(s);
     a.smax_out = s->slots + SLOT_SMAX;
+    a.flags = flags;
     // stage 1: q1 = 1*q^n + 0*q* + (1*dt) L(q^n)
     a.qin = s->q[qn]; a.A = s->q[qn]; a.B = nullptr; a.qout = s->q[q1];
     a.a1 = 1.0; a.a2 = 0.0; a.bdt = 1.0 * dt;
@@ -500,8 +632,10 @@ int validate(const fin_params* p)
     const int H = 3;
     if ((p->bc_xlow == FIN_BC_PERIODIC && p->mx < H) || (p->bc_ylow == FIN_BC_PERIODIC && p->my < H))
         return set_err(FIN_ERR_ARG, "periodic direction shorter than the stencil halo");
-    if (p->precision != FIN_PREC_FP64 && p->precision != FIN_PREC_FP32)
-        return set_err(FIN_ERR_UNSUPPORTED, "precision form not built");
+    if (p->precision != FIN_PREC_FP64 && p->precision != FIN_PREC_FP32 && p->precision != FIN_PREC_HYBRID)
+        return set_err(FIN_ERR_ARG, "unknown precision form");
+    if (p->precision == FIN_PREC_HYBRID && p->time_stepping_method != FIN_TS_RK)
+        return set_err(FIN_ERR_UNSUPPORTED, "the hybrid form is built for SSP-RK3");
     return FIN_OK;
 }
 
@@ -569,8 +703,18 @@ int fin_create(const fin_params* p, fin_solver** out)
         return set_err(FIN_ERR_CUDA, std::string(what) + ": " + cudaGetErrorString(e));
     };
     cudaError_t e;
-    for (int b = 0; b < 4; b++)
+    const int nbuf = p->precision == FIN_PREC_HYBRID ? 5 : 4;
+    for (int b = 0; b < nbuf; b++)
         if ((e = cudaMalloc(&s->q[b], MEQN * s->plane * sizeof(double))) != cudaSuccess) return fail(e, "cudaMalloc state");
+    if (p->precision == FIN_PREC_HYBRID) {
+        const size_t nf = size_t(p->mx + 1) * p->my + size_t(p->mx) * (p->my + 1);
+        if ((e = cudaMalloc(&s->flags, nf)) != cudaSuccess) return fail(e, "cudaMalloc flags");
+        if ((e = cudaMalloc(&s->ind_count, 16)) != cudaSuccess) return fail(e, "cudaMalloc counter");
+        if ((e = cudaMemset(s->ind_count, 0, 16)) != cudaSuccess) return fail(e, "memset");
+        s->zthr = 0.0f;
+        s->judge_every = 20;
+        s->judge_tol = 1e-3;
+    }
     if (p->time_stepping_method != FIN_TS_RK) {
         s->gplane = (size_t(p->mx + 6) * (p->my + 6) + 31) / 32 * 32;
         if ((e = cudaMalloc(&s->Fg, MEQN * s->gplane * sizeof(double))) != cudaSuccess) return fail(e, "cudaMalloc F");
@@ -585,7 +729,7 @@ int fin_create(const fin_params* p, fin_solver** out)
     for (int k = 0; k < 6; k++)
         if ((e = cudaEventCreate(&s->kev[k])) != cudaSuccess) return fail(e, "event");
     if ((e = cudaMemsetAsync(s->slots, 0, NSLOTS * sizeof(double), s->stream)) != cudaSuccess) return fail(e, "memset");
-    for (int b = 0; b < 4; b++)
+    for (int b = 0; b < nbuf; b++)
         if ((e = cudaMemsetAsync(s->q[b], 0, MEQN * s->plane * sizeof(double), s->stream)) != cudaSuccess) return fail(e, "memset");
     if ((e = cudaStreamSynchronize(s->stream)) != cudaSuccess) return fail(e, "sync");
     s->t = 0.0;
@@ -597,7 +741,10 @@ int fin_destroy(fin_solver* s)
 {
     if (!s) return FIN_OK;
     if (s->stream) cudaStreamSynchronize(s->stream);
-    for (int b = 0; b < 4; b++) cudaFree(s->q[b]);
+    for (int b = 0; b < NBUF; b++) cudaFree(s->q[b]);
+    cudaFree(s->mlpP);
+    cudaFree(s->flags);
+    cudaFree(s->ind_count);
     cudaFree(s->slots);
     cudaFree(s->d_aos);
     cudaFree(s->d_aux);
@@ -739,6 +886,65 @@ int fin_construct_l(fin_solver* s, const double* q_host, double* L_host, double*
     return check_status(s);
 }
 
+int fin_set_indicator(fin_solver* s, const float* params, float z_threshold, int judge_every, double judge_tol)
+{
+    if (!s || !params) return set_err(FIN_ERR_ARG, "null argument");
+    if (s->p.precision != FIN_PREC_HYBRID) return set_err(FIN_ERR_ARG, "the solver was not created in the hybrid form");
+    if (!s->mlpP) CK(cudaMalloc(&s->mlpP, mlp::NPARAM * sizeof(float)));
+    CK(cudaMemcpyAsync(s->mlpP, params, mlp::NPARAM * sizeof(float), cudaMemcpyHostToDevice, s->stream));
+    CK(cudaStreamSynchronize(s->stream));
+    s->zthr = z_threshold;
+    s->judge_every = judge_every;
+    s->judge_tol = judge_tol;
+    s->hyb_off = 0;
+    return FIN_OK;
+}
+
+int fin_hybrid_stats(fin_solver* s, long long* troubled_faces, long long* faces, long long* judges, long long* reverts)
+{
+    if (!s) return set_err(FIN_ERR_ARG, "null solver");
+    if (s->ind_count) {
+        unsigned long long c = 0;
+        CK(cudaMemcpyAsync(&c, s->ind_count, sizeof(c), cudaMemcpyDeviceToHost, s->stream));
+        CK(cudaStreamSynchronize(s->stream));
+        s->troubled_last = (long long)c;
+    }
+    if (troubled_faces) *troubled_faces = s->troubled_last;
+    if (faces) *faces = s->faces;
+    if (judges) *judges = s->judges;
+    if (reverts) *reverts = s->reverts;
+    return FIN_OK;
+}
+
+int fin_face_samples(fin_solver* s, long long offset, long long stride, long long max_n, float* X_host,
+                     unsigned char* y_host, long long* n_out)
+{
+    if (!s || !X_host || !y_host || !n_out || stride < 1 || offset < 0) return set_err(FIN_ERR_ARG, "bad argument");
+    const fin_params& p = s->p;
+    const long long nf = (long long)(p.mx + 1) * p.my + (long long)p.mx * (p.my + 1);
+    long long n = offset < nf ? (nf - offset + stride - 1) / stride : 0;
+    if (n > max_n) n = max_n;
+    *n_out = n;
+    if (n == 0) return FIN_OK;
+    int rc;
+    if (p.global_alpha && !s->alpha_valid && (rc = compute_alpha(s, s->cur))) return rc;
+    float* dX = nullptr;
+    unsigned char* dy = nullptr;
+    CK(cudaMallocAsync(&dX, size_t(n) * ind::NFEAT * sizeof(float), s->stream));
+    CK(cudaMallocAsync(&dy, size_t(n), s->stream));
+    k_face_samples<<<grid_blocks(size_t(n)), 256, 0, s->stream>>>(
+        s->q[s->cur], s->plane, p.mx, p.my, p.bc_xlow, p.bc_xhigh, p.bc_ylow, p.bc_yhigh, p.gamma, p.epsilon,
+        p.power_param, p.alpha_scaling, p.global_alpha ? alpha_slot(s, s->cur) : nullptr, offset, stride, n, dX, dy);
+    s->launches++;
+    CK(cudaGetLastError());
+    CK(cudaMemcpyAsync(X_host, dX, size_t(n) * ind::NFEAT * sizeof(float), cudaMemcpyDeviceToHost, s->stream));
+    CK(cudaMemcpyAsync(y_host, dy, size_t(n), cudaMemcpyDeviceToHost, s->stream));
+    CK(cudaFreeAsync(dX, s->stream));
+    CK(cudaFreeAsync(dy, s->stream));
+    CK(cudaStreamSynchronize(s->stream));
+    return FIN_OK;
+}
+
 // ConstructIntegratedR, 1-state (lib/2d/ConstructIntegratedR.cpp:59-296).
 int fin_construct_integrated_r(fin_solver* s, double dt, const double* q_host, double* F_host, double* G_host)
 {
@@ -778,6 +984,7 @@ int fin_step_fixed(fin_solver* s, double dt, double* cfl_out)
     bool nonfinite = false;
     if ((rc = get_cfl(s, dt, 1e300, &cfl, &nonfinite))) return rc;
     if ((rc = collect_kernel_times(s))) return rc;
+    settle_judge(s, nxt, dt, &cfl);
     if (nonfinite) return set_err(FIN_ERR_NONFINITE, "non-finite wave speed or state");
     float ms = 0.f;
     CK(cudaEventElapsedTime(&ms, s->ev0, s->ev1));
@@ -823,6 +1030,7 @@ int fin_advance(fin_solver* s, double tend, double* dtv, int max_steps, int* nst
             bool nonfinite = false;
             if ((rc = get_cfl(s, dt, dtv[2], &cfl, &nonfinite))) goto done;
             if ((rc = collect_kernel_times(s))) goto done;
+            settle_judge(s, nxt, dt, &cfl);
             // Qnew's time after the step: RK3 keeps UpdateSoln.cpp:27's
             // bookkeeping over its stages; FinSolveMD.cpp:162 and
             // FinSolveLxW.cpp:175 set Qold.t + dt (= told + dt here).

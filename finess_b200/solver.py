@@ -59,6 +59,15 @@ def load_library(path=LIB_PATH):
     lib.fin_set_kernel_timing.argtypes = [vp, C.c_int]
     lib.fin_kernel_time.argtypes = [vp, C.POINTER(C.c_double), C.POINTER(C.c_longlong)]
     lib.fin_fma_peak.argtypes = [C.c_int, C.POINTER(C.c_double)]
+    lib.fin_set_indicator.argtypes = [vp, np.ctypeslib.ndpointer(np.float32, flags="C_CONTIGUOUS"), C.c_float,
+                                      C.c_int, C.c_double]
+    lib.fin_set_indicator.restype = C.c_int
+    lib.fin_hybrid_stats.argtypes = [vp] + [C.POINTER(C.c_longlong)] * 4
+    lib.fin_hybrid_stats.restype = C.c_int
+    lib.fin_face_samples.argtypes = [vp, C.c_longlong, C.c_longlong, C.c_longlong,
+                                     np.ctypeslib.ndpointer(np.float32, flags="C_CONTIGUOUS"),
+                                     np.ctypeslib.ndpointer(np.uint8, flags="C_CONTIGUOUS"), C.POINTER(C.c_longlong)]
+    lib.fin_face_samples.restype = C.c_int
     lib.fin_construct_integrated_r.argtypes = [vp, C.c_double, _dp, _dp, _dp]
     lib.fin_construct_integrated_r.restype = C.c_int
     lib.fin_params_from_ini.argtypes = [C.c_char_p, P]
@@ -166,6 +175,29 @@ class Solver:
         G = np.zeros(ghosted_shape(self.p))
         _check(self.lib.fin_construct_integrated_r(self.h, dt, np.ascontiguousarray(q, dtype=np.float64), F, G))
         return F, G
+
+    def set_indicator(self, params, z_threshold=0.0, judge_every=20, judge_tol=1e-3):
+        """Hybrid form: the troubled-face network's parameters and the judge step."""
+        _check(self.lib.fin_set_indicator(self.h, np.ascontiguousarray(params, dtype=np.float32), z_threshold,
+                                          judge_every, judge_tol))
+
+    def hybrid_stats(self):
+        v = [C.c_longlong() for _ in range(4)]
+        _check(self.lib.fin_hybrid_stats(self.h, *[C.byref(x) for x in v]))
+        return {"troubled_faces": v[0].value, "faces": v[1].value, "judges": v[2].value, "reverts": v[3].value}
+
+    def face_samples(self, offset=0, stride=1, max_n=None):
+        """Indicator features (n x 20) and WENO-JS labels of the current state's faces."""
+        p = self.p
+        nf = (p.mx + 1) * p.my + p.mx * (p.my + 1)
+        n = (nf - offset + stride - 1) // stride
+        if max_n is not None:
+            n = min(n, max_n)
+        X = np.zeros((n, 20), dtype=np.float32)
+        y = np.zeros(n, dtype=np.uint8)
+        nout = C.c_longlong()
+        _check(self.lib.fin_face_samples(self.h, offset, stride, n, X, y, C.byref(nout)))
+        return X[:nout.value], y[:nout.value]
 
     def advance(self, tend, dtv, max_steps):
         """FinSolveRK stopping after max_steps accepted steps; returns (dtv, nsteps)."""

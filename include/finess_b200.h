@@ -207,6 +207,24 @@ int fin_mlp_gradients(fin_mlp* m, const float* X_host, const unsigned char* y_ho
 int fin_mlp_train(fin_mlp* m, const float* X_host, const unsigned char* y_host, long long n, int epochs, int batch,
                   float lr, float pos_weight, unsigned long long seed, float* epoch_loss);
 
+/* ---- hybrid form (precision FIN_PREC_HYBRID) --------------------------- */
+/* Network parameters (fin_mlp_nparam() floats) for the solver's troubled-face
+ * indicator; faces whose logit exceeds z_threshold (and their 3 x 3
+ * same-direction neighbours) take full WENO, all others the linear FD5
+ * weights.  Every judge_every-th step is recomputed with full WENO from the
+ * same state; a relative L-infinity difference above judge_tol reverts the
+ * step to the full result and switches the indicator off for judge_every
+ * steps (judge_every = 0: no judge).  Without this call the hybrid form runs
+ * full WENO in FP32. */
+int fin_set_indicator(fin_solver* s, const float* params, float z_threshold, int judge_every, double judge_tol);
+/* Troubled faces flagged in the last indicator pass, faces per pass, judge
+ * steps run and steps reverted. */
+int fin_hybrid_stats(fin_solver* s, long long* troubled_faces, long long* faces, long long* judges, long long* reverts);
+/* Training samples of the current state: features (20 floats) and labels of
+ * faces offset, offset + stride, ... (x faces, then y faces), at most max_n. */
+int fin_face_samples(fin_solver* s, long long offset, long long stride, long long max_n, float* X_host,
+                     unsigned char* y_host, long long* n_out);
+
 /* ---- for callers that cannot allocate device memory ------------------- */
 /* No counterpart in the reference.  For callers that must not call
  * cudaMalloc (an application whose own allocator owns the device, or a loop

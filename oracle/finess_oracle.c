@@ -847,3 +847,79 @@ void oracle_conservation_totals(const fin_params* p, const double* q, double* to
         totals[m - 1] = s;
     }
 }
+
+
+/* ---------------------------------------------------------------------- */
+/* Troubled-cell indicator: features and labels of every face              */
+/* ---------------------------------------------------------------------- */
+
+/* x faces ((mx+1) x my, j fastest) then y faces (mx x (my+1)); face (i, j)
+ * separates 0-based cells i-1 and i along its direction, stencil cells
+ * i-3 .. i+2 (ConstructL.cpp:94-113).  q ghosted with BCs applied.
+ *   X[f*20 + 5t + s]: (w_k(s+1) - w_k(s)) / max(max_s |.|, 1e-3), w = L q at
+ *     the face average, fields k = 0, mu, mv, 4 (t = 0..3);
+ *   y[f]: 1 if the WENO5-JS weights of gp or gm of any of those fields depart
+ *     from (0.1, 0.6, 0.3) by more than 10 % (WenoReconstruct.cpp:104,131-134). */
+void oracle_face_samples(const fin_params* p, const double* q, double* X, unsigned char* y)
+{
+    const grid_t g = grid_of(p, p->mx, p->my);
+    double alpha1 = 0., alpha2 = 0.;
+    if (p->global_alpha) oracle_global_wave_spd(p, q, &alpha1, &alpha2);
+    long long f = 0;
+    for (int ixy = 1; ixy <= 2; ixy++) {
+        const int ni = ixy == 1 ? g.mx + 1 : g.mx, nj = ixy == 1 ? g.my : g.my + 1;
+        for (int i = 0; i < ni; i++)
+            for (int j = 0; j < nj; j++, f++) {
+                const int di = ixy == 1 ? 1 : 0, dj = ixy == 1 ? 0 : 1;
+                /* 1-based cells of the stencil: (i+1) + di*(s-3), (j+1) + dj*(s-3) */
+                double Qs[6][MEQN_MAX], Fs[6][MEQN_MAX];
+                for (int s = 0; s < 6; s++) {
+                    const int I = i + 1 + di * (s - 3), J = j + 1 + dj * (s - 3);
+                    const double* Qp = q + IDX(&g, I, J, 1);
+                    double fx[MEQN_MAX], fy[MEQN_MAX];
+                    euler_flux(p->gamma, Qp, fx, fy);
+                    for (int m = 0; m < 5; m++) {
+                        Qs[s][m] = Qp[m];
+                        Fs[s][m] = ixy == 1 ? fx[m] : fy[m];
+                    }
+                }
+                double Qavg[MEQN_MAX];
+                for (int m = 0; m < 5; m++) Qavg[m] = 0.5 * (Qs[3][m] + Qs[2][m]);
+                eig_t el = euler_eig(ixy, p->gamma, Qavg, 0);
+                double W[6][MEQN_MAX], G[6][MEQN_MAX];
+                for (int s = 0; s < 6; s++) {
+                    euler_left(&el, Qs[s], W[s]);
+                    euler_left(&el, Fs[s], G[s]);
+                }
+                const int fields[4] = {0, el.mu, el.mv, 4};
+                for (int t = 0; t < 4; t++) {
+                    double d[5], mm = 1e-3;
+                    for (int s = 0; s < 5; s++) {
+                        d[s] = W[s + 1][fields[t]] - W[s][fields[t]];
+                        if (fabs(d[s]) > mm) mm = fabs(d[s]);
+                    }
+                    for (int s = 0; s < 5; s++) X[f * 20 + t * 5 + s] = d[s] / mm;
+                }
+                double s1, s2;
+                if (ixy == 1) euler_wave_spd(p->gamma, 1.0, 0.0, Qs[2], Qs[3], &s1, &s2);
+                else euler_wave_spd(p->gamma, 0.0, 1.0, Qs[2], Qs[3], &s1, &s2);
+                const double alpha = Max(ixy == 1 ? alpha1 : alpha2, Max(fabs(s1), fabs(s2)));
+                const double la = p->alpha_scaling * alpha;
+                double dep = 0.0;
+                for (int t = 0; t < 4; t++) {
+                    const int k = fields[t];
+                    double gp[5], gm[5], w[3];
+                    for (int s = 0; s < 5; s++) {
+                        gp[s] = 0.5 * (G[s][k] + la * W[s][k]);
+                        gm[s] = 0.5 * (G[5 - s][k] - la * W[5 - s][k]);
+                    }
+                    static const double dl[3] = {0.1, 0.6, 0.3};
+                    oracle_weno_js5_weights(p->epsilon, p->power_param, gp, w);
+                    for (int r = 0; r < 3; r++) dep = Max(dep, fabs(w[r] - dl[r]) / dl[r]);
+                    oracle_weno_js5_weights(p->epsilon, p->power_param, gm, w);
+                    for (int r = 0; r < 3; r++) dep = Max(dep, fabs(w[r] - dl[r]) / dl[r]);
+                }
+                y[f] = dep > 0.1 ? 1 : 0;
+            }
+    }
+}

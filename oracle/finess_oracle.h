@@ -55,6 +55,10 @@ int oracle_construct_lxwl(const fin_params* p, const double* q, const double* F,
 /* ConSoln totals (lib/2d/ConSoln.cpp:52-64): naive serial sum of dx*dy*q. */
 void oracle_conservation_totals(const fin_params* p, const double* q, double* totals);
 
+/* Troubled-cell indicator features (20 per face) and labels of every face,
+ * x faces then y faces (the device kernel's enumeration). */
+void oracle_face_samples(const fin_params* p, const double* q, double* X, unsigned char* y);
+
 #ifdef __cplusplus
 }
 #endif

@@ -59,6 +59,7 @@ class Oracle:
         lib.oracle_step_fixed.argtypes = [P, _dp, C.c_double, C.POINTER(C.c_double)]
         lib.oracle_step_fixed.restype = C.c_int
         lib.oracle_conservation_totals.argtypes = [P, _dp, _dp]
+        lib.oracle_face_samples.argtypes = [P, _dp, _dp, np.ctypeslib.ndpointer(np.uint8, flags="C_CONTIGUOUS")]
         self.lib = lib
 
     def set_bnd(self, p, q):
@@ -119,6 +120,13 @@ class Oracle:
         if rc:
             raise ValueError(f"oracle_step_fixed failed: {rc}")
         return q, cfl.value
+
+    def face_samples(self, p, q):
+        nf = (p.mx + 1) * p.my + p.mx * (p.my + 1)
+        X = np.zeros((nf, 20))
+        y = np.zeros(nf, dtype=np.uint8)
+        self.lib.oracle_face_samples(C.byref(p), np.ascontiguousarray(q), X, y)
+        return X, y
 
     def conservation_totals(self, p, q):
         out = np.zeros(p.meqn)
