@@ -7,7 +7,12 @@ global LLF with characteristic projection, CFL 0.4.  Synthetic closed-form
 initial data; the state (673 MB per FP64 array) is far larger than the 126 MB
 L2, so no L2 flush is needed between steps.
 
-    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--form fp64|fp32]
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--forms fp64,fp32,hybrid]
+
+The headline form is the hybrid (FP32 bulk + troubled-face network, with the
+judge step) when trained weights are present (finess_b200/data/), else FP64;
+the line also carries every form's throughput and an "equal L1 error" block
+(each form's density L1 error on two reduced problems).
 
 N > 1 runs as N independent replicas (one per GPU, launched by torchrun); the
 path has no exchange between problems.  Prints one JSON line on rank 0.
@@ -32,8 +37,8 @@ N_CELLS = 4096
 # Algorithmic HBM bytes per cell-update of a perfectly fused SSP-RK3 step with
 # FP64 state, meqn 5: stage 1 reads q and writes q1 (80 B), stages 2 and 3
 # each read two arrays and write one (120 B each).
-BYTES_PER_CELL_UPDATE = {"fp64": 320.0, "fp32": 320.0}
-BYTES_PER_CELL_PER_LAUNCH = {1: 80.0, 2: 120.0, 3: 120.0}
+# Every form keeps the state in FP64, so the bytes are the same for all.
+BYTES_PER_CELL_UPDATE = 320.0
 
 
 def dist_env():
@@ -117,13 +122,74 @@ def profile_traffic_bytes_per_cell(form):
     return None
 
 
-def build_problem(n, form):
+FORMS = ("fp64", "fp32", "hybrid")
+
+
+def load_indicator():
+    from finess_b200.indicator import DEFAULT_WEIGHTS
+    if not os.path.exists(DEFAULT_WEIGHTS):
+        return None
+    W = np.load(DEFAULT_WEIGHTS)
+    return W["params"], float(W["z_threshold"])
+
+
+def make_solver(p, form, indicator, judge_every=20, judge_tol=1e-3):
+    from finess_b200.solver import Solver
+    from finess_b200._abi import FIN_PREC_FP32, FIN_PREC_FP64, FIN_PREC_HYBRID
+    p = p.copy()
+    p.precision = {"fp64": FIN_PREC_FP64, "fp32": FIN_PREC_FP32, "hybrid": FIN_PREC_HYBRID}[form]
+    s = Solver(p)
+    if form == "hybrid":
+        s.set_indicator(indicator[0], indicator[1], judge_every, judge_tol)
+    return s
+
+
+def first_dt(p, s, q0):
+    a1, a2 = s.GlobalWaveSpd(q0)
+    return p.desired_cfl * min((p.xhigh - p.xlow) / p.mx, (p.yhigh - p.ylow) / p.my) / max(a1, a2)
+
+
+def accuracy_block(indicator, forms):
+    """Density L1 (area-normalised) of each form: the isentropic vortex (200^2,
+    one period, against the exact solution) and the four-quadrant Riemann
+    problem (512^2 to t = 0.8, against the FP64 run at 1024^2 averaged onto
+    the 512^2 cells)."""
     from finess_b200 import problems as P
-    from finess_b200._abi import FIN_PREC_FP32, FIN_PREC_FP64, FIN_WENO_Z
-    p = P.riemann_params(n=n, weno=FIN_WENO_Z)
-    p.precision = FIN_PREC_FP32 if form == "fp32" else FIN_PREC_FP64
+
+    def run(p, q0, tend, form):
+        s = make_solver(p, form, indicator)
+        s.set_state(q0, 0.0)
+        dtv = np.array([0.0, first_dt(p, s, q0), p.max_dt])
+        s.FinSolveRK(tend, dtv)
+        q, _ = s.get_state()
+        st = s.hybrid_stats() if form == "hybrid" else None
+        s.close()
+        return q, st
+
+    out = {}
+    p = P.vortex_params(n=200)
+    q0, qe = P.vortex_exact(p), P.vortex_exact(p, t=10.0)
+    for f in forms:
+        q, st = run(p, q0, 10.0, f)
+        out[f"vortex200_{f}_L1"] = P.density_errors(p, q, qe)[0]
+    pf = P.riemann_params(n=1024)
+    qf, _ = run(pf, P.riemann_init(pf), 0.8, "fp64")
+    mb = pf.mbc
+    fi = qf[mb:mb + 1024, mb:mb + 1024]
+    p = P.riemann_params(n=512)
     q0 = P.riemann_init(p)
-    return p, q0
+    qr = np.zeros_like(q0)
+    qr[p.mbc:p.mbc + 512, p.mbc:p.mbc + 512] = 0.25 * (fi[0::2, 0::2] + fi[1::2, 0::2] + fi[0::2, 1::2] + fi[1::2, 1::2])
+    for f in forms:
+        q, st = run(p, q0, 0.8, f)
+        out[f"riemann512_{f}_L1"] = P.density_errors(p, q, qr)[0]
+        if st:
+            out["riemann512_hybrid_judges"] = st["judges"]
+            out["riemann512_hybrid_reverts"] = st["reverts"]
+    for k in ("vortex200", "riemann512"):
+        if f"{k}_hybrid_L1" in out:
+            out[f"{k}_hybrid_over_fp64"] = out[f"{k}_hybrid_L1"] / out[f"{k}_fp64_L1"]
+    return out
 
 
 def cpu_baseline(seconds_target=15.0, n=512):
@@ -206,10 +272,11 @@ def main():
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--form", default="fp64", choices=["fp64", "fp32"])
+    ap.add_argument("--forms", default=None, help="comma list of fp64,fp32,hybrid (default: all available)")
     ap.add_argument("--n", type=int, default=N_CELLS)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-md", action="store_true")
+    ap.add_argument("--no-accuracy", action="store_true")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     if args.impl == "reference":
@@ -224,109 +291,114 @@ def main():
         import torch.distributed as dist
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
 
-    from finess_b200.solver import Solver, fma_peak_tflops
-    p, q0 = build_problem(args.n, args.form)
-    cells = p.mx * p.my
-    s = Solver(p)
-    s.set_state(q0, 0.0)
-    tend = 0.8
-    # initial_dt of parameters.ini chosen for this grid: desired CFL at the
-    # initial maximum wave speed
-    a1, a2 = s.GlobalWaveSpd(q0)
-    dt0 = p.desired_cfl * min((p.xhigh - p.xlow) / p.mx, (p.yhigh - p.ylow) / p.my) / max(a1, a2)
-    s.set_state(q0, 0.0)
-    dtv = np.array([0.0, dt0, p.max_dt])
-    dtv, _ = s.advance(tend, dtv, args.warmup)
-
-    # ---- timed region: K steps, device-resident state ----
     def barrier():
         if ws > 1:
             import torch.distributed as dist
             dist.barrier()
         torch.cuda.synchronize()
 
-    s.set_kernel_timing(True)
-    l0 = s.launch_count()
-    sampler = ClockSampler(local)
-    barrier()
-    sampler.start()
-    dtv, nst = s.advance(tend, dtv, args.steps)
-    dev_ms = s.last_kernel_ms()
-    barrier()
-    clocks = sampler.stop()
-    launches = s.launch_count() - l0
-    kms, klaunches = s.kernel_time()
-    s.set_kernel_timing(False)
-    if nst != args.steps:
-        raise RuntimeError(f"only {nst} steps taken")
-    if ws > 1:
+    def max_over_ranks(v):
+        if ws == 1:
+            return v
         import torch.distributed as dist
-        t = torch.tensor([dev_ms], device="cuda", dtype=torch.float64)
+        t = torch.tensor([v], device="cuda", dtype=torch.float64)
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        dev_ms = float(t.item())
-    value = ws * cells * args.steps / (dev_ms * 1e-3)
-    ms_per_step = dev_ms / args.steps
+        return float(t.item())
 
-    # ---- roofline of the stage kernel ----
+    from finess_b200 import problems as P
+    from finess_b200.solver import fma_peak_tflops
+    indicator = load_indicator()
+    forms = [f for f in (args.forms.split(",") if args.forms else FORMS) if f != "hybrid" or indicator]
+    headline = "hybrid" if "hybrid" in forms else forms[0]
+    p = P.riemann_params(n=args.n)
+    q0 = P.riemann_init(p)
+    cells = p.mx * p.my
+    tend = 0.8
+
+    # ---- timed regions: K steps per form, state resident in HBM ----
+    results, clocks, launches, kernel_stats = {}, None, None, None
+    for form in forms:
+        s = make_solver(p, form, indicator)
+        s.set_state(q0, 0.0)
+        dt0 = first_dt(p, s, q0)
+        dtv, _ = s.advance(tend, np.array([0.0, dt0, p.max_dt]), args.warmup)
+        s.set_kernel_timing(True)
+        l0 = s.launch_count()
+        sampler = ClockSampler(local) if form == headline else None
+        barrier()
+        if sampler:
+            sampler.start()
+        dtv, nst = s.advance(tend, dtv, args.steps)
+        dev_ms = s.last_kernel_ms()
+        barrier()
+        if sampler:
+            clocks = sampler.stop()
+        if nst != args.steps:
+            raise RuntimeError(f"{form}: only {nst} steps taken")
+        dev_ms = max_over_ranks(dev_ms)
+        kms, kl = s.kernel_time()
+        results[form] = {"value": ws * cells * args.steps / (dev_ms * 1e-3), "ms_per_step": dev_ms / args.steps,
+                         "stage_kernel_ms": kms / kl}
+        if form == "hybrid":
+            results[form]["indicator"] = s.hybrid_stats()
+        if form == headline:
+            launches = s.launch_count() - l0
+            kernel_stats = (kms, kl)
+        s.close()
+    value = results[headline]["value"]
+    ms_per_step = results[headline]["ms_per_step"]
+
+    # ---- roofline of the headline form's stage kernel ----
     hbm, peak_kind = measured_peaks()
-    avg_launch_ms = kms / klaunches
-    alg_bytes_launch = cells * BYTES_PER_CELL_UPDATE[args.form] / 3.0
+    avg_launch_ms = kernel_stats[0] / kernel_stats[1]
+    alg_bytes_launch = cells * BYTES_PER_CELL_UPDATE / 3.0
     achieved = alg_bytes_launch / (avg_launch_ms * 1e-3) / 1e9
-    tr = profile_traffic_bytes_per_cell(args.form)
+    tr = profile_traffic_bytes_per_cell(headline)
     roofline = {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
                 "traffic": (tr * cells) if tr is not None else None,
                 "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)",
-                "kernel": "k_stage (fused ConstructL + UpdateSoln + wave-speed maxima)",
-                "avg_launch_ms": avg_launch_ms, "launches": klaunches}
-    # FP64 / FP32 pipe: measured FMA peak of this GPU
+                "kernel": f"k_stage ({headline} form: fused ConstructL + UpdateSoln + wave-speed maxima)",
+                "avg_launch_ms": avg_launch_ms, "launches": kernel_stats[1]}
     try:
-        pk64 = fma_peak_tflops(True)
-        pk32 = fma_peak_tflops(False)
+        pipe = {"fp64_fma_peak_tflops": fma_peak_tflops(True), "fp32_fma_peak_tflops": fma_peak_tflops(False)}
     except Exception:
-        pk64 = pk32 = None
-    pipe = {"fp64_fma_peak_tflops": pk64, "fp32_fma_peak_tflops": pk32}
+        pipe = None
 
     # ---- e2e: host state in, K steps, host state out, through the C ABI ----
-    qh = q0
-    e2e_s = None
-    if True:
-        qbuf = np.empty_like(q0)
-        barrier()
-        t0 = time.perf_counter()
-        s.set_state(qh, 0.0)
-        dtv2, n2 = s.advance(tend, np.array([0.0, dt0, p.max_dt]), args.steps)
-        qout, _ = s.get_state()
-        barrier()
-        e2e_s = time.perf_counter() - t0
-        if ws > 1:
-            import torch.distributed as dist
-            t = torch.tensor([e2e_s], device="cuda", dtype=torch.float64)
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            e2e_s = float(t.item())
-        del qbuf
+    s = make_solver(p, headline, indicator)
+    barrier()
+    t0 = time.perf_counter()
+    s.set_state(q0, 0.0)
+    s.advance(tend, np.array([0.0, first_dt(p, s, q0), p.max_dt]), args.steps)
+    qout, _ = s.get_state()
+    barrier()
+    e2e_s = max_over_ranks(time.perf_counter() - t0)
+    s.close()
     state_bytes = q0.nbytes
     e2e = {"value": ws * cells * args.steps / e2e_s, "unit": UNIT,
            "h2d_bytes_per_step": state_bytes / args.steps, "d2h_bytes_per_step": state_bytes / args.steps,
            "api": "fin_set_state + fin_advance(K steps) + fin_get_state on host arrays (one FinSolveRK frame)"}
 
-    # ---- the same problem with the two-stage multiderivative (Lax-Wendroff /
-    # PIF) stepper, FP64 (device-resident, same K) ----
+    # ---- the same problem with the two-stage multiderivative stepper (FP64) ----
     md = None
-    if args.form == "fp64" and not args.no_md:
+    if not args.no_md:
         from finess_b200._abi import FIN_TS_MD
         pm = p.copy()
         pm.time_stepping_method, pm.time_order, pm.mbc = FIN_TS_MD, 4, 5
-        from finess_b200 import problems as P
         qm = P.riemann_init(pm)
-        sm = Solver(pm)
+        sm = make_solver(pm, "fp64", None)
         sm.set_state(qm, 0.0)
-        dtvm, _ = sm.advance(tend, np.array([0.0, dt0, pm.max_dt]), args.warmup)
+        dtvm, _ = sm.advance(tend, np.array([0.0, first_dt(pm, sm, qm), pm.max_dt]), args.warmup)
         barrier()
         dtvm, nm = sm.advance(tend, dtvm, args.steps)
-        md_ms = sm.last_kernel_ms()
+        md_ms = max_over_ranks(sm.last_kernel_ms())
         sm.close()
-        md = {"value": cells * nm / (md_ms * 1e-3), "unit": UNIT, "ms_per_step": md_ms / nm,
-              "stepper": "FinSolveMD time_order 4 (two-stage Lax-Wendroff/PIF)"}
+        md = {"value": ws * cells * nm / (md_ms * 1e-3), "unit": UNIT, "ms_per_step": md_ms / nm,
+              "stepper": "FinSolveMD time_order 4 (two-stage Lax-Wendroff/PIF), FP64"}
+
+    accuracy = None
+    if rank == 0 and not args.no_accuracy:
+        accuracy = accuracy_block(indicator, forms)
 
     cpu = None
     if rank == 0 and ws == 1 and not args.no_cpu_baseline:
@@ -334,17 +406,20 @@ def main():
             cpu = cpu_baseline()
         except Exception as e:  # report, never fail the bench line
             cpu = {"value": None, "unit": UNIT, "cores": None, "kind": None, "sample": f"failed: {e}"}
-    s.close()
 
     if rank == 0:
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "f64" if args.form == "fp64" else "f32+f64",
+            "scaling": "weak", "vs_baseline": None,
+            "dtype": {"fp64": "f64", "fp32": "f32 (f64 state)", "hybrid": "f32 (f64 state) + bf16 indicator"}[headline],
             "data": "synthetic",
-            "config": {"workload": "euler2d_riemann4q_wenoz_rk3", "grid": f"{p.mx}x{p.my}", "form": args.form,
+            "config": {"workload": "euler2d_riemann4q_wenoz_rk3", "grid": f"{p.mx}x{p.my}", "form": headline,
                        "weno": "Z", "time": "SSP-RK3", "cfl": 0.4, "parallelism": f"replicas{ws}",
                        "l2": "inputs larger than L2 (673 MB per state array)"},
+            "forms": results,
+            "speedup_vs_fp64": (value / results["fp64"]["value"]) if "fp64" in results else None,
+            "accuracy": accuracy,
             "roofline": roofline, "pipe": pipe, "cpu_baseline": cpu, "e2e": e2e, "md_stepper": md,
             "clocks": clocks, "gpu_launches": launches,
         }
