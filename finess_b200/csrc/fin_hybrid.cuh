@@ -4,6 +4,7 @@
 #pragma once
 #include "fin_indicator.cuh"
 #include "fin_mlp.cuh"
+#include "fin_stage.cuh"
 
 namespace fin {
 
@@ -18,29 +19,107 @@ struct IndicatorArgs {
     unsigned char* flags;      // x faces then y faces
     unsigned int* status;
     unsigned long long* count; // troubled faces (accumulated)
+    int tma;                   // tm maps q (box (TJ+8) x (TI+6) x 5, as the stage kernel's)
+    CUtensorMap tm;
 };
 
-struct IndSmem {
-    alignas(128) mlp::Weights w;
-    alignas(128) __nv_bfloat16 Xs[mlp::TILE * mlp::KIN];
-    alignas(128) __nv_bfloat16 G1s[mlp::TILE * mlp::NH];
-    uint64_t mbar;
+namespace ind {
+
+// The network as the indicator kernel holds it: W1 with the layer-1 bias in
+// its input column NIN (the feature row carries a 1 there, so the tensor
+// core adds the BF16 bias), and W2 and w3 halved, because the kernel stores
+// 2 gelu(x) = x (1 + tanh(...)) -- one FMA after the tanh -- and a factor 2
+// is exact in BF16 and FP32.  The results equal the plain network's.
+struct IndWeights {
+    alignas(128) __nv_bfloat16 W1[mlp::NH * mlp::KIN];
+    alignas(128) __nv_bfloat16 W2[mlp::NH * mlp::NH];
+    float b2[mlp::NH], w3h[mlp::NH], b3;
+};
+
+__device__ __forceinline__ void load_ind_weights(IndWeights& w, const float* P, int tid, int nthreads)
+{
+    using namespace mlp;
+    for (int e = tid; e < NH * KIN; e += nthreads) {
+        const int o = e / KIN, i = e - o * KIN;
+        const float v = i < NIN ? P[OFF_W1 + o * NIN + i] : (i == NIN ? P[OFF_B1 + o] : 0.0f);
+        w.W1[tc::kmaj(o, i, KIN)] = __float2bfloat16_rn(v);
+    }
+    for (int e = tid; e < NH * NH; e += nthreads) {
+        const int o = e / NH, i = e - o * NH;
+        w.W2[tc::kmaj(o, i, NH)] = __float2bfloat16_rn(0.5f * bf16r(P[OFF_W2 + o * NH + i]));
+    }
+    for (int e = tid; e < NH; e += nthreads) {
+        w.b2[e] = P[OFF_B2 + e];
+        w.w3h[e] = 0.5f * bf16r(P[OFF_W3 + e]);
+    }
+    if (tid == 0) w.b3 = P[OFF_B3];
+}
+
+// 2 gelu(x) in the tanh form (the constants of mlp::gelu).
+__device__ __forceinline__ float gelu2(float x)
+{
+    return fmaf(x, mlp::tanh_approx(x * fmaf(mlp::GK1, x * x, mlp::GK0)), x);
+}
+
+// D (TMEM columns at tmem_d) = A (128 x 32, K-major) * B (32 x 32, K-major)^T,
+// issued by one thread, no commit.
+__device__ __forceinline__ void mma_128x32x32(uint32_t tmem_d, const __nv_bfloat16* A, const __nv_bfloat16* B)
+{
+    constexpr uint32_t idesc = tc::idesc_bf16(128, mlp::NH);
+    const uint32_t a0 = tc::smem_addr(A), b0 = tc::smem_addr(B);
+#pragma unroll
+    for (int kk = 0; kk < 2; kk++) {
+        const uint64_t ad = tc::smem_desc(a0 + kk * 256, 128, (mlp::KIN / 8) * 128);
+        const uint64_t bd = tc::smem_desc(b0 + kk * 256, 128, (mlp::KIN / 8) * 128);
+        tc::mma_bf16(tmem_d, ad, bd, idesc, kk > 0 ? 1u : 0u);
+    }
+}
+
+}  // namespace ind
+
+// Shared memory of the indicator kernel for the stage kernel's tile shape.
+// The four 128-row feature matrices X are overwritten by the layer-1
+// activations once the layer-1 products have completed.
+template <class Cfg>
+struct IndTile {
+    ind::IndWeights w;
+    alignas(128) __nv_bfloat16 X[4 * 128 * mlp::KIN];
+    alignas(128) double stg[MEQN * Cfg::RI * Cfg::SJ];
+    float qs[MEQN * Cfg::RI * Cfg::RJ];
+    uint64_t mbar_tma, mbar_mma;
     uint32_t tmem;
     int abort;
     unsigned int cnt;
 };
 
-// One flag per face of the state a.q: 128 faces per tile, one per thread.
-__global__ void __launch_bounds__(mlp::TILE) k_indicator(const IndicatorArgs a)
+// One flag per face of the state a.q.  Persistent CTAs walk the stage
+// kernel's TI x TJ cell tiles; per tile the CTA owns the x faces of rows
+// i0 .. i0+TI-1 and the y faces of columns j0 .. j0+TJ-1 (the last tile row /
+// column also the domain's last face row / column): at most 511 faces, laid
+// out as four 128-row matrices (slots 0..255 x faces (fi, fj) = (s / 16,
+// s % 16), slots 256..510 y faces (fi, fj) = ((s-256) / 17, (s-256) % 17)).
+//   1. q's tile + halo: TMA (prefetched during the previous tile) or remap
+//      loads, FP64 -> FP32 in shared memory;
+//   2. each thread: the features of its two slots from shared memory;
+//   3. layer 1 on tcgen05 (4 x two K=16 steps into TMEM columns 0..127);
+//   4. 2 gelu, BF16, back into the X matrices; layer 2 into the same columns;
+//   5. 2 gelu + b2 -> output layer in FP32 -> flag.
+// TMEM lane quarter q = warp % 4 holds rows 32q .. 32q+31 of every matrix;
+// warps 0-3 take matrices 0 and 1, warps 4-7 matrices 2 and 3.
+template <class Cfg>
+__global__ void __launch_bounds__(Cfg::NT, 3) k_indicator(const __grid_constant__ IndicatorArgs a)
 {
     using namespace mlp;
+    constexpr int TI = Cfg::TI, TJ = Cfg::TJ, H = Cfg::H, RI = Cfg::RI, RJ = Cfg::RJ, PQ = RI * RJ;
+    static_assert(Cfg::NT == 256 && (TI + 1) * TJ <= 256 && TI * (TJ + 1) <= 255 && TJ == 16, "face slots");
     extern __shared__ __align__(128) unsigned char smem_raw[];
-    IndSmem& S = *reinterpret_cast<IndSmem*>(smem_raw);
-    const int tid = threadIdx.x, warp = tid >> 5;
-    load_weights(S.w, a.P, tid, TILE);
-    if (warp == 0) tc::tmem_alloc(&S.tmem, 64);
+    IndTile<Cfg>& S = *reinterpret_cast<IndTile<Cfg>*>(smem_raw);
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    ind::load_ind_weights(S.w, a.P, tid, Cfg::NT);
+    if (warp == 0) tc::tmem_alloc(&S.tmem, 128);
     if (tid == 0) {
-        tc::mbar_init(&S.mbar, 1);
+        tc::mbar_init(&S.mbar_tma, 1);
+        tc::mbar_init(&S.mbar_mma, 1);
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
         S.abort = 0;
         S.cnt = 0;
@@ -49,61 +128,144 @@ __global__ void __launch_bounds__(mlp::TILE) k_indicator(const IndicatorArgs a)
     __syncthreads();
     tc::fence_after_sync();
     const uint32_t tmem = S.tmem;
-    const uint32_t lane_base = uint32_t(warp * 32) << 16;
-    uint32_t phase = 0;
-    const long long nf = (long long)(a.mx + 1) * a.my + (long long)a.mx * (a.my + 1);
-    const long long ntiles = (nf + TILE - 1) / TILE;
-    for (long long t = blockIdx.x; t < ntiles; t += gridDim.x) {
-        const long long f = t * TILE + tid;
-        float x[ind::NFEAT];
-        if (f < nf) {
-            bool isx;
-            int i, j;
-            ind::face_of(f, a.mx, a.my, isx, i, j);
-            ind::face_features<float>(a.q, a.plane, a.mx, a.my, a.bc, a.gamma, isx, i, j, x);
-        } else {
-#pragma unroll
-            for (int k = 0; k < ind::NFEAT; k++) x[k] = 0.0f;
+    const uint32_t lane_base = uint32_t((warp & 3) * 32) << 16;
+    const int mx = a.mx, my = a.my;
+    const int ntj = (my + TJ - 1) / TJ;
+    const long long ntiles = (long long)((mx + TI - 1) / TI) * ntj;
+    const long long nxf = (long long)(mx + 1) * my;
+    const bool aligned = (tc::smem_addr(S.stg) & 127u) == 0;
+    if (a.tma && !aligned && tid == 0) atomicOr(a.status, 16u);
+    uint32_t tma_phase = 0, mma_phase = 0;
+    // TMA of tile t's box into stg when the tile qualifies (one thread issues)
+    auto issue = [&](long long t) -> bool {
+        const int ti0 = int(t / ntj) * TI, tj0 = int(t % ntj) * TJ;
+        if (!(a.tma && aligned && tma_interior<Cfg>(ti0, tj0, mx, my))) return false;
+        if (tid == 0) {
+            tc::mbar_expect_tx(&S.mbar_tma, uint32_t(Cfg::STG_BYTES));
+            tc::tma_load_3d(S.stg, &a.tm, tj0 - 4, ti0 - H, 0, &S.mbar_tma);
         }
-#pragma unroll
-        for (int k = 0; k < KIN; k++) S.Xs[tc::kmaj(tid, k, KIN)] = __float2bfloat16_rn(k < NIN ? x[k] : 0.0f);
-        tc::fence_smem_to_async();
+        return true;
+    };
+    bool pending = (long long)blockIdx.x < ntiles ? issue(blockIdx.x) : false;
+    for (long long t = blockIdx.x; t < ntiles; t += gridDim.x) {
+        const int i0 = int(t / ntj) * TI, j0 = int(t % ntj) * TJ;
+        // ---- 1. stage the tile ----
+        if (pending) {
+            if (!tc::mbar_wait(&S.mbar_tma, tma_phase, 1u << 24)) {
+                atomicOr(a.status, 8u);
+                tc::mbar_wait(&S.mbar_tma, tma_phase, 1u << 24);
+                S.abort = 1;
+            }
+            tma_phase ^= 1;
+        } else {
+            stage_remap<Cfg>(S.stg, a.q, a.plane, i0, j0, mx, my, a.bc, tid);
+            __syncthreads();
+        }
+        stage_convert<Cfg, float>(S.stg, S.qs, tid);
+        tc::fence_smem_to_async();     // the reads of stg precede the next TMA write into it
         __syncthreads();
-        if (tid == 0) gemm_tile_k32(tmem, S.Xs, S.w.W1, &S.mbar);
-        if (!tc::mbar_wait(&S.mbar, phase)) S.abort = 1;
-        phase ^= 1;
-        tc::fence_after_sync();
-        float h[32];
-        tc::tmem_ld32(tmem + lane_base, h);
+        if (S.abort) { pending = false; break; }
+        pending = t + gridDim.x < ntiles ? issue(t + gridDim.x) : false;
+        // ---- 2. features of the thread's two slots ----
+        long long gface[2];
+#pragma unroll 1
+        for (int h = 0; h < 2; h++) {
+            const int mt = 2 * (warp >> 2) + h, row = 32 * (warp & 3) + lane, sl = 128 * mt + row;
+            float xr[KIN];
 #pragma unroll
-        for (int o = 0; o < NH; o++) S.G1s[tc::kmaj(tid, o, NH)] = __float2bfloat16_rn(gelu(h[o] + S.w.b1[o]));
+            for (int k = 0; k < KIN; k++) xr[k] = 0.0f;
+            gface[h] = -1;
+            bool isx = sl < 256;
+            int fi, fj;
+            if (isx) { fi = sl >> 4; fj = sl & 15; }
+            else { const int v = sl - 256; fi = v / (TJ + 1); fj = v - fi * (TJ + 1); }
+            const int gi = i0 + fi, gj = j0 + fj;
+            bool own;
+            if (isx) own = gj < my && gi <= mx && (fi < TI || gi == mx);
+            else own = sl < 511 && gi < mx && gj <= my && (fj < TJ || gj == my);
+            if (own) {
+                gface[h] = isx ? (long long)gi * my + gj : nxf + (long long)gi * (my + 1) + gj;
+                const int cn = isx ? 1 : 2, ct = isx ? 2 : 1;
+                const int base = isx ? (H + fi - 3) * RJ + (H + fj) : (H + fi) * RJ + (H + fj - 3);
+                const int str = isx ? RJ : 1;
+                float Q[6][MEQN];
+#pragma unroll
+                for (int st = 0; st < 6; st++) {
+                    const int o = base + st * str;
+                    Q[st][0] = S.qs[o];
+                    Q[st][1] = S.qs[cn * PQ + o];
+                    Q[st][2] = S.qs[ct * PQ + o];
+                    Q[st][3] = S.qs[3 * PQ + o];
+                    Q[st][4] = S.qs[4 * PQ + o];
+                }
+                ind::stencil_features<float>(Q, a.gamma, xr);
+                xr[NIN] = 1.0f;   // the layer-1 bias input
+            }
+            store_row32(S.X + mt * 128 * KIN, row, xr);
+        }
+        tc::fence_smem_to_async();
+        tc::fence_before_sync();
+        __syncthreads();
+        // ---- 3. layer 1 ----
+        if (tid == 0) {
+            tc::fence_after_sync();
+#pragma unroll
+            for (int mt = 0; mt < 4; mt++) ind::mma_128x32x32(tmem + 32 * mt, S.X + mt * 128 * KIN, S.w.W1);
+            tc::commit(&S.mbar_mma);
+        }
+        if (!tc::mbar_wait(&S.mbar_mma, mma_phase)) S.abort = 1;
+        mma_phase ^= 1;
+        tc::fence_after_sync();
+        // ---- 4. 2 gelu of layer 1 into the X matrices; layer 2 ----
+#pragma unroll 1
+        for (int h = 0; h < 2; h++) {
+            const int mt = 2 * (warp >> 2) + h, row = 32 * (warp & 3) + lane;
+            float v[32];
+            tc::tmem_ld32(tmem + lane_base + 32 * mt, v);
+#pragma unroll
+            for (int o = 0; o < NH; o++) v[o] = ind::gelu2(v[o]);
+            store_row32(S.X + mt * 128 * KIN, row, v);
+        }
         tc::fence_smem_to_async();
         tc::fence_before_sync();
         __syncthreads();
         if (S.abort) break;
-        if (tid == 0) gemm_tile_k32(tmem + 32, S.G1s, S.w.W2, &S.mbar);
-        if (!tc::mbar_wait(&S.mbar, phase)) S.abort = 1;
-        phase ^= 1;
-        tc::fence_after_sync();
-        tc::tmem_ld32(tmem + lane_base + 32, h);
-        float zz = S.w.b3;
+        if (tid == 0) {
+            tc::fence_after_sync();
 #pragma unroll
-        for (int o = 0; o < NH; o++) zz += S.w.w3[o] * bf16r(gelu(h[o] + S.w.b2[o]));
-        if (f < nf) {
-            const unsigned char fl = zz > a.zthr ? 1 : 0;
-            a.flags[f] = fl;
-            if (fl) atomicAdd(&S.cnt, 1u);
+            for (int mt = 0; mt < 4; mt++) ind::mma_128x32x32(tmem + 32 * mt, S.X + mt * 128 * KIN, S.w.W2);
+            tc::commit(&S.mbar_mma);
+        }
+        if (!tc::mbar_wait(&S.mbar_mma, mma_phase)) S.abort = 1;
+        mma_phase ^= 1;
+        tc::fence_after_sync();
+        // ---- 5. output layer and flags ----
+#pragma unroll 1
+        for (int h = 0; h < 2; h++) {
+            const int mt = 2 * (warp >> 2) + h;
+            float v[32];
+            tc::tmem_ld32(tmem + lane_base + 32 * mt, v);
+            float zz = S.w.b3;
+#pragma unroll
+            for (int o = 0; o < NH; o++) zz = fmaf(S.w.w3h[o], ind::gelu2(v[o] + S.w.b2[o]), zz);
+            const bool fl = gface[h] >= 0 && zz > a.zthr;
+            if (gface[h] >= 0) a.flags[gface[h]] = fl ? 1 : 0;
+            const unsigned bal = __ballot_sync(0xffffffffu, fl);
+            if (lane == 0 && bal) atomicAdd(&S.cnt, unsigned(__popc(bal)));
         }
         tc::fence_before_sync();
         __syncthreads();
         if (S.abort) break;
     }
+    // a copy still in flight lands before the shared memory is released
+    if (pending && !tc::mbar_wait(&S.mbar_tma, tma_phase, 1u << 24)) atomicOr(a.status, 8u);
     __syncthreads();
     if (tid == 0) {
         if (S.abort) atomicOr(a.status, 4u);
         atomicAdd(a.count, (unsigned long long)S.cnt);
     }
-    if (warp == 0) tc::tmem_free(tmem, 64);
+    tc::fence_after_sync();
+    if (warp == 0) tc::tmem_free(tmem, 128);
 }
 
 // Training samples: features and labels of faces f0, f0 + stride, ...

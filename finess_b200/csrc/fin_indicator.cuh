@@ -48,22 +48,11 @@ __device__ __forceinline__ size_t stencil_cell(bool isx, int i, int j, int s, in
     return size_t(bc_remap(ci, mx, bc[0], bc[1])) * my + bc_remap(cj, my, bc[2], bc[3]);
 }
 
-// Features of one face in arithmetic R from the state planes q.
+// Features of one face in arithmetic R from its 6-point stencil Q[s][m]
+// (normal frame: rho, m_n, m_t, m_w, E).
 template <class R>
-__device__ __forceinline__ void face_features(const double* q, size_t plane, int mx, int my, const int* bc, R gamma,
-                                              bool isx, int i, int j, float* x)
+__device__ __forceinline__ void stencil_features(const R (&Q)[6][MEQN], R gamma, float* x)
 {
-    const int cn = isx ? 1 : 2, ct = isx ? 2 : 1;
-    R Q[6][MEQN];
-#pragma unroll
-    for (int s = 0; s < 6; s++) {
-        const size_t c = stencil_cell(isx, i, j, s, mx, my, bc);
-        Q[s][0] = R(q[c]);
-        Q[s][1] = R(q[cn * plane + c]);
-        Q[s][2] = R(q[ct * plane + c]);
-        Q[s][3] = R(q[3 * plane + c]);
-        Q[s][4] = R(q[4 * plane + c]);
-    }
     R Qa[MEQN];
 #pragma unroll
     for (int m = 0; m < MEQN; m++) Qa[m] = R(0.5) * (Q[3][m] + Q[2][m]);
@@ -91,6 +80,25 @@ __device__ __forceinline__ void face_features(const double* q, size_t plane, int
 #pragma unroll
         for (int s = 0; s < 5; s++) x[k * 5 + s] = float(d[s] * inv);
     }
+}
+
+// Features of one face in arithmetic R from the state planes q.
+template <class R>
+__device__ __forceinline__ void face_features(const double* q, size_t plane, int mx, int my, const int* bc, R gamma,
+                                              bool isx, int i, int j, float* x)
+{
+    const int cn = isx ? 1 : 2, ct = isx ? 2 : 1;
+    R Q[6][MEQN];
+#pragma unroll
+    for (int s = 0; s < 6; s++) {
+        const size_t c = stencil_cell(isx, i, j, s, mx, my, bc);
+        Q[s][0] = R(__ldg(q + c));
+        Q[s][1] = R(__ldg(q + cn * plane + c));
+        Q[s][2] = R(__ldg(q + ct * plane + c));
+        Q[s][3] = R(__ldg(q + 3 * plane + c));
+        Q[s][4] = R(__ldg(q + 4 * plane + c));
+    }
+    stencil_features<R>(Q, gamma, x);
 }
 
 // WENO5-JS weights departure of one 5-point stencil: max_j |w_j - d_j| / d_j.

@@ -116,7 +116,7 @@ template <int MODE, int TI, int TJ>
 __global__ void __launch_bounds__(TI * TJ) k_intflux(const IntFluxArgs a)
 {
     constexpr int HB = 2, BI = TI + 2 * HB, BJ = TJ + 2 * HB, PB = BI * BJ;
-    extern __shared__ __align__(16) unsigned char smem_raw[];
+    extern __shared__ __align__(128) unsigned char smem_raw[];
     double* qb = reinterpret_cast<double*>(smem_raw);   // [5][BI][BJ]
     double* fb = qb + MEQN * PB;                       // [5][BI][BJ]  f
     double* gb = fb + MEQN * PB;                       // [5][BI][BJ]  g

@@ -67,11 +67,10 @@ __global__ void __launch_bounds__(TILE) k_mlp_forward(const float* X, long long 
     const long long ntiles = (n + TILE - 1) / TILE;
     for (long long t = blockIdx.x; t < ntiles; t += gridDim.x) {
         const long long row = t * TILE + tid;
+        float xr[KIN];
 #pragma unroll
-        for (int k = 0; k < KIN; k++) {
-            const float x = (row < n && k < NIN) ? X[row * NIN + k] : 0.0f;
-            S.Xs[tc::kmaj(tid, k, KIN)] = __float2bfloat16_rn(x);
-        }
+        for (int k = 0; k < KIN; k++) xr[k] = (row < n && k < NIN) ? X[row * NIN + k] : 0.0f;
+        store_row32(S.Xs, tid, xr);
         tc::fence_smem_to_async();
         __syncthreads();
         if (tid == 0) gemm_tile_k32(tmem, S.Xs, S.w.W1, &S.mbar);
@@ -81,7 +80,8 @@ __global__ void __launch_bounds__(TILE) k_mlp_forward(const float* X, long long 
         float h[32];
         tc::tmem_ld32(tmem + lane_base, h);
 #pragma unroll
-        for (int o = 0; o < NH; o++) S.G1s[tc::kmaj(tid, o, NH)] = __float2bfloat16_rn(gelu(h[o] + S.w.b1[o]));
+        for (int o = 0; o < NH; o++) h[o] = gelu(h[o] + S.w.b1[o]);
+        store_row32(S.G1s, tid, h);
         tc::fence_smem_to_async();
         tc::fence_before_sync();
         __syncthreads();
@@ -93,7 +93,7 @@ __global__ void __launch_bounds__(TILE) k_mlp_forward(const float* X, long long 
         tc::tmem_ld32(tmem + lane_base + 32, h);
         float zz = S.w.b3;
 #pragma unroll
-        for (int o = 0; o < NH; o++) zz += S.w.w3[o] * bf16r(gelu(h[o] + S.w.b2[o]));
+        for (int o = 0; o < NH; o++) zz += S.w.w3[o] * gelu(h[o] + S.w.b2[o]);
         if (row < n) z[row] = zz;
         tc::fence_before_sync();
         __syncthreads();
@@ -190,7 +190,7 @@ __global__ void __launch_bounds__(TILE) k_mlp_train(const float* X, const unsign
 #pragma unroll
     for (int o = 0; o < NH; o++) {
         a2[o] += S.w.b2[o];
-        g[o] = bf16r(gelu(a2[o]));
+        g[o] = gelu(a2[o]);
         zz += S.w.w3[o] * g[o];
     }
     // ---- loss: weighted binary cross-entropy on the logit, mean over the batch ----

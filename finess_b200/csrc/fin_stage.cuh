@@ -29,6 +29,7 @@
 // next-stage wave speed -> block max -> one atomicMax per block.
 #pragma once
 #include "fin_device.cuh"
+#include "fin_tc.cuh"
 
 namespace fin {
 
@@ -48,7 +49,8 @@ struct StageArgs {
     double* smax_out;         // [2] max face speed over GetCFL's faces; nullptr = skip
     double* face_alpha_x;     // optional per-face alpha, (mx+1)*my, face-major i then j
     double* face_alpha_y;     // optional per-face alpha, mx*(my+1)
-    unsigned int* status;     // bit 0: non-finite speed, bit 1: negative p or rho
+    unsigned int* status;     // bit 0: non-finite speed, bit 1: negative p or rho, bit 3: TMA wait ran out,
+                              // bit 4: misaligned TMA destination (remap path taken)
     int bc[4];                // xlow, xhigh, ylow, yhigh
     // Lax-Wendroff / multiderivative stages (ConstructLxWL): the split fluxes
     // are the time-integrated F, G (ghosted (mx+6) x (my+6) planes) instead of
@@ -61,6 +63,13 @@ struct StageArgs {
     // 3 x 3 window of same-direction faces around it is set, else the linear
     // FD5 weights (lib/WenoReconstruct.cpp:580-616).
     const unsigned char* flags;
+    // Hybrid form on grids whose row pitch suits TMA (my even): tensor maps
+    // of q_in (box (TJ+8) x (TI+6) x 5, the tile with its halo) and of the
+    // stage operand that is not q_in (box TJ x TI x 5); tiles clear of the
+    // domain boundary stage both with one TMA transaction each.
+    int tma;
+    CUtensorMap tm_in;
+    CUtensorMap tm_A;
 };
 
 template <int TI_, int TJ_, int NT_>
@@ -79,7 +88,94 @@ struct TileCfg {
     }
     template <class R>
     __host__ __device__ static constexpr size_t smem_bytes() { return red_offset<R>() + 4 * (NT / 32) * sizeof(double); }
+    // Hybrid form, after the reduction scratch: the troubled-face count, the
+    // list of troubled faces (work-list indices), and the flag windows the
+    // 3 x 3 dilation reads: x faces rows i0-1 .. i0+TI+1, cols j0-1 .. j0+TJ;
+    // y faces rows i0-1 .. i0+TI, cols j0-1 .. j0+TJ+1.
+    static constexpr int FXR = TI + 3, FXC = TJ + 2, FYR = TI + 2, FYC = TJ + 3;
+    __host__ __device__ static constexpr size_t hyb_bytes()
+    {
+        return (4 + 2 * size_t(NFX + NFY) + size_t(FXR) * FXC + size_t(FYR) * FYC + 15) / 16 * 16;
+    }
+    // Hybrid form, 128-byte aligned after that: the FP64 staging tile of q_in
+    // (rows i0-3 .. i0+TI+2, columns j0-4 .. j0+TJ+3, so the TMA box starts
+    // on a 16-byte boundary), the FP64 tile of the other stage operand, and
+    // the mbarrier of the two copies.
+    // A TMA destination must start on a 128-byte boundary, so each buffer is
+    // padded to a multiple of 128 bytes.
+    static constexpr int SJ = TJ + 8;
+    static constexpr size_t STG_BYTES = size_t(MEQN) * RI * SJ * 8;
+    static constexpr size_t ABUF_BYTES = size_t(MEQN) * TI * TJ * 8;
+    __host__ __device__ static constexpr size_t pad128(size_t b) { return (b + 127) / 128 * 128; }
+    template <class R>
+    __host__ __device__ static constexpr size_t stg_offset() { return pad128(smem_bytes<R>() + hyb_bytes()); }
+    template <class R>
+    __host__ __device__ static constexpr size_t abuf_offset() { return stg_offset<R>() + pad128(STG_BYTES); }
+    template <class R>
+    __host__ __device__ static constexpr size_t mbar_offset() { return abuf_offset<R>() + pad128(ABUF_BYTES); }
+    template <class R>
+    __host__ __device__ static constexpr size_t hyb_smem_bytes() { return mbar_offset<R>() + 16; }
 };
+
+// Staging of q_in's tile + 3-cell halo (the cross region: rows i0-3 ..
+// i0+TI+2 at columns j0 .. j0+TJ-1, columns j0-3 .. j0+TJ+2 at rows i0 ..
+// i0+TI-1) as FP64 in stg [M][RI][SJ], column jj of the tile frame at jj+1.
+// A tile whose box (rows i0-3 .. i0+TI+2, columns j0-4 .. j0+TJ+3) lies in
+// the domain is staged by one TMA copy; any other by loads through the
+// boundary remap.
+template <class Cfg>
+__device__ __forceinline__ bool tma_interior(int i0, int j0, int mx, int my)
+{
+    return i0 >= Cfg::H && i0 + Cfg::TI + Cfg::H <= mx && j0 >= 4 && j0 + Cfg::TJ + 4 <= my;
+}
+
+template <class Cfg>
+__device__ __forceinline__ void stage_remap(double* stg, const double* q, size_t plane, int i0, int j0, int mx, int my,
+                                            const int* bc, int tid)
+{
+    constexpr int H = Cfg::H, TI = Cfg::TI, TJ = Cfg::TJ, RI = Cfg::RI, RJ = Cfg::RJ;
+    for (int e = tid; e < RI * RJ; e += Cfg::NT) {
+        const int ii = e / RJ, jj = e - ii * RJ;
+        const bool xin = ii >= H && ii < H + TI, yin = jj >= H && jj < H + TJ;
+        if (!xin && !yin) continue;
+        const int gi = bc_remap(i0 + ii - H, mx, bc[0], bc[1]);
+        const int gj = bc_remap(j0 + jj - H, my, bc[2], bc[3]);
+        const size_t g = size_t(gi) * my + gj;
+#pragma unroll
+        for (int m = 0; m < MEQN; m++) stg[(m * RI + ii) * Cfg::SJ + jj + 1] = __ldg(q + m * plane + g);
+    }
+}
+
+template <class Cfg, class R>
+__device__ __forceinline__ void stage_convert(const double* stg, R* qs, int tid)
+{
+    constexpr int H = Cfg::H, TI = Cfg::TI, TJ = Cfg::TJ, RI = Cfg::RI, RJ = Cfg::RJ;
+    for (int e = tid; e < RI * RJ; e += Cfg::NT) {
+        const int ii = e / RJ, jj = e - ii * RJ;
+        const bool xin = ii >= H && ii < H + TI, yin = jj >= H && jj < H + TJ;
+        if (!xin && !yin) continue;
+#pragma unroll
+        for (int m = 0; m < MEQN; m++) qs[m * RI * RJ + e] = R(stg[(m * RI + ii) * Cfg::SJ + jj + 1]);
+    }
+}
+
+// 6-point flux of a face that takes the linear FD5 weights: with v+- =
+// 0.5 f +- l q, the reference's characteristic form R FD5(L v+) + R FD5'(L v-)
+// (ConstructL.cpp:179-250 with WenoReconstruct_FD5, WenoReconstruct.cpp:
+// 580-616) equals FD5(v+) + FD5'(v-) component by component, because the
+// reconstruction is linear and R L = I.  FD5 has the weights (2, -13, 47, 27,
+// -3)/60 on points 0..4 and FD5' the same on points 5..1, so the face flux is
+//   (1/30) [ (f0+f5) - 8 (f1+f4) + 37 (f2+f3)                      (0.5 f terms)
+//          + l ((q0-q5) - 5 (q1-q4) + 10 (q2-q3)) ]                  (l = lah)
+// with f the half fluxes held in shared memory: 12 operations per component
+// instead of a projection, two reconstructions and a back projection.
+template <class R>
+__device__ __forceinline__ R linear_face(const R* f, int fstr, const R* q, int qstr, R lah)
+{
+    const R sf = fma(R(37), f[-1 * fstr] + f[0], fma(R(-8), f[-2 * fstr] + f[fstr], f[-3 * fstr] + f[2 * fstr]));
+    const R sq = fma(R(10), q[-1 * qstr] - q[0], fma(R(-5), q[-2 * qstr] - q[qstr], q[-3 * qstr] - q[2 * qstr]));
+    return fma(lah, sq, sf) * R(1.0 / 30.0);
+}
 
 // Resident blocks per SM the register budget is sized for: FP64 faces need
 // about 110 registers a thread, FP32 about 70.
@@ -92,8 +188,15 @@ struct TileCfg {
 #ifndef FIN_MINB_F32
 #define FIN_MINB_F32 3
 #endif
-template <class R> struct MinBlocks { static constexpr int value = FIN_MINB_F64; };
-template <> struct MinBlocks<float> { static constexpr int value = FIN_MINB_F32; };
+// The hybrid form's faces are mostly the 12-operation linear flux; its full
+// WENO pass runs on few faces, so it trades registers (spills there) for
+// resident blocks.
+#ifndef FIN_MINB_HYB
+#define FIN_MINB_HYB 3
+#endif
+template <class R, bool HYB = false> struct MinBlocks { static constexpr int value = FIN_MINB_F64; };
+template <> struct MinBlocks<float, false> { static constexpr int value = FIN_MINB_F32; };
+template <> struct MinBlocks<float, true> { static constexpr int value = FIN_MINB_HYB; };
 
 // Scalar parameters read from kernel-parameter space where they are used
 // (keeps them out of the register budget of the face loop).
@@ -155,12 +258,12 @@ __device__ __forceinline__ void right_add(const typename Euler::Eig<R>& e, int k
 }
 
 template <class R, int VER, bool P2, class Cfg, bool FG = false, bool HYB = false>
-__global__ void __launch_bounds__(Cfg::NT, MinBlocks<R>::value) k_stage(const StageArgs a)
+__global__ void __launch_bounds__(Cfg::NT, MinBlocks<R, HYB>::value) k_stage(const __grid_constant__ StageArgs a)
 {
     constexpr int TI = Cfg::TI, TJ = Cfg::TJ, NT = Cfg::NT, H = Cfg::H;
     constexpr int RI = Cfg::RI, RJ = Cfg::RJ;
     constexpr int PQ = RI * RJ;                    // plane size of qs and prim
-    extern __shared__ __align__(16) unsigned char smem_raw[];
+    extern __shared__ __align__(128) unsigned char smem_raw[];
     R* qs = reinterpret_cast<R*>(smem_raw);        // [M][RI][RJ]
     R* fs = qs + MEQN * PQ;                        // [M][RI][TJ]   0.5 * f
     R* gs = fs + MEQN * RI * TJ;                   // [M][TI][RJ]   0.5 * g
@@ -175,15 +278,69 @@ __global__ void __launch_bounds__(Cfg::NT, MinBlocks<R>::value) k_stage(const St
 #define gamma (Par<R>::gamma(a))
 
     // ---- phase 0: load the tile + halo, boundary conditions by remap ----
-    for (int e = tid; e < PQ; e += NT) {
-        const int ii = e / RJ, jj = e - ii * RJ;
-        const bool xin = ii >= H && ii < H + TI, yin = jj >= H && jj < H + TJ;
-        if (!xin && !yin) continue;
-        const int gi = bc_remap(i0 + ii - H, mx, a.bc[0], a.bc[1]);
-        const int gj = bc_remap(j0 + jj - H, my, a.bc[2], a.bc[3]);
-        const size_t g = size_t(gi) * my + gj;
+    unsigned char* hyb = smem_raw + Cfg::template smem_bytes<R>();
+    int* ntrb = reinterpret_cast<int*>(hyb);
+    short* tlist = reinterpret_cast<short*>(hyb + 4);
+    unsigned char* fxw = hyb + 4 + 2 * (Cfg::NFX + Cfg::NFY);
+    unsigned char* fyw = fxw + Cfg::FXR * Cfg::FXC;
+    double* stg = reinterpret_cast<double*>(smem_raw + Cfg::template stg_offset<R>());    // [M][RI][SJ]
+    double* abuf = reinterpret_cast<double*>(smem_raw + Cfg::template abuf_offset<R>());  // [M][TI][TJ]
+    uint64_t* mbar = reinterpret_cast<uint64_t*>(smem_raw + Cfg::template mbar_offset<R>());
+    bool a_smem = false;
+    if (HYB) {
+        // Tiles whose halo lies inside the domain: one TMA copy of q_in's
+        // tile + halo (and one of the other stage operand's tile), issued
+        // first so they are in flight while the flags arrive.  Other tiles
+        // load with the boundary remap.  Either way q_in lands in FP64 in
+        // the staging tile, whose interior the stage update reads again.
+        // (the destinations' 128-byte alignment is checked too: a violation
+        // is reported in the status word and the tile takes the remap path)
+        const bool aligned = ((tc::smem_addr(stg) | tc::smem_addr(abuf)) & 127u) == 0;
+        if (a.tma && !aligned && tid == 0) atomicOr(a.status, 16u);
+        const bool tma_tile = a.tma && aligned && tma_interior<Cfg>(i0, j0, mx, my);
+        const double* ext = (a.A && a.A != a.qin) ? a.A : ((a.B && a.B != a.qin) ? a.B : nullptr);
+        a_smem = tma_tile && ext != nullptr;
+        if (tma_tile && tid == 0) {
+            tc::mbar_init(mbar, 1);
+            asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+            tc::mbar_expect_tx(mbar, uint32_t(Cfg::STG_BYTES + (a_smem ? Cfg::ABUF_BYTES : 0)));
+            tc::tma_load_3d(stg, &a.tm_in, j0 - 4, i0 - H, 0, mbar);
+            if (a_smem) tc::tma_load_3d(abuf, &a.tm_A, j0, i0, 0, mbar);
+        }
+        if (!tma_tile) stage_remap<Cfg>(stg, a.qin, a.plane, i0, j0, mx, my, a.bc, tid);
+        // the flag windows of the 3 x 3 dilation (faces outside the domain
+        // count as smooth)
+        const long long nxf = (long long)(mx + 1) * my;
+        for (int e = tid; e < Cfg::FXR * Cfg::FXC; e += NT) {
+            const int r = e / Cfg::FXC, c = e - r * Cfg::FXC;
+            const int a1 = i0 - 1 + r, b1 = j0 - 1 + c;
+            fxw[e] = (a1 >= 0 && a1 <= mx && b1 >= 0 && b1 < my) ? a.flags[(long long)a1 * my + b1] : 0;
+        }
+        for (int e = tid; e < Cfg::FYR * Cfg::FYC; e += NT) {
+            const int r = e / Cfg::FYC, c = e - r * Cfg::FYC;
+            const int a1 = i0 - 1 + r, b1 = j0 - 1 + c;
+            fyw[e] = (a1 >= 0 && a1 < mx && b1 >= 0 && b1 <= my) ? a.flags[nxf + (long long)a1 * (my + 1) + b1] : 0;
+        }
+        if (tid == 0) *ntrb = 0;
+        __syncthreads();
+        if (tma_tile && !tc::mbar_wait(mbar, 0, 1u << 24)) {
+            // the copy did not land in time: report it, and give it one more
+            // bounded wait before the shared memory is read or released
+            atomicOr(a.status, 8u);
+            tc::mbar_wait(mbar, 0, 1u << 24);
+        }
+        stage_convert<Cfg, R>(stg, qs, tid);
+    } else {
+        for (int e = tid; e < PQ; e += NT) {
+            const int ii = e / RJ, jj = e - ii * RJ;
+            const bool xin = ii >= H && ii < H + TI, yin = jj >= H && jj < H + TJ;
+            if (!xin && !yin) continue;
+            const int gi = bc_remap(i0 + ii - H, mx, a.bc[0], a.bc[1]);
+            const int gj = bc_remap(j0 + jj - H, my, a.bc[2], a.bc[3]);
+            const size_t g = size_t(gi) * my + gj;
 #pragma unroll
-        for (int m = 0; m < MEQN; m++) qs[m * PQ + e] = R(__ldg(a.qin + m * a.plane + g));
+            for (int m = 0; m < MEQN; m++) qs[m * PQ + e] = R(__ldg(a.qin + m * a.plane + g));
+        }
     }
     __syncthreads();
 
@@ -249,8 +406,84 @@ __global__ void __launch_bounds__(Cfg::NT, MinBlocks<R>::value) k_stage(const St
     const R ag2 = a.alpha_in ? R(a.alpha_in[1]) : R(0);
     R smax_x = R(0), smax_y = R(0);
     bool neg = false, nonfinite = false;
+    if (HYB) {
+        // Hybrid pass A, every face: the LLF speed (and the CFL / status
+        // bookkeeping), the dilated flag, and for smooth faces the linear
+        // flux.  Troubled faces go to a block-local list for pass B.
 #pragma unroll 1
-    for (int w = tid; w < Cfg::NFX + Cfg::NFY; w += NT) {
+        for (int wb = 0; wb < Cfg::NFX + Cfg::NFY; wb += NT) {
+            const int w = wb + tid;
+            bool push = false;
+            if (w < Cfg::NFX + Cfg::NFY) {
+                const bool isx = w < Cfg::NFX;
+                int fi, fj, qbase, qstr, fbase, fstr, fplane;
+                const R* fl;
+                if (isx) {
+                    fi = w / TJ; fj = w - fi * TJ;
+                    qbase = (H + fi) * RJ + (H + fj); qstr = RJ;
+                    fl = fs; fbase = (H + fi) * TJ + fj; fstr = TJ; fplane = RI * TJ;
+                } else {
+                    const int v = w - Cfg::NFX;
+                    fi = v / (TJ + 1); fj = v - fi * (TJ + 1);
+                    qbase = (H + fi) * RJ + (H + fj); qstr = 1;
+                    fl = gs; fbase = fi * RJ + (H + fj); fstr = 1; fplane = TI * RJ;
+                }
+                const int ql = qbase - qstr;
+                const int un = isx ? 0 : 1;
+                const R unl = prim[un * PQ + ql], unr = prim[un * PQ + qbase];
+                const R pl = prim[2 * PQ + ql], pr = prim[2 * PQ + qbase];
+                const R cl = prim[3 * PQ + ql], cr = prim[3 * PQ + qbase];
+                const R rho = R(0.5) * (qs[qbase] + qs[ql]);
+                const R ua = R(0.5) * (unl + unr);
+                const R pa = R(0.5) * (pl + pr);
+                const R ca = fsqrt(fabs(gamma * pa * rcp(rho)));
+                if (pa < R(0) || rho < R(0)) neg = true;
+                const R s1 = Min(unl - cl, ua - ca);
+                const R s2 = Max(unr + cr, ua + ca);
+                const R alpha = Max(isx ? ag1 : ag2, Max(fabs(s1), fabs(s2)));
+                if (!(alpha <= R(1e30))) nonfinite = true;
+                bool trb = false;
+                const unsigned char* win = isx ? fxw + fi * Cfg::FXC + fj : fyw + fi * Cfg::FYC + fj;
+                const int wc = isx ? Cfg::FXC : Cfg::FYC;
+#pragma unroll
+                for (int di = 0; di < 3; di++)
+                    trb |= (win[di * wc] | win[di * wc + 1] | win[di * wc + 2]) != 0;
+                if (isx) {
+                    const int gfi = i0 + fi, gj = j0 + fj;
+                    if (gfi < mx && gj < my && alpha <= R(1e30)) smax_x = Max(smax_x, alpha);
+                    if (a.face_alpha_x && gfi <= mx && gj < my) a.face_alpha_x[size_t(gfi) * my + gj] = double(alpha);
+                } else {
+                    const int gi = i0 + fi, gfj = j0 + fj;
+                    if (gi < mx && gfj < my && alpha <= R(1e30)) smax_y = Max(smax_y, alpha);
+                    if (a.face_alpha_y && gi < mx && gfj <= my) a.face_alpha_y[size_t(gi) * (my + 1) + gfj] = double(alpha);
+                }
+                if (trb) {
+                    push = true;
+                } else {
+                    const R lah = R(0.5) * Par<R>::ascale(a) * alpha;
+                    R* dst = isx ? Fh + fi * TJ + fj : Gh + fi * (TJ + 1) + fj;
+                    const int dplane = isx ? (TI + 1) * TJ : TI * (TJ + 1);
+#pragma unroll
+                    for (int m = 0; m < MEQN; m++)
+                        dst[m * dplane] = linear_face<R>(fl + m * fplane + fbase, fstr, qs + m * PQ + qbase, qstr, lah);
+                }
+            }
+            // warp-aggregated append to the troubled list
+            const unsigned bal = __ballot_sync(0xffffffffu, push);
+            if (bal) {
+                const int lane = tid & 31;
+                int base = 0;
+                if (lane == __ffs(bal) - 1) base = atomicAdd(ntrb, __popc(bal));
+                base = __shfl_sync(0xffffffffu, base, __ffs(bal) - 1);
+                if (push) tlist[base + __popc(bal & ((1u << lane) - 1u))] = short(w);
+            }
+        }
+        __syncthreads();
+    }
+    const int nwork = HYB ? *ntrb : Cfg::NFX + Cfg::NFY;
+#pragma unroll 1
+    for (int k = tid; k < nwork; k += NT) {
+        const int w = HYB ? int(tlist[k]) : k;
         const bool isx = w < Cfg::NFX;
         int fi, fj, qbase, qstr, fbase, fstr, fplane;
         const R* fl;
@@ -292,27 +525,6 @@ __global__ void __launch_bounds__(Cfg::NT, MinBlocks<R>::value) k_stage(const St
             alpha = Max(isx ? ag1 : ag2, Max(fabs(s1), fabs(s2)));
         }
         if (!(alpha <= R(1e30))) nonfinite = true;
-        bool trb = true;
-        if (HYB) {
-            trb = false;
-            const long long nxf = (long long)(mx + 1) * my;
-            if (isx) {
-                const int gfi = i0 + fi, gj = j0 + fj;
-                for (int di = -1; di <= 1; di++)
-                    for (int dj = -1; dj <= 1; dj++) {
-                        const int a1 = gfi + di, b1 = gj + dj;
-                        if (a1 >= 0 && a1 <= mx && b1 >= 0 && b1 < my) trb |= a.flags[(long long)a1 * my + b1] != 0;
-                    }
-            } else {
-                const int gi = i0 + fi, gfj = j0 + fj;
-                for (int di = -1; di <= 1; di++)
-                    for (int dj = -1; dj <= 1; dj++) {
-                        const int a1 = gi + di, b1 = gfj + dj;
-                        if (a1 >= 0 && a1 < mx && b1 >= 0 && b1 <= my)
-                            trb |= a.flags[nxf + (long long)a1 * (my + 1) + b1] != 0;
-                    }
-            }
-        }
         // gp = 0.5 (L f + l_alpha L q) = L (0.5 f + 0.5 l_alpha q), points
         // 0..4; gm the same with -l_alpha, points 5..1 (ConstructL.cpp:179-185).
         const R lah = R(0.5) * Par<R>::ascale(a) * alpha;
@@ -349,7 +561,7 @@ __global__ void __launch_bounds__(Cfg::NT, MinBlocks<R>::value) k_stage(const St
                     up[t] = k == 0 ? p0[t] : p4[t];
                     um[t] = k == 0 ? m0[t] : m4[t];
                 }
-                right_add<R>(ev, k == 0 ? 0 : 4, (trb ? weno_pair<R, VER, P2>(up, um, eps, pw) : weno_pair<R, FIN_WENO_FD, true>(up, um, eps, pw)), fh);
+                right_add<R>(ev, k == 0 ? 0 : 4, weno_pair<R, VER, P2>(up, um, eps, pw), fh);
             }
         }
         {
@@ -373,7 +585,7 @@ __global__ void __launch_bounds__(Cfg::NT, MinBlocks<R>::value) k_stage(const St
                     m1[5 - s] = Euler::left1(ev, rw, v);
                 }
             }
-            right_add<R>(ev, 1, (trb ? weno_pair<R, VER, P2>(p1, m1, eps, pw) : weno_pair<R, FIN_WENO_FD, true>(p1, m1, eps, pw)), fh);
+            right_add<R>(ev, 1, weno_pair<R, VER, P2>(p1, m1, eps, pw), fh);
         }
         {
             // pass 3: fields 2 and 3 (rows v_t - u2 v0 and v_w - u3 v0)
@@ -405,7 +617,7 @@ __global__ void __launch_bounds__(Cfg::NT, MinBlocks<R>::value) k_stage(const St
                     up[t] = k == 0 ? p2[t] : p3[t];
                     um[t] = k == 0 ? m2[t] : m3[t];
                 }
-                right_add<R>(ev, k == 0 ? 2 : 3, (trb ? weno_pair<R, VER, P2>(up, um, eps, pw) : weno_pair<R, FIN_WENO_FD, true>(up, um, eps, pw)), fh);
+                right_add<R>(ev, k == 0 ? 2 : 3, weno_pair<R, VER, P2>(up, um, eps, pw), fh);
             }
         }
         // Back to (rho, rho u, rho v, rho w, E) and store.
@@ -449,17 +661,27 @@ __global__ void __launch_bounds__(Cfg::NT, MinBlocks<R>::value) k_stage(const St
             double L = -(f1 - f0) * a.rdx;
             L = L - (g1 - g0) * a.rdy;
             double v = 0.0;
-            if (a.A) v = a.a1 * a.A[m * a.plane + g];
-            if (a.B) v = v + a.a2 * a.B[m * a.plane + g];
+            if (HYB) {
+                // stage operands from shared memory where they were staged
+                const double qin_c = stg[(m * RI + H + ci) * Cfg::SJ + H + cj + 1];
+                if (a.A) v = a.a1 * (a.A == a.qin ? qin_c : (a_smem ? abuf[(m * TI + ci) * TJ + cj] : a.A[m * a.plane + g]));
+                if (a.B) v = v + a.a2 * (a.B == a.qin ? qin_c : (a_smem ? abuf[(m * TI + ci) * TJ + cj] : a.B[m * a.plane + g]));
+            } else {
+                if (a.A) v = a.a1 * a.A[m * a.plane + g];
+                if (a.B) v = v + a.a2 * a.B[m * a.plane + g];
+            }
             v = v + a.bdt * L;
             qn[m] = v;
             a.qout[m * a.plane + g] = v;
         }
         if (a.alpha_out) {
             // GlobalWaveSpd.cpp:71-76 on the new state, both directions.
-            const double qy[MEQN] = {qn[0], qn[2], qn[1], qn[3], qn[4]};
-            const double sx = Euler::cell_speed(Euler::cell(gam, qn));
-            const double sy = Euler::cell_speed(Euler::cell(gam, qy));
+            // The FP32 forms use it only as the FP32 LLF speed of the next
+            // stage, so they evaluate it in FP32.
+            const R qx[MEQN] = {R(qn[0]), R(qn[1]), R(qn[2]), R(qn[3]), R(qn[4])};
+            const R qy[MEQN] = {qx[0], qx[2], qx[1], qx[3], qx[4]};
+            const double sx = double(Euler::cell_speed(Euler::cell(R(gam), qx)));
+            const double sy = double(Euler::cell_speed(Euler::cell(R(gam), qy)));
             if (!(sx <= 1e300) || !(sy <= 1e300)) nonfinite = true;
             if (sx <= 1e300) cs_x = Max(cs_x, sx);
             if (sy <= 1e300) cs_y = Max(cs_y, sy);

@@ -14,6 +14,7 @@
 // Every wait is bounded: a kernel that runs out of iterations records it in
 // a status word and returns without further tensor-core work.
 #pragma once
+#include <cuda.h>
 #include <cuda_runtime.h>
 #include <cuda_bf16.h>
 #include <stdint.h>
@@ -95,6 +96,25 @@ __device__ __forceinline__ bool mbar_wait(uint64_t* mbar, uint32_t parity, uint3
         if (done) return true;
     }
     return false;
+}
+
+// The issuing thread arrives on the mbarrier and announces the bytes the
+// tensor copies of this phase will deliver.
+__device__ __forceinline__ void mbar_expect_tx(uint64_t* mbar, uint32_t bytes)
+{
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" : : "r"(smem_addr(mbar)), "r"(bytes) : "memory");
+}
+
+// Tiled TMA load of a 3D box (x fastest) of the tensor behind the map into
+// shared memory, completion counted on mbar.  x times the element size must
+// be a multiple of 16 bytes (the caller guarantees it).  No multicast.
+__device__ __forceinline__ void tma_load_3d(void* dst, const CUtensorMap* map, int x, int y, int z, uint64_t* mbar)
+{
+    asm volatile(
+        "cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4}], [%5];"
+        :
+        : "r"(smem_addr(dst)), "l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(y), "r"(z), "r"(smem_addr(mbar))
+        : "memory");
 }
 
 // TMEM allocation by one full warp: writes the base address into *dst.

@@ -47,9 +47,46 @@ int set_err(int code, const std::string& msg)
 #endif
 using Cfg = TileCfg<FIN_TILE_TI, FIN_TILE_TJ, FIN_TILE_NT>;
 
+// cuTensorMapEncodeTiled through the runtime's driver entry point (no link
+// dependency on libcuda).
+typedef CUresult (*EncodeTiledFn)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
+                                  const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
+                                  CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+EncodeTiledFn encode_tiled()
+{
+    static EncodeTiledFn fn = nullptr;
+    static bool tried = false;
+    if (!tried) {
+        tried = true;
+        void* p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPointByVersion("cuTensorMapEncodeTiled", &p, 12000, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = reinterpret_cast<EncodeTiledFn>(p);
+    }
+    return fn;
+}
+
+// Map of one state buffer as a 3D FP64 tensor (j, i, component): row pitch
+// my*8 bytes, component pitch plane*8 bytes (both multiples of 16 when my is
+// even), box box_j x box_i x 5.
+bool make_state_map(CUtensorMap* m, double* base, int mx, int my, size_t plane, int box_j, int box_i)
+{
+    EncodeTiledFn fn = encode_tiled();
+    if (!fn || (my & 1)) return false;
+    const cuuint64_t dims[3] = {cuuint64_t(my), cuuint64_t(mx), cuuint64_t(MEQN)};
+    const cuuint64_t strides[2] = {cuuint64_t(my) * 8, cuuint64_t(plane) * 8};
+    const cuuint32_t box[3] = {cuuint32_t(box_j), cuuint32_t(box_i), cuuint32_t(MEQN)};
+    const cuuint32_t es[3] = {1, 1, 1};
+    return fn(m, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 3, base, dims, strides, box, es, CU_TENSOR_MAP_INTERLEAVE_NONE,
+              CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) ==
+           CUDA_SUCCESS;
+}
+
 // Reduction slots (doubles) in one device block, reset by one memset per step.
 // The status word (bit 0: non-finite speed or state, bit 1: negative p or rho,
-// bit 2: a tensor-core wait ran out) sits in slot STATUS so one copy returns it
+// bit 2: a tensor-core wait ran out, bit 3: a TMA copy wait ran out, bit 4: a TMA
+// destination was misaligned) sits in slot STATUS so one copy returns it
 // with the maxima.  SMAX_ALT keeps the face-speed maxima of the hybrid attempt
 // while a judge step recomputes with full WENO; DIFF receives the judge's
 // max |q_hybrid - q_full| and max |q_full|.
@@ -96,6 +133,11 @@ struct fin_solver {
     bool alpha_valid;       // slots hold alpha of q[cur]
     double last_ms;
     long long launches;
+    // TMA tensor maps of the state buffers for the hybrid stages (tile with
+    // halo / interior tile boxes); tma_ok when all were encoded
+    CUtensorMap tm_q[NBUF];
+    CUtensorMap tm_a[NBUF];
+    bool tma_ok;
 };
 
 // ---------------------------------------------------------------------------
@@ -206,10 +248,17 @@ __global__ void k_fma_peak(R* out, int iters, R a, R b)
 // ---------------------------------------------------------------------------
 namespace {
 
+int buffer_of(const fin_solver* s, const double* ptr)
+{
+    for (int b = 0; b < NBUF; b++)
+        if (ptr && s->q[b] == ptr) return b;
+    return -1;
+}
+
 template <class R, int VER, bool P2, bool FG = false, bool HYB = false>
 int launch_stage_t(fin_solver* s, const StageArgs& a)
 {
-    const size_t smem = Cfg::smem_bytes<R>();
+    const size_t smem = HYB ? Cfg::template hyb_smem_bytes<R>() : Cfg::template smem_bytes<R>();
     auto kern = k_stage<R, VER, P2, Cfg, FG, HYB>;
     static bool configured = false;   // per instantiation; attribute is per device function
     if (!configured) {
@@ -217,7 +266,21 @@ int launch_stage_t(fin_solver* s, const StageArgs& a)
         configured = true;
     }
     dim3 grid((a.my + Cfg::TJ - 1) / Cfg::TJ, (a.mx + Cfg::TI - 1) / Cfg::TI);
-    kern<<<grid, Cfg::NT, smem, s->stream>>>(a);
+    if (HYB) {
+        // the tensor maps of q_in and of the operand that is not q_in
+        StageArgs b = a;
+        b.tma = 0;
+        const double* ext = (a.A && a.A != a.qin) ? a.A : ((a.B && a.B != a.qin) ? a.B : nullptr);
+        const int iq = buffer_of(s, a.qin), ie = buffer_of(s, ext);
+        if (s->tma_ok && iq >= 0 && (!ext || ie >= 0)) {
+            b.tma = 1;
+            b.tm_in = s->tm_q[iq];
+            if (ext) b.tm_A = s->tm_a[ie];
+        }
+        kern<<<grid, Cfg::NT, smem, s->stream>>>(b);
+    } else {
+        kern<<<grid, Cfg::NT, smem, s->stream>>>(a);
+    }
     s->launches++;
     CK(cudaGetLastError());
     return FIN_OK;
@@ -401,17 +464,22 @@ int launch_indicator(fin_solver* s, int buf)
     ia.flags = s->flags;
     ia.status = s->status;
     ia.count = s->ind_count;
+    ia.tma = 0;
+    if (s->tma_ok) {
+        ia.tma = 1;
+        ia.tm = s->tm_q[buf];
+    }
     static bool configured = false;
-    const size_t smem = std::max(sizeof(IndSmem), size_t(29 * 1024));   // <= 8 CTAs per SM: TMEM never waits
+    const size_t smem = sizeof(IndTile<Cfg>);
     if (!configured) {
-        CK(cudaFuncSetAttribute(k_indicator, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
+        CK(cudaFuncSetAttribute(k_indicator<Cfg>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
         configured = true;
     }
     CK(cudaMemsetAsync(s->ind_count, 0, sizeof(unsigned long long), s->stream));
     const long long nf = (long long)(s->p.mx + 1) * s->p.my + (long long)s->p.mx * (s->p.my + 1);
-    const long long tiles = (nf + mlp::TILE - 1) / mlp::TILE;
-    const int grid = int(std::min<long long>(tiles, 148 * 8));
-    k_indicator<<<grid, mlp::TILE, smem, s->stream>>>(ia);
+    const long long tiles = (long long)((s->p.mx + Cfg::TI - 1) / Cfg::TI) * ((s->p.my + Cfg::TJ - 1) / Cfg::TJ);
+    const int grid = int(std::min<long long>(tiles, 148 * 3));
+    k_indicator<Cfg><<<grid, Cfg::NT, smem, s->stream>>>(ia);
     s->launches++;
     s->faces = nf;
     CK(cudaGetLastError());
@@ -591,6 +659,8 @@ int get_cfl(fin_solver* s, double dt, double dtmax, double* cfl, bool* nonfinite
     unsigned int st;
     memcpy(&st, s->h_slots + SLOT_STATUS, sizeof(st));
     *nonfinite = (st & 1u) != 0;
+    if (st & 12u) return set_err(FIN_ERR_CUDA, "a bounded device wait (tensor-core or TMA copy) ran out");
+    if (st & 16u) return set_err(FIN_ERR_CUDA, "a TMA destination in shared memory was not 128-byte aligned");
     if (dt > dtmax) return set_err(FIN_ERR_DT_BOUNDS, "dt is out of bounds");
     double c = -100.0;
     c = Max(dt * s->h_slots[SLOT_SMAX] / s->dx, c);
@@ -714,6 +784,11 @@ int fin_create(const fin_params* p, fin_solver** out)
         s->zthr = 0.0f;
         s->judge_every = 20;
         s->judge_tol = 1e-3;
+        bool ok = true;
+        for (int b = 0; b < nbuf && ok; b++)
+            ok = make_state_map(&s->tm_q[b], s->q[b], p->mx, p->my, s->plane, Cfg::SJ, Cfg::RI) &&
+                 make_state_map(&s->tm_a[b], s->q[b], p->mx, p->my, s->plane, Cfg::TJ, Cfg::TI);
+        s->tma_ok = ok;
     }
     if (p->time_stepping_method != FIN_TS_RK) {
         s->gplane = (size_t(p->mx + 6) * (p->my + 6) + 31) / 32 * 32;

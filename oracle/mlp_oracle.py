@@ -4,15 +4,15 @@ kernels of finess_b200/csrc/fin_mlp.cu.
 
 Two forms:
 * ``forward_emulated`` / ``grads_emulated`` round to BF16 exactly where the
-  device does (inputs, hidden activations, weights, back-propagated
-  activation gradients), so they should agree with the device to FP32
-  accumulation error;
+  device does (inputs, the layer-1 activations, the weights and the layer-1
+  bias, back-propagated activation gradients; the layer-2 activations enter
+  the FP32 output layer unrounded), so they agree with the device to FP32
+  accumulation error and the hardware tanh approximation;
 * ``forward_exact`` / ``grads_exact`` have no rounding, for finite-difference
   checks of the back-propagation itself.
 Parameter layout: W1[32][20], b1[32], W2[32][32], b2[32], w3[32], b3.
 """
 import numpy as np
-from scipy.special import erf
 
 NIN, NH = 20, 32
 OFF_W1 = 0
@@ -43,22 +43,29 @@ def unpack(P):
     return W1, b1, W2, b2, w3, b3
 
 
+# GELU in its tanh form (Hendrycks & Gimpel, arXiv:1606.08415, eq. for the
+# tanh approximation): gelu(x) = x/2 (1 + tanh(k0 x + k1 x^3)).
+GK0 = np.sqrt(2.0 / np.pi)
+GK1 = GK0 * 0.044715
+
+
 def gelu(x):
-    return 0.5 * x * (1.0 + erf(x / np.sqrt(2.0)))
+    return 0.5 * x * (1.0 + np.tanh(x * (GK0 + GK1 * x * x)))
 
 
 def gelu_grad(x):
-    return 0.5 * (1.0 + erf(x / np.sqrt(2.0))) + x * np.exp(-0.5 * x * x) / np.sqrt(2.0 * np.pi)
+    t = np.tanh(x * (GK0 + GK1 * x * x))
+    return 0.5 * (1.0 + t) + 0.5 * x * (1.0 - t * t) * (GK0 + 3.0 * GK1 * x * x)
 
 
 def _forward(P, X, rnd):
     W1, b1, W2, b2, w3, b3 = unpack(P)
     r = bf16 if rnd else (lambda v: np.asarray(v, dtype=np.float64))
     xb = r(X)
-    a1 = xb @ r(W1).T + b1
+    a1 = xb @ r(W1).T + r(b1)
     g1 = r(gelu(a1))
     a2 = g1 @ r(W2).T + b2
-    g2 = r(gelu(a2))
+    g2 = gelu(a2)
     z = g2 @ r(w3) + b3
     return xb, a1, g1, a2, g2, z
 

@@ -81,3 +81,56 @@ def test_hybrid_with_nothing_flagged_is_linear_fd5_and_judge_reverts():
         a.step_fixed(5e-4)
         st = a.hybrid_stats()
     assert st["troubled_faces"] == 0 and st["judges"] == 1 and st["reverts"] == 1
+
+
+def test_hybrid_smooth_faces_equal_reference_fd5(oracle):
+    """With nothing flagged every face takes the component-wise 6-point form of
+    the linear FD5 flux.  The reference's FD5 path projects onto characteristic
+    fields, reconstructs and projects back; the two agree because the
+    reconstruction is linear and R L = I, so one hybrid step must match the
+    oracle's FP64 weno_version=FD step to FP32 rounding."""
+    from finess_b200.solver import Solver
+    import mlp_oracle as M
+    from finess_b200._abi import FIN_WENO_FD
+    Pm = np.zeros(M.NPARAM, dtype=np.float32)
+    Pm[M.OFF_B3] = -10.0
+    p = P.vortex_params(n=48, weno=FIN_WENO_JS)
+    q = oracle.set_bnd(p, P.vortex_exact(p))
+    ph = p.copy(); ph.precision = FIN_PREC_HYBRID
+    dt = 0.02
+    with Solver(ph) as a:
+        a.set_indicator(Pm, 0.0, judge_every=0)
+        a.set_state(q)
+        a.step_fixed(dt)
+        qa, _ = a.get_state()
+        assert a.hybrid_stats()["troubled_faces"] == 0
+    po = p.copy(); po.weno_version = FIN_WENO_FD
+    qo, _ = oracle.step_fixed(po, q, dt)
+    err = rel_linf(interior(p, qa), interior(p, qo))
+    assert err <= 1e-6, err
+
+
+@pytest.mark.parametrize("case", [0, 2])
+def test_indicator_flags_match_oracle_network(oracle, case):
+    """The device indicator (features + network on tensor cores + threshold)
+    flags the same number of faces as the oracle network applied to the
+    oracle's FP64 features, up to faces within rounding of the threshold."""
+    from finess_b200.indicator import DEFAULT_WEIGHTS
+    from finess_b200.solver import Solver
+    import mlp_oracle as M
+    W = np.load(DEFAULT_WEIGHTS)
+    params, zthr = W["params"], float(W["z_threshold"])
+    p, q = _cases()[case]
+    q = oracle.set_bnd(p, q)
+    Xo, _ = oracle.face_samples(p, q)
+    zo = M.forward_emulated(params, Xo)
+    n_oracle = int(np.sum(zo > zthr))
+    near = int(np.sum(np.abs(zo - zthr) < 0.05))
+    ph = p.copy(); ph.precision = FIN_PREC_HYBRID
+    with Solver(ph) as a:
+        a.set_indicator(params, zthr, judge_every=0)
+        a.set_state(q)
+        a.step_fixed(1e-5)
+        st = a.hybrid_stats()
+    assert st["faces"] == len(Xo)
+    assert abs(st["troubled_faces"] - n_oracle) <= max(near, 2), (st, n_oracle, near)
