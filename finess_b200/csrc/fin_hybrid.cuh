@@ -16,7 +16,7 @@ struct IndicatorArgs {
     float gamma;
     const float* P;            // network parameters (FP32, mlp::NPARAM)
     float zthr;                // a face is troubled when its logit exceeds zthr
-    unsigned char* flags;      // x faces then y faces
+    unsigned* flags;           // bit masks (flag_wx / flag_wy layout), zeroed before the launch
     unsigned int* status;
     unsigned long long* count; // troubled faces (accumulated)
     int tma;                   // tm maps q (box (TJ+8) x (TI+6) x 5, as the stage kernel's)
@@ -132,7 +132,6 @@ __global__ void __launch_bounds__(Cfg::NT, 3) k_indicator(const __grid_constant_
     const int mx = a.mx, my = a.my;
     const int ntj = (my + TJ - 1) / TJ;
     const long long ntiles = (long long)((mx + TI - 1) / TI) * ntj;
-    const long long nxf = (long long)(mx + 1) * my;
     const bool aligned = (tc::smem_addr(S.stg) & 127u) == 0;
     if (a.tma && !aligned && tid == 0) atomicOr(a.status, 16u);
     uint32_t tma_phase = 0, mma_phase = 0;
@@ -167,14 +166,17 @@ __global__ void __launch_bounds__(Cfg::NT, 3) k_indicator(const __grid_constant_
         if (S.abort) { pending = false; break; }
         pending = t + gridDim.x < ntiles ? issue(t + gridDim.x) : false;
         // ---- 2. features of the thread's two slots ----
-        long long gface[2];
+        long long fword[2];   // flag word of the slot's face (-1: not owned)
+        unsigned fbit[2];
+        const int wx = flag_wx(my), wy = flag_wy(my);
 #pragma unroll 1
         for (int h = 0; h < 2; h++) {
             const int mt = 2 * (warp >> 2) + h, row = 32 * (warp & 3) + lane, sl = 128 * mt + row;
             float xr[KIN];
 #pragma unroll
             for (int k = 0; k < KIN; k++) xr[k] = 0.0f;
-            gface[h] = -1;
+            fword[h] = -1;
+            fbit[h] = 0;
             bool isx = sl < 256;
             int fi, fj;
             if (isx) { fi = sl >> 4; fj = sl & 15; }
@@ -184,7 +186,8 @@ __global__ void __launch_bounds__(Cfg::NT, 3) k_indicator(const __grid_constant_
             if (isx) own = gj < my && gi <= mx && (fi < TI || gi == mx);
             else own = sl < 511 && gi < mx && gj <= my && (fj < TJ || gj == my);
             if (own) {
-                gface[h] = isx ? (long long)gi * my + gj : nxf + (long long)gi * (my + 1) + gj;
+                fword[h] = isx ? (long long)gi * wx + (gj >> 5) : (long long)(mx + 1) * wx + (long long)gi * wy + (gj >> 5);
+                fbit[h] = 1u << (gj & 31);
                 const int cn = isx ? 1 : 2, ct = isx ? 2 : 1;
                 const int base = isx ? (H + fi - 3) * RJ + (H + fj) : (H + fi) * RJ + (H + fj - 3);
                 const int str = isx ? RJ : 1;
@@ -248,8 +251,8 @@ __global__ void __launch_bounds__(Cfg::NT, 3) k_indicator(const __grid_constant_
             float zz = S.w.b3;
 #pragma unroll
             for (int o = 0; o < NH; o++) zz = fmaf(S.w.w3h[o], ind::gelu2(v[o] + S.w.b2[o]), zz);
-            const bool fl = gface[h] >= 0 && zz > a.zthr;
-            if (gface[h] >= 0) a.flags[gface[h]] = fl ? 1 : 0;
+            const bool fl = fword[h] >= 0 && zz > a.zthr;
+            if (fl) atomicOr(a.flags + fword[h], fbit[h]);
             const unsigned bal = __ballot_sync(0xffffffffu, fl);
             if (lane == 0 && bal) atomicAdd(&S.cnt, unsigned(__popc(bal)));
         }

@@ -17,6 +17,7 @@
 // on load by the boundary remap (no ghost writes, no BC pass).
 //
 // Per block, shared memory holds (R = double or float):
+//   prim [4][TI+6][TJ+6]  u, v, p, c of the cells
 //   qs  [M][TI+6][TJ+6]   stage input with a 3-cell halo (corners unused)
 //   fs  [M][TI+6][TJ]     x flux f at the x-stencil cells
 //   gs  [M][TI][TJ+6]     y flux g at the y-stencil cells
@@ -58,11 +59,11 @@ struct StageArgs {
     const double* Fg;
     const double* Gg;
     size_t gplane;
-    // Hybrid form: troubled-face flags of the step (x faces then y faces, as
-    // written by the indicator).  A face takes full WENO when any flag in the
-    // 3 x 3 window of same-direction faces around it is set, else the linear
-    // FD5 weights (lib/WenoReconstruct.cpp:580-616).
-    const unsigned char* flags;
+    // Hybrid form: troubled-face flags of the step as bit masks (layout of
+    // flag_wx / flag_wy below, written by the indicator).  A face takes full
+    // WENO when any flag in the 3 x 3 window of same-direction faces around
+    // it is set, else the linear FD5 weights (lib/WenoReconstruct.cpp:580-616).
+    const unsigned* flags;
     // Hybrid form on grids whose row pitch suits TMA (my even): tensor maps
     // of q_in (box (TJ+8) x (TI+6) x 5, the tile with its halo) and of the
     // stage operand that is not q_in (box TJ x TI x 5); tiles clear of the
@@ -71,6 +72,22 @@ struct StageArgs {
     CUtensorMap tm_in;
     CUtensorMap tm_A;
 };
+
+// Troubled-face flags, one bit per face: x faces (rows 0 .. mx) take
+// flag_wx words per row, bit b of word k being column 32 k + b; the y faces
+// (rows 0 .. mx-1, columns 0 .. my) follow with flag_wy words per row.
+__host__ __device__ __forceinline__ int flag_wx(int my) { return (my + 31) >> 5; }
+__host__ __device__ __forceinline__ int flag_wy(int my) { return (my + 32) >> 5; }
+__host__ __device__ __forceinline__ size_t flag_words(int mx, int my)
+{
+    return size_t(mx + 1) * flag_wx(my) + size_t(mx) * flag_wy(my);
+}
+// Bits of columns b0 .. b0+31 of one mask row from the words holding them
+// (k = b0 >> 5 and k + 1; columns outside the row read as 0).
+__device__ __forceinline__ unsigned row_bits(unsigned lo, unsigned hi, int b0)
+{
+    return unsigned(((unsigned long long)hi << 32 | lo) >> (b0 & 31));
+}
 
 template <int TI_, int TJ_, int NT_>
 struct TileCfg {
@@ -88,14 +105,16 @@ struct TileCfg {
     }
     template <class R>
     __host__ __device__ static constexpr size_t smem_bytes() { return red_offset<R>() + 4 * (NT / 32) * sizeof(double); }
-    // Hybrid form, after the reduction scratch: the troubled-face count, the
-    // list of troubled faces (work-list indices), and the flag windows the
-    // 3 x 3 dilation reads: x faces rows i0-1 .. i0+TI+1, cols j0-1 .. j0+TJ;
-    // y faces rows i0-1 .. i0+TI, cols j0-1 .. j0+TJ+1.
+    // Hybrid form, after the reduction scratch: the troubled-face count; the
+    // flag windows of the 3 x 3 dilation as one bit mask per face row (x
+    // faces: rows i0-1 .. i0+TI+1, bit c = column j0-1+c, c < TJ+2; y faces:
+    // rows i0-1 .. i0+TI, c < TJ+3), each already dilated along j; the list
+    // of troubled faces (work-list indices).
     static constexpr int FXR = TI + 3, FXC = TJ + 2, FYR = TI + 2, FYC = TJ + 3;
+    static_assert(FYC <= 32, "flag row masks are 32-bit words");
     __host__ __device__ static constexpr size_t hyb_bytes()
     {
-        return (4 + 2 * size_t(NFX + NFY) + size_t(FXR) * FXC + size_t(FYR) * FYC + 15) / 16 * 16;
+        return (4 + 4 * size_t(FXR + FYR) + 2 * size_t(NFX + NFY) + 15) / 16 * 16;
     }
     // Hybrid form, 128-byte aligned after that: the FP64 staging tile of q_in
     // (rows i0-3 .. i0+TI+2, columns j0-4 .. j0+TJ+3, so the TMA box starts
@@ -264,12 +283,16 @@ __global__ void __launch_bounds__(Cfg::NT, MinBlocks<R, HYB>::value) k_stage(con
     constexpr int RI = Cfg::RI, RJ = Cfg::RJ;
     constexpr int PQ = RI * RJ;                    // plane size of qs and prim
     extern __shared__ __align__(128) unsigned char smem_raw[];
-    R* qs = reinterpret_cast<R*>(smem_raw);        // [M][RI][RJ]
+    // prim holds u, v, p, c per cell: planes [4][RI][RJ], or in the hybrid
+    // form one 16-byte (u, v, p, c) per cell, so a face reads its two cells
+    // with two vector loads
+    R* prim = reinterpret_cast<R*>(smem_raw);      // [4][RI][RJ] | [RI][RJ][4]
+    R* qs = prim + Cfg::NPRIM * PQ;                // [M][RI][RJ]
     R* fs = qs + MEQN * PQ;                        // [M][RI][TJ]   0.5 * f
     R* gs = fs + MEQN * RI * TJ;                   // [M][TI][RJ]   0.5 * g
     R* Fh = gs + MEQN * TI * RJ;                   // [M][TI+1][TJ]
     R* Gh = Fh + MEQN * (TI + 1) * TJ;             // [M][TI][TJ+1]
-    R* prim = Gh + MEQN * TI * (TJ + 1);           // [4][RI][RJ]   u, v, p, c
+    float4* prim4 = reinterpret_cast<float4*>(smem_raw);
     double* red = reinterpret_cast<double*>(smem_raw + Cfg::template red_offset<R>());
 
     const int tid = threadIdx.x;
@@ -280,13 +303,32 @@ __global__ void __launch_bounds__(Cfg::NT, MinBlocks<R, HYB>::value) k_stage(con
     // ---- phase 0: load the tile + halo, boundary conditions by remap ----
     unsigned char* hyb = smem_raw + Cfg::template smem_bytes<R>();
     int* ntrb = reinterpret_cast<int*>(hyb);
-    short* tlist = reinterpret_cast<short*>(hyb + 4);
-    unsigned char* fxw = hyb + 4 + 2 * (Cfg::NFX + Cfg::NFY);
-    unsigned char* fyw = fxw + Cfg::FXR * Cfg::FXC;
+    unsigned* fxm = reinterpret_cast<unsigned*>(hyb + 4);     // [FXR]
+    unsigned* fym = fxm + Cfg::FXR;                          // [FYR]
+    short* tlist = reinterpret_cast<short*>(fym + Cfg::FYR);   // [NFX + NFY]
     double* stg = reinterpret_cast<double*>(smem_raw + Cfg::template stg_offset<R>());    // [M][RI][SJ]
     double* abuf = reinterpret_cast<double*>(smem_raw + Cfg::template abuf_offset<R>());  // [M][TI][TJ]
     uint64_t* mbar = reinterpret_cast<uint64_t*>(smem_raw + Cfg::template mbar_offset<R>());
     bool a_smem = false;
+    // hybrid: the mask words of the flag windows, loaded first (x rows by
+    // warp 0, y rows by warp 1) so they arrive while the tile is staged
+    unsigned fw_lo = 0, fw_hi = 0;
+    if (HYB) {
+        const int wx = flag_wx(my), wy = flag_wy(my), k = (j0 - 1) >> 5;
+        const unsigned* row = nullptr;
+        int nw = 0;
+        if (tid < Cfg::FXR) {
+            const int a1 = i0 - 1 + tid;
+            if (a1 >= 0 && a1 <= mx) { row = a.flags + size_t(a1) * wx; nw = wx; }
+        } else if (tid >= 32 && tid < 32 + Cfg::FYR) {
+            const int a1 = i0 - 1 + (tid - 32);
+            if (a1 >= 0 && a1 < mx) { row = a.flags + size_t(mx + 1) * wx + size_t(a1) * wy; nw = wy; }
+        }
+        if (row) {
+            if (k >= 0 && k < nw) fw_lo = __ldg(row + k);
+            if (k + 1 < nw) fw_hi = __ldg(row + k + 1);
+        }
+    }
     if (HYB) {
         // Tiles whose halo lies inside the domain: one TMA copy of q_in's
         // tile + halo (and one of the other stage operand's tile), issued
@@ -308,18 +350,14 @@ __global__ void __launch_bounds__(Cfg::NT, MinBlocks<R, HYB>::value) k_stage(con
             if (a_smem) tc::tma_load_3d(abuf, &a.tm_A, j0, i0, 0, mbar);
         }
         if (!tma_tile) stage_remap<Cfg>(stg, a.qin, a.plane, i0, j0, mx, my, a.bc, tid);
-        // the flag windows of the 3 x 3 dilation (faces outside the domain
-        // count as smooth)
-        const long long nxf = (long long)(mx + 1) * my;
-        for (int e = tid; e < Cfg::FXR * Cfg::FXC; e += NT) {
-            const int r = e / Cfg::FXC, c = e - r * Cfg::FXC;
-            const int a1 = i0 - 1 + r, b1 = j0 - 1 + c;
-            fxw[e] = (a1 >= 0 && a1 <= mx && b1 >= 0 && b1 < my) ? a.flags[(long long)a1 * my + b1] : 0;
-        }
-        for (int e = tid; e < Cfg::FYR * Cfg::FYC; e += NT) {
-            const int r = e / Cfg::FYC, c = e - r * Cfg::FYC;
-            const int a1 = i0 - 1 + r, b1 = j0 - 1 + c;
-            fyw[e] = (a1 >= 0 && a1 < mx && b1 >= 0 && b1 <= my) ? a.flags[nxf + (long long)a1 * (my + 1) + b1] : 0;
+        // the flag windows of the 3 x 3 dilation as row masks, dilated along
+        // j (faces outside the domain count as smooth)
+        if (tid < Cfg::FXR) {
+            const unsigned msk = row_bits(fw_lo, fw_hi, j0 - 1) & ((1u << Cfg::FXC) - 1u);
+            fxm[tid] = msk | (msk >> 1) | (msk >> 2);
+        } else if (tid >= 32 && tid < 32 + Cfg::FYR) {
+            const unsigned msk = row_bits(fw_lo, fw_hi, j0 - 1) & ((1u << Cfg::FYC) - 1u);
+            fym[tid - 32] = msk | (msk >> 1) | (msk >> 2);
         }
         if (tid == 0) *ntrb = 0;
         __syncthreads();
@@ -329,7 +367,7 @@ __global__ void __launch_bounds__(Cfg::NT, MinBlocks<R, HYB>::value) k_stage(con
             atomicOr(a.status, 8u);
             tc::mbar_wait(mbar, 0, 1u << 24);
         }
-        stage_convert<Cfg, R>(stg, qs, tid);
+        // (the FP64 -> R conversion into qs happens in phase 1, cell by cell)
     } else {
         for (int e = tid; e < PQ; e += NT) {
             const int ii = e / RJ, jj = e - ii * RJ;
@@ -341,8 +379,8 @@ __global__ void __launch_bounds__(Cfg::NT, MinBlocks<R, HYB>::value) k_stage(con
 #pragma unroll
             for (int m = 0; m < MEQN; m++) qs[m * PQ + e] = R(__ldg(a.qin + m * a.plane + g));
         }
+        __syncthreads();
     }
-    __syncthreads();
 
     // ---- phase 1: per cell of the cross region: FluxFunc (FluxFunc.cpp:19-42,
     // once per cell instead of once per stencil point of every face), halved
@@ -351,14 +389,27 @@ __global__ void __launch_bounds__(Cfg::NT, MinBlocks<R, HYB>::value) k_stage(con
         const int ii = e / RJ, jj = e - ii * RJ;
         const bool xin = ii >= H && ii < H + TI, yin = jj >= H && jj < H + TJ;
         if (!xin && !yin) continue;
-        const R rho = qs[e], m1 = qs[PQ + e], m2 = qs[2 * PQ + e], m3 = qs[3 * PQ + e], en = qs[4 * PQ + e];
+        R rho, m1, m2, m3, en;
+        if (HYB) {
+            // hybrid: the staged FP64 tile, narrowed here and kept in qs
+            const double* sp = stg + ii * Cfg::SJ + jj + 1;
+            rho = R(sp[0]); m1 = R(sp[RI * Cfg::SJ]); m2 = R(sp[2 * RI * Cfg::SJ]);
+            m3 = R(sp[3 * RI * Cfg::SJ]); en = R(sp[4 * RI * Cfg::SJ]);
+            qs[e] = rho; qs[PQ + e] = m1; qs[2 * PQ + e] = m2; qs[3 * PQ + e] = m3; qs[4 * PQ + e] = en;
+        } else {
+            rho = qs[e]; m1 = qs[PQ + e]; m2 = qs[2 * PQ + e]; m3 = qs[3 * PQ + e]; en = qs[4 * PQ + e];
+        }
         const R ir = rcp(rho);
         const R u1 = m1 * ir, u2 = m2 * ir, u3 = m3 * ir;
         const R press = (gamma - R(1)) * (en - R(0.5) * rho * (u1 * u1 + u2 * u2 + u3 * u3));
-        prim[e] = u1;
-        prim[PQ + e] = u2;
-        prim[2 * PQ + e] = press;
-        prim[3 * PQ + e] = fsqrt(fabs(gamma * press * ir));
+        if (HYB) {
+            prim4[e] = make_float4(float(u1), float(u2), float(press), float(fsqrt(fabs(gamma * press * ir))));
+        } else {
+            prim[e] = u1;
+            prim[PQ + e] = u2;
+            prim[2 * PQ + e] = press;
+            prim[3 * PQ + e] = fsqrt(fabs(gamma * press * ir));
+        }
         if (FG) {
             // 0.5 * F, 0.5 * G of the integrated-flux kernel, unremapped: it
             // covers the 3-cell ghost frame; cells of a partial tile beyond it
@@ -429,10 +480,10 @@ __global__ void __launch_bounds__(Cfg::NT, MinBlocks<R, HYB>::value) k_stage(con
                     fl = gs; fbase = fi * RJ + (H + fj); fstr = 1; fplane = TI * RJ;
                 }
                 const int ql = qbase - qstr;
-                const int un = isx ? 0 : 1;
-                const R unl = prim[un * PQ + ql], unr = prim[un * PQ + qbase];
-                const R pl = prim[2 * PQ + ql], pr = prim[2 * PQ + qbase];
-                const R cl = prim[3 * PQ + ql], cr = prim[3 * PQ + qbase];
+                const float4 PL = prim4[ql], PR = prim4[qbase];
+                const R unl = isx ? PL.x : PL.y, unr = isx ? PR.x : PR.y;
+                const R pl = PL.z, pr = PR.z;
+                const R cl = PL.w, cr = PR.w;
                 const R rho = R(0.5) * (qs[qbase] + qs[ql]);
                 const R ua = R(0.5) * (unl + unr);
                 const R pa = R(0.5) * (pl + pr);
@@ -442,12 +493,8 @@ __global__ void __launch_bounds__(Cfg::NT, MinBlocks<R, HYB>::value) k_stage(con
                 const R s2 = Max(unr + cr, ua + ca);
                 const R alpha = Max(isx ? ag1 : ag2, Max(fabs(s1), fabs(s2)));
                 if (!(alpha <= R(1e30))) nonfinite = true;
-                bool trb = false;
-                const unsigned char* win = isx ? fxw + fi * Cfg::FXC + fj : fyw + fi * Cfg::FYC + fj;
-                const int wc = isx ? Cfg::FXC : Cfg::FYC;
-#pragma unroll
-                for (int di = 0; di < 3; di++)
-                    trb |= (win[di * wc] | win[di * wc + 1] | win[di * wc + 2]) != 0;
+                const unsigned* fm = isx ? fxm : fym;
+                const bool trb = (((fm[fi] | fm[fi + 1] | fm[fi + 2]) >> fj) & 1u) != 0;
                 if (isx) {
                     const int gfi = i0 + fi, gj = j0 + fj;
                     if (gfi < mx && gj < my && alpha <= R(1e30)) smax_x = Max(smax_x, alpha);
@@ -512,9 +559,16 @@ __global__ void __launch_bounds__(Cfg::NT, MinBlocks<R, HYB>::value) k_stage(con
         R alpha;
         {
             const int un = isx ? 0 : 1;
-            const R unl = prim[un * PQ + ql], unr = prim[un * PQ + qbase];
-            const R pl = prim[2 * PQ + ql], pr = prim[2 * PQ + qbase];
-            const R cl = prim[3 * PQ + ql], cr = prim[3 * PQ + qbase];
+            R unl, unr, pl, pr, cl, cr;
+            if (HYB) {
+                const float4 PL = prim4[ql], PR = prim4[qbase];
+                unl = isx ? PL.x : PL.y; unr = isx ? PR.x : PR.y;
+                pl = PL.z; pr = PR.z; cl = PL.w; cr = PR.w;
+            } else {
+                unl = prim[un * PQ + ql]; unr = prim[un * PQ + qbase];
+                pl = prim[2 * PQ + ql]; pr = prim[2 * PQ + qbase];
+                cl = prim[3 * PQ + ql]; cr = prim[3 * PQ + qbase];
+            }
             const R rho = Qa[0];
             const R ua = R(0.5) * (unl + unr);
             const R pa = R(0.5) * (pl + pr);
@@ -656,10 +710,13 @@ __global__ void __launch_bounds__(Cfg::NT, MinBlocks<R, HYB>::value) k_stage(con
 #pragma unroll
         for (int m = 0; m < MEQN; m++) {
             // ConstructL.cpp:396-398
-            const double f1 = Fh[m * (TI + 1) * TJ + (ci + 1) * TJ + cj], f0 = Fh[m * (TI + 1) * TJ + ci * TJ + cj];
-            const double g1 = Gh[m * TI * (TJ + 1) + ci * (TJ + 1) + cj + 1], g0 = Gh[m * TI * (TJ + 1) + ci * (TJ + 1) + cj];
-            double L = -(f1 - f0) * a.rdx;
-            L = L - (g1 - g0) * a.rdy;
+            // (the FP32 forms difference their FP32 fluxes in FP32 and widen
+            // the result once)
+            const R f1 = Fh[m * (TI + 1) * TJ + (ci + 1) * TJ + cj], f0 = Fh[m * (TI + 1) * TJ + ci * TJ + cj];
+            const R g1 = Gh[m * TI * (TJ + 1) + ci * (TJ + 1) + cj + 1], g0 = Gh[m * TI * (TJ + 1) + ci * (TJ + 1) + cj];
+            R Lr = -(f1 - f0) * R(a.rdx);
+            Lr = Lr - (g1 - g0) * R(a.rdy);
+            const double L = double(Lr);
             double v = 0.0;
             if (HYB) {
                 // stage operands from shared memory where they were staged

@@ -122,7 +122,7 @@ struct fin_solver {
     double step_ms;
     // hybrid form
     float* mlpP;            // network parameters on the device
-    unsigned char* flags;   // troubled-face flags of the current step
+    unsigned* flags;        // troubled-face flag masks of the current step
     unsigned long long* ind_count;
     float zthr;
     int judge_every;
@@ -446,7 +446,7 @@ int launch_intflux(fin_solver* s, int mode, const double* q1, const double* q2, 
     return FIN_OK;
 }
 
-int take_stages_rk(fin_solver* s, double dt, int nxt, const unsigned char* flags, int q1, int q2);
+int take_stages_rk(fin_solver* s, double dt, int nxt, const unsigned* flags, int q1, int q2);
 
 // Troubled-face flags of q[buf] (fin_hybrid.cuh).
 int launch_indicator(fin_solver* s, int buf)
@@ -476,6 +476,7 @@ int launch_indicator(fin_solver* s, int buf)
         configured = true;
     }
     CK(cudaMemsetAsync(s->ind_count, 0, sizeof(unsigned long long), s->stream));
+    CK(cudaMemsetAsync(s->flags, 0, flag_words(s->p.mx, s->p.my) * sizeof(unsigned), s->stream));
     const long long nf = (long long)(s->p.mx + 1) * s->p.my + (long long)s->p.mx * (s->p.my + 1);
     const long long tiles = (long long)((s->p.mx + Cfg::TI - 1) / Cfg::TI) * ((s->p.my + Cfg::TJ - 1) / Cfg::TJ);
     const int grid = int(std::min<long long>(tiles, 148 * 3));
@@ -607,7 +608,7 @@ void settle_judge(fin_solver* s, int nxt, double dt, double* cfl)
 // The stages of one step of size dt from q[cur] into q[nxt] (RK3:
 // FinSolveRK.cpp:158-211 with SetRKinfo.cpp:50-64).  Leaves the face-speed
 // maxima of the step in slots SMAX and alpha(q[nxt]) in its slot.
-int take_stages_rk(fin_solver* s, double dt, int nxt, const unsigned char* flags, int q1, int q2)
+int take_stages_rk(fin_solver* s, double dt, int nxt, const unsigned* flags, int q1, int q2)
 {
     const fin_params& p = s->p;
     if (p.time_order != 3)
@@ -777,8 +778,8 @@ int fin_create(const fin_params* p, fin_solver** out)
     for (int b = 0; b < nbuf; b++)
         if ((e = cudaMalloc(&s->q[b], MEQN * s->plane * sizeof(double))) != cudaSuccess) return fail(e, "cudaMalloc state");
     if (p->precision == FIN_PREC_HYBRID) {
-        const size_t nf = size_t(p->mx + 1) * p->my + size_t(p->mx) * (p->my + 1);
-        if ((e = cudaMalloc(&s->flags, nf)) != cudaSuccess) return fail(e, "cudaMalloc flags");
+        if ((e = cudaMalloc(&s->flags, flag_words(p->mx, p->my) * sizeof(unsigned))) != cudaSuccess)
+            return fail(e, "cudaMalloc flags");
         if ((e = cudaMalloc(&s->ind_count, 16)) != cudaSuccess) return fail(e, "cudaMalloc counter");
         if ((e = cudaMemset(s->ind_count, 0, 16)) != cudaSuccess) return fail(e, "memset");
         s->zthr = 0.0f;
