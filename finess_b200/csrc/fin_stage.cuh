@@ -71,6 +71,7 @@ struct StageArgs {
     int tma;
     CUtensorMap tm_in;
     CUtensorMap tm_A;
+    CUtensorMap tm_qi;   // q_in with the interior-tile box (TJ x TI x 5)
 };
 
 // Troubled-face flags, one bit per face: x faces (rows 0 .. mx) take

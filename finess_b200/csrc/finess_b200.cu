@@ -16,6 +16,7 @@
 #include <algorithm>
 #include "finess_b200.h"
 #include "fin_stage.cuh"
+#include "fin_stage_hyb.cuh"
 #include "fin_intflux.cuh"
 #include "fin_hybrid.cuh"
 
@@ -314,17 +315,40 @@ int launch_stage_fg(fin_solver* s, const StageArgs& a)
     return set_err(FIN_ERR_ARG, "weno_version");
 }
 
+// Hybrid stages (fin_stage_hyb.cuh): persistent CTAs, two per SM.
+template <int VER, bool P2>
+int launch_stage_hyb_t(fin_solver* s, const StageArgs& a)
+{
+    using Lh = HybSmem<HybCfg>;
+    auto kern = k_stage_hyb<VER, P2, HybCfg>;
+    static bool configured = false;   // per instantiation
+    if (!configured) {
+        CK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(Lh::BYTES)));
+        configured = true;
+    }
+    StageArgs b = a;
+    b.tma = 0;
+    const double* ext = (a.A && a.A != a.qin) ? a.A : ((a.B && a.B != a.qin) ? a.B : nullptr);
+    const int iq = buffer_of(s, a.qin), ie = buffer_of(s, ext);
+    if (s->tma_ok && iq >= 0 && (!ext || ie >= 0)) {
+        b.tma = 1;
+        b.tm_in = s->tm_q[iq];
+        if (ext) b.tm_A = s->tm_a[ie];
+    }
+    const long long tiles = (long long)((a.mx + HybCfg::TI - 1) / HybCfg::TI) * ((a.my + HybCfg::TJ - 1) / HybCfg::TJ);
+    kern<<<unsigned(tiles), HybCfg::NT, Lh::BYTES, s->stream>>>(b);
+    s->launches++;
+    CK(cudaGetLastError());
+    return FIN_OK;
+}
+
 // Hybrid stages: FP32 with per-face choice between full WENO and FD5.
 int launch_stage_hyb(fin_solver* s, const StageArgs& a)
 {
     const bool p2 = s->p.power_param == 2.0;
     switch (s->p.weno_version) {
-    case FIN_WENO_JS:
-        return p2 ? launch_stage_t<float, FIN_WENO_JS, true, false, true>(s, a)
-                  : launch_stage_t<float, FIN_WENO_JS, false, false, true>(s, a);
-    case FIN_WENO_Z:
-        return p2 ? launch_stage_t<float, FIN_WENO_Z, true, false, true>(s, a)
-                  : launch_stage_t<float, FIN_WENO_Z, false, false, true>(s, a);
+    case FIN_WENO_JS: return p2 ? launch_stage_hyb_t<FIN_WENO_JS, true>(s, a) : launch_stage_hyb_t<FIN_WENO_JS, false>(s, a);
+    case FIN_WENO_Z: return p2 ? launch_stage_hyb_t<FIN_WENO_Z, true>(s, a) : launch_stage_hyb_t<FIN_WENO_Z, false>(s, a);
     case FIN_WENO_FD: return launch_stage_t<float, FIN_WENO_FD, true, false, false>(s, a);
     }
     return set_err(FIN_ERR_ARG, "weno_version");
