@@ -130,6 +130,8 @@ struct fin_solver {
     double judge_tol;
     long long hstep, judges, reverts, troubled_last, faces;
     int hyb_off;            // steps left with the indicator switched off after a revert
+    int ind_every;          // the indicator runs every ind_every accepted steps (>= 1)
+    int ind_since;          // accepted steps since its last run; -1: flags not valid for q[cur]
     bool judge_pending;     // the last take_stages ran a judge (results in q[nxt] and q[4])
     bool alpha_valid;       // slots hold alpha of q[cur]
     double last_ms;
@@ -582,7 +584,10 @@ int take_stages(fin_solver* s, double dt, int nxt)
         s->hyb_off--;
         return take_stages_rk(s, dt, nxt, nullptr, q1, q2);
     }
-    if ((rc = launch_indicator(s, s->cur))) return rc;
+    if (s->ind_since < 0 || s->ind_since >= s->ind_every) {
+        if ((rc = launch_indicator(s, s->cur))) return rc;
+        s->ind_since = 0;
+    }
     if ((rc = take_stages_rk(s, dt, nxt, s->flags, q1, q2))) return rc;
     s->hstep++;
     if (s->judge_every > 0 && s->hstep % s->judge_every == 0) {
@@ -615,7 +620,11 @@ void settle_judge(fin_solver* s, int nxt, double dt, double* cfl)
         // q[nxt] <- the full-WENO result (pointer swap), with its alpha slot
         s->reverts++;
         s->hyb_off = s->judge_every;
+        s->ind_since = -1;
+        // the buffers trade places, and their tensor maps with them
         std::swap(s->q[4], s->q[nxt]);
+        std::swap(s->tm_q[4], s->tm_q[nxt]);
+        std::swap(s->tm_a[4], s->tm_a[nxt]);
         cudaMemcpyAsync(alpha_slot(s, nxt), alpha_slot(s, 4), 2 * sizeof(double), cudaMemcpyDeviceToDevice, s->stream);
         sx = s->h_slots[SLOT_SMAX];
         sy = s->h_slots[SLOT_SMAX + 1];
@@ -809,6 +818,8 @@ int fin_create(const fin_params* p, fin_solver** out)
         s->zthr = 0.0f;
         s->judge_every = 20;
         s->judge_tol = 1e-3;
+        s->ind_every = 1;
+        s->ind_since = -1;
         bool ok = true;
         for (int b = 0; b < nbuf && ok; b++)
             ok = make_state_map(&s->tm_q[b], s->q[b], p->mx, p->my, s->plane, Cfg::SJ, Cfg::RI) &&
@@ -887,6 +898,7 @@ int fin_set_state(fin_solver* s, const double* q_host, double t)
     int rc = upload(s, q_host, s->cur);
     if (rc) return rc;
     s->t = t;
+    s->ind_since = -1;
     CK(cudaMemsetAsync(s->slots + SLOT_STATUS, 0, sizeof(double), s->stream));
     if ((rc = compute_alpha(s, s->cur))) return rc;
     s->alpha_valid = true;
@@ -997,6 +1009,17 @@ int fin_set_indicator(fin_solver* s, const float* params, float z_threshold, int
     s->judge_every = judge_every;
     s->judge_tol = judge_tol;
     s->hyb_off = 0;
+    s->ind_since = -1;
+    if (s->ind_every < 1) s->ind_every = 1;
+    return FIN_OK;
+}
+
+int fin_set_indicator_every(fin_solver* s, int every)
+{
+    if (!s) return set_err(FIN_ERR_ARG, "null argument");
+    if (every < 1) return set_err(FIN_ERR_ARG, "the indicator period must be at least one step");
+    s->ind_every = every;
+    s->ind_since = -1;
     return FIN_OK;
 }
 
@@ -1090,6 +1113,7 @@ int fin_step_fixed(fin_solver* s, double dt, double* cfl_out)
     CK(cudaEventElapsedTime(&ms, s->ev0, s->ev1));
     s->last_ms = ms;
     s->cur = nxt;
+    if (s->ind_since >= 0) s->ind_since++;
     s->alpha_valid = true;
     s->t = s->t + dt;
     if (cfl_out) *cfl_out = cfl;
@@ -1156,6 +1180,7 @@ int fin_advance(fin_solver* s, double tend, double* dtv, int max_steps, int* nst
             if (cfl <= CFL_max) {
                 m_accept = 1;
                 s->cur = nxt;          // accept: q^{n+1} becomes q^n (alpha slot travels with it)
+                if (s->ind_since >= 0) s->ind_since++;
                 s->t = t_new;
             } else {
                 t = told;              // reject: q^n was never overwritten

@@ -62,6 +62,8 @@ def load_library(path=LIB_PATH):
     lib.fin_set_indicator.argtypes = [vp, np.ctypeslib.ndpointer(np.float32, flags="C_CONTIGUOUS"), C.c_float,
                                       C.c_int, C.c_double]
     lib.fin_set_indicator.restype = C.c_int
+    lib.fin_set_indicator_every.argtypes = [vp, C.c_int]
+    lib.fin_set_indicator_every.restype = C.c_int
     lib.fin_hybrid_stats.argtypes = [vp] + [C.POINTER(C.c_longlong)] * 4
     lib.fin_hybrid_stats.restype = C.c_int
     lib.fin_face_samples.argtypes = [vp, C.c_longlong, C.c_longlong, C.c_longlong,
@@ -176,10 +178,12 @@ class Solver:
         _check(self.lib.fin_construct_integrated_r(self.h, dt, np.ascontiguousarray(q, dtype=np.float64), F, G))
         return F, G
 
-    def set_indicator(self, params, z_threshold=0.0, judge_every=20, judge_tol=1e-3):
-        """Hybrid form: the troubled-face network's parameters and the judge step."""
+    def set_indicator(self, params, z_threshold=0.0, judge_every=20, judge_tol=1e-3, every=1):
+        """Hybrid form: the troubled-face network's parameters, the judge step,
+        and the indicator's period in accepted steps."""
         _check(self.lib.fin_set_indicator(self.h, np.ascontiguousarray(params, dtype=np.float32), z_threshold,
                                           judge_every, judge_tol))
+        _check(self.lib.fin_set_indicator_every(self.h, every))
 
     def hybrid_stats(self):
         v = [C.c_longlong() for _ in range(4)]

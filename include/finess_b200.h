@@ -217,6 +217,11 @@ int fin_mlp_train(fin_mlp* m, const float* X_host, const unsigned char* y_host, 
  * steps (judge_every = 0: no judge).  Without this call the hybrid form runs
  * full WENO in FP32. */
 int fin_set_indicator(fin_solver* s, const float* params, float z_threshold, int judge_every, double judge_tol);
+/* The indicator's period: it runs on q^n of every `every`-th accepted step
+ * (default 1) and its flags serve the steps in between; the 3 x 3 dilation of
+ * the flags covers the one face a feature can travel at CFL <= 0.5 per step
+ * over two steps.  FIN_ERR_ARG for every < 1. */
+int fin_set_indicator_every(fin_solver* s, int every);
 /* Troubled faces flagged in the last indicator pass, faces per pass, judge
  * steps run and steps reverted. */
 int fin_hybrid_stats(fin_solver* s, long long* troubled_faces, long long* faces, long long* judges, long long* reverts);

@@ -134,3 +134,62 @@ def test_indicator_flags_match_oracle_network(oracle, case):
         st = a.hybrid_stats()
     assert st["faces"] == len(Xo)
     assert abs(st["troubled_faces"] - n_oracle) <= max(near, 2), (st, n_oracle, near)
+
+
+def test_hybrid_after_revert_continues_on_the_right_buffers():
+    """A revert swaps the hybrid attempt's buffer with the full-WENO one; the
+    hybrid steps after it must read the swapped buffers (their TMA maps travel
+    with them).  Schedule with a network that flags nothing, judge every 2nd
+    hybrid step at tolerance 0 (always reverts): FD5, JS, JS, JS, FD5, JS --
+    replayed with FP32 solvers of the two reconstructions."""
+    from finess_b200.solver import Solver
+    import mlp_oracle as M
+    from finess_b200._abi import FIN_WENO_FD
+    Pm = np.zeros(M.NPARAM, dtype=np.float32)
+    Pm[M.OFF_B3] = -10.0
+    p = P.vortex_params(n=64, weno=FIN_WENO_JS)
+    q0 = P.vortex_exact(p)
+    dt = 0.02
+    ph = p.copy(); ph.precision = FIN_PREC_HYBRID
+    with Solver(ph) as a:
+        a.set_indicator(Pm, 0.0, judge_every=2, judge_tol=0.0)
+        a.set_state(q0)
+        for _ in range(6):
+            a.step_fixed(dt)
+        qa, _ = a.get_state()
+        st = a.hybrid_stats()
+    assert st["judges"] == 2 and st["reverts"] == 2
+    pf = p.copy(); pf.precision = FIN_PREC_FP32
+    pd = pf.copy(); pd.weno_version = FIN_WENO_FD
+    q = q0
+    with Solver(pf) as js, Solver(pd) as fd:
+        for form in ("FD", "JS", "JS", "JS", "FD", "JS"):
+            s = fd if form == "FD" else js
+            s.set_state(q)
+            s.step_fixed(dt)
+            q, _ = s.get_state()
+    err = rel_linf(interior(p, qa), interior(p, q))
+    assert err <= 1e-5, err
+
+
+def test_indicator_period():
+    """With period 2 the indicator runs on every other step; the flags of a
+    network that flags everything give the same state either way."""
+    from finess_b200.solver import Solver
+    import mlp_oracle as M
+    Pm = np.zeros(M.NPARAM, dtype=np.float32)
+    Pm[M.OFF_B3] = 10.0
+    p = P.riemann_params(n=64, weno=FIN_WENO_Z)
+    p.precision = FIN_PREC_HYBRID
+    q0 = P.riemann_init(p)
+    out = {}
+    for every in (1, 2):
+        with Solver(p) as a:
+            a.set_indicator(Pm, 0.0, judge_every=0, every=every)
+            a.set_state(q0)
+            n0 = a.launch_count()
+            for _ in range(4):
+                a.step_fixed(5e-4)
+            out[every] = (a.launch_count() - n0, a.get_state()[0])
+    assert out[1][0] - out[2][0] == 2
+    assert rel_linf(interior(p, out[2][1]), interior(p, out[1][1])) == 0.0
