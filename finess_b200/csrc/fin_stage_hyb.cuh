@@ -25,23 +25,36 @@ namespace fin {
 
 using HybCfg = TileCfg<15, 16, 256>;
 
+// Resident CTAs per SM the kernel is laid out for: 3 keeps the update's
+// stage operands in shared memory (q_in's interior in the staging tile, the
+// other operand by a second TMA copy); 4 shares the staging tile's space with
+// the face fluxes and reads both operands from L2 (q_in's interior is there
+// from the tile's own copy, the other operand is prefetched into L2 by TMA),
+// within 64 registers a thread.
+#ifndef FIN_HYB_CTAS
+#define FIN_HYB_CTAS 4
+#endif
+
 // Shared-memory layout (byte offsets) of k_stage_hyb.
 template <class Cfg>
 struct HybSmem {
     static constexpr int TI = Cfg::TI, TJ = Cfg::TJ, RI = Cfg::RI, RJ = Cfg::RJ, NT = Cfg::NT;
+    static constexpr bool SHARE = FIN_HYB_CTAS >= 4;
     static constexpr size_t PRIM = 0;                                                    // float4 [RI][RJ]
     static constexpr size_t FQX = PRIM + size_t(RI) * RJ * 16;                          // float2 [M][RI][TJ]
     static constexpr size_t FQY = FQX + size_t(MEQN) * RI * TJ * 8;                     // float2 [M][TI][RJ]
-    static constexpr size_t FH = FQY + size_t(MEQN) * TI * RJ * 8;                      // float [M][TI+1][TJ]
+    static constexpr size_t FHGH = size_t(MEQN) * ((TI + 1) * TJ + TI * (TJ + 1)) * 4;  // Fh, Gh bytes
+    static constexpr size_t STG = Cfg::pad128(FQY + size_t(MEQN) * TI * RJ * 8);        // double [M][RI][SJ]
+    static constexpr size_t FH = SHARE ? STG : STG + Cfg::pad128(Cfg::STG_BYTES);       // float [M][TI+1][TJ]
     static constexpr size_t GH = FH + size_t(MEQN) * (TI + 1) * TJ * 4;                 // float [M][TI][TJ+1]
-    static constexpr size_t RED = (GH + size_t(MEQN) * TI * (TJ + 1) * 4 + 15) / 16 * 16;  // double [NT/32][4]
+    static constexpr size_t EBUF = Cfg::pad128(SHARE ? STG + Cfg::STG_BYTES : FH + FHGH);   // double [M][TI][TJ]
+    static constexpr size_t RED = SHARE ? EBUF : EBUF + Cfg::ABUF_BYTES;               // double [NT/32][4]
     static constexpr size_t MASK = RED + size_t(NT / 32) * 4 * 8;                       // unsigned [FXR + FYR]
     static constexpr size_t NTRB = MASK + 4 * size_t(Cfg::FXR + Cfg::FYR);              // int
     static constexpr size_t TLIST = NTRB + 4;                                            // short [NFX + NFY]
-    static constexpr size_t STG = Cfg::pad128(TLIST + 2 * size_t(Cfg::NFX + Cfg::NFY)); // double [M][RI][SJ]
-    static constexpr size_t EBUF = STG + Cfg::pad128(Cfg::STG_BYTES);                   // double [M][TI][TJ]
-    static constexpr size_t MBAR = EBUF + Cfg::pad128(Cfg::ABUF_BYTES);                 // uint64
+    static constexpr size_t MBAR = (TLIST + 2 * size_t(Cfg::NFX + Cfg::NFY) + 7) / 8 * 8;   // uint64
     static constexpr size_t BYTES = MBAR + 8;
+    static_assert(!SHARE || FHGH <= Cfg::STG_BYTES, "the face fluxes fit the staging tile");
 };
 
 // linear_face on (0.5 f, q) pairs: P points at stencil point 3.
@@ -106,7 +119,7 @@ __device__ __forceinline__ void hyb_troubled_face(int w, const float2* fqx, cons
 }
 
 template <int VER, bool P2, class Cfg>
-__global__ void __launch_bounds__(Cfg::NT, 3) k_stage_hyb(const __grid_constant__ StageArgs a)
+__global__ void __launch_bounds__(Cfg::NT, FIN_HYB_CTAS) k_stage_hyb(const __grid_constant__ StageArgs a)
 {
     using R = float;
     using L = HybSmem<Cfg>;
@@ -136,20 +149,20 @@ __global__ void __launch_bounds__(Cfg::NT, 3) k_stage_hyb(const __grid_constant_
     const float ag1 = a.alpha_in ? float(a.alpha_in[0]) : 0.0f;
     const float ag2 = a.alpha_in ? float(a.alpha_in[1]) : 0.0f;
     const double* ext = (a.A && a.A != a.qin) ? a.A : ((a.B && a.B != a.qin) ? a.B : nullptr);
-    const bool aligned = ((tc::smem_addr(stg) | tc::smem_addr(ebuf)) & 127u) == 0;
+    const bool aligned = ((tc::smem_addr(stg) | (L::SHARE ? 0u : tc::smem_addr(ebuf))) & 127u) == 0;
     if (a.tma && !aligned && tid == 0) atomicOr(a.status, 16u);
     const bool tt = a.tma && aligned && tma_interior<Cfg>(i0, j0, mx, my);
-    float smax_x = 0.0f, smax_y = 0.0f;
-    double cs_x = 0.0, cs_y = 0.0;
+    float smax_x = 0.0f, smax_y = 0.0f, csx = 0.0f, csy = 0.0f;
     bool neg = false, nonfinite = false;
     // ---- phase 0: q_in's tile + halo and the other operand's interior by
     // TMA (or q_in through the boundary remap); the flag masks ----
     if (tt && tid == 0) {
         tc::mbar_init(mbq, 1);
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
-        tc::mbar_expect_tx(mbq, uint32_t(Cfg::STG_BYTES + (ext ? Cfg::ABUF_BYTES : 0)));
+        tc::mbar_expect_tx(mbq, uint32_t(Cfg::STG_BYTES + (ext && !L::SHARE ? Cfg::ABUF_BYTES : 0)));
         tc::tma_load_3d(stg, &a.tm_in, j0 - 4, i0 - H, 0, mbq);
-        if (ext) tc::tma_load_3d(ebuf, &a.tm_A, j0, i0, 0, mbq);
+        if (ext && !L::SHARE) tc::tma_load_3d(ebuf, &a.tm_A, j0, i0, 0, mbq);
+        if (ext && L::SHARE) tc::tma_prefetch_3d(&a.tm_A, j0, i0, 0);
     }
     {
         const int wx = flag_wx(my), wy = flag_wy(my);
@@ -296,51 +309,68 @@ __global__ void __launch_bounds__(Cfg::NT, 3) k_stage_hyb(const __grid_constant_
         __syncthreads();
         // ---- phase 3: flux difference (ConstructL.cpp:396-398), update
         // (UpdateSoln.cpp:29-35), next-stage wave speed (GlobalWaveSpd.cpp:71-76) ----
-        for (int c = tid; c < TT; c += NT) {
-            const int ci = c / TJ, cj = c - ci * TJ;
-            const int gi = i0 + ci, gj = j0 + cj;
-            if (gi >= mx || gj >= my) continue;
-            const size_t g = size_t(gi) * my + gj;
-            double qn[MEQN];
+        {
+            // operand selection and constants hoisted out of the cell loop
+            const bool hasA = a.A != nullptr, hasB = a.B != nullptr;
+            const bool Aq = a.A == a.qin, Bq = a.B == a.qin;
+            const double a1 = a.a1, a2 = a.a2, bdt = a.bdt;
+            const float rdx = float(a.rdx), rdy = float(a.rdy);
+            const size_t plane = a.plane;
+            for (int c = tid; c < TT; c += NT) {
+                const int ci = c / TJ, cj = c - ci * TJ;
+                const int gi = i0 + ci, gj = j0 + cj;
+                if (gi >= mx || gj >= my) continue;
+                const size_t g = size_t(gi) * my + gj;
+                const float* fh = Fh + ci * TJ + cj;
+                const float* gh = Gh + ci * (TJ + 1) + cj;
+                const double* si = stg + (H + ci) * Cfg::SJ + H + cj + 1;
+                const double* se = ebuf + c;
+                const double* ge = ext ? ext + g : nullptr;
+                double* out = a.qout + g;
+                float qf[MEQN];
 #pragma unroll
-            for (int m = 0; m < MEQN; m++) {
-                const float f1 = Fh[m * (TI + 1) * TJ + (ci + 1) * TJ + cj], f0 = Fh[m * (TI + 1) * TJ + ci * TJ + cj];
-                const float g1 = Gh[m * TI * (TJ + 1) + ci * (TJ + 1) + cj + 1], g0 = Gh[m * TI * (TJ + 1) + ci * (TJ + 1) + cj];
-                float Lr = -(f1 - f0) * float(a.rdx);
-                Lr = Lr - (g1 - g0) * float(a.rdy);
-                const double qi = stg[(m * RI + H + ci) * Cfg::SJ + H + cj + 1];
-                const double qe = ext ? (tt ? ebuf[m * TT + c] : ext[m * a.plane + g]) : 0.0;
-                double v = 0.0;
-                if (a.A) v = a.a1 * (a.A == a.qin ? qi : qe);
-                if (a.B) v = v + a.a2 * (a.B == a.qin ? qi : qe);
-                v = v + a.bdt * double(Lr);
-                qn[m] = v;
-                a.qout[m * a.plane + g] = v;
-            }
-            if (a.alpha_out) {
-                const float qx[MEQN] = {float(qn[0]), float(qn[1]), float(qn[2]), float(qn[3]), float(qn[4])};
-                const float qy[MEQN] = {qx[0], qx[2], qx[1], qx[3], qx[4]};
-                const float sx = Euler::cell_speed(Euler::cell(gam, qx));
-                const float sy = Euler::cell_speed(Euler::cell(gam, qy));
-                if (!(sx <= 1e30f) || !(sy <= 1e30f)) nonfinite = true;
-                if (sx <= 1e30f) cs_x = Max(cs_x, double(sx));
-                if (sy <= 1e30f) cs_y = Max(cs_y, double(sy));
+                for (int m = 0; m < MEQN; m++) {
+                    const float f1 = fh[m * (TI + 1) * TJ + TJ], f0 = fh[m * (TI + 1) * TJ];
+                    const float g1 = gh[m * TI * (TJ + 1) + 1], g0 = gh[m * TI * (TJ + 1)];
+                    const float Lr = -(f1 - f0) * rdx - (g1 - g0) * rdy;
+                    const double qi = L::SHARE ? a.qin[m * plane + g] : si[m * RI * Cfg::SJ];
+                    const double qe = (tt && !L::SHARE) ? se[m * TT] : (ge ? ge[m * plane] : 0.0);
+                    double v = hasA ? a1 * (Aq ? qi : qe) : 0.0;
+                    if (hasB) v = v + a2 * (Bq ? qi : qe);
+                    v = v + bdt * double(Lr);
+                    out[m * plane] = v;
+                    qf[m] = float(v);
+                }
+                if (a.alpha_out) {
+                    // GlobalWaveSpd.cpp:71-76 in both directions; with Ql = Qr
+                    // max(|u_n - c|, |u_n + c|) is |u_n| + c, and p, c are
+                    // the same for both directions
+                    const float ir = rcp(qf[0]);
+                    const float u1 = qf[1] * ir, u2 = qf[2] * ir, u3 = qf[3] * ir;
+                    const float press = (gam - 1.0f) * (qf[4] - 0.5f * qf[0] * (u1 * u1 + u2 * u2 + u3 * u3));
+                    const float cc = fsqrt(fabsf(gam * press * ir));
+                    const float sx = fabsf(u1) + cc, sy = fabsf(u2) + cc;
+                    if (!(sx <= 1e30f) || !(sy <= 1e30f)) nonfinite = true;
+                    if (sx <= 1e30f) csx = Max(csx, sx);
+                    if (sy <= 1e30f) csy = Max(csy, sy);
+                }
             }
         }
     }
 
-    // ---- block reductions of the four maxima, one atomic each ----
-    double v4[4] = {double(smax_x), double(smax_y), cs_x, cs_y};
+    // ---- block reductions of the four maxima (FP32 values, reduced in
+    // FP32), one atomic each ----
+    float v4[4] = {smax_x, smax_y, csx, csy};
 #pragma unroll
     for (int k = 0; k < 4; k++) {
-        double v = v4[k] <= 1e300 ? v4[k] : 0.0;
+        float v = v4[k] <= 1e30f ? v4[k] : 0.0f;
 #pragma unroll
         for (int o = 16; o > 0; o >>= 1) v = Max(v, __shfl_xor_sync(0xffffffffu, v, o));
         v4[k] = v;
     }
     if (lane == 0) {
 #pragma unroll
-        for (int k = 0; k < 4; k++) red[(tid >> 5) * 4 + k] = v4[k];
+        for (int k = 0; k < 4; k++) red[(tid >> 5) * 4 + k] = double(v4[k]);
     }
     if (neg) atomicOr(a.status, 2u);
     if (nonfinite) atomicOr(a.status, 1u);

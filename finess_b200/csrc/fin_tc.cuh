@@ -117,6 +117,16 @@ __device__ __forceinline__ void tma_load_3d(void* dst, const CUtensorMap* map, i
         : "memory");
 }
 
+// The same box of a 3D tensor prefetched into L2 only (no shared memory, no
+// completion to wait for).
+__device__ __forceinline__ void tma_prefetch_3d(const CUtensorMap* map, int x, int y, int z)
+{
+    asm volatile("cp.async.bulk.prefetch.tensor.3d.L2.global.tile [%0, {%1, %2, %3}];"
+                 :
+                 : "l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(y), "r"(z)
+                 : "memory");
+}
+
 // TMEM allocation by one full warp: writes the base address into *dst.
 __device__ __forceinline__ void tmem_alloc(uint32_t* dst, uint32_t ncols)
 {
