@@ -116,7 +116,11 @@ struct fin_solver {
     cudaStream_t stream;
     cudaEvent_t ev0, ev1;
     cudaEvent_t kev[6];     // start/stop of the three stage kernels of the last step
-    bool time_kernels;      // record kev around each stage launch
+    cudaEvent_t iev[2];     // start/stop of the indicator launch of the last step
+    bool time_kernels;      // record kev around each stage launch (and iev)
+    bool ind_timed;         // the last step launched the indicator under timing
+    double ind_ms;          // accumulated indicator-kernel time
+    long long ind_launches;
     double kernel_ms;       // accumulated stage-kernel time since the last reset
     long long kernel_launches;
     double t;               // Qnew.get_t()
@@ -387,6 +391,13 @@ int collect_kernel_times(fin_solver* s)
         s->kernel_ms += ms;
         s->kernel_launches++;
     }
+    if (s->ind_timed) {
+        float ms = 0.f;
+        CK(cudaEventElapsedTime(&ms, s->iev[0], s->iev[1]));
+        s->ind_ms += ms;
+        s->ind_launches++;
+        s->ind_timed = false;
+    }
     return FIN_OK;
 }
 
@@ -585,7 +596,12 @@ int take_stages(fin_solver* s, double dt, int nxt)
         return take_stages_rk(s, dt, nxt, nullptr, q1, q2);
     }
     if (s->ind_since < 0 || s->ind_since >= s->ind_every) {
+        if (s->time_kernels) CK(cudaEventRecord(s->iev[0], s->stream));
         if ((rc = launch_indicator(s, s->cur))) return rc;
+        if (s->time_kernels) {
+            CK(cudaEventRecord(s->iev[1], s->stream));
+            s->ind_timed = true;
+        }
         s->ind_since = 0;
     }
     if ((rc = take_stages_rk(s, dt, nxt, s->flags, q1, q2))) return rc;
@@ -593,7 +609,11 @@ int take_stages(fin_solver* s, double dt, int nxt)
     if (s->judge_every > 0 && s->hstep % s->judge_every == 0) {
         CK(cudaMemcpyAsync(s->slots + SLOT_SMAX_ALT, s->slots + SLOT_SMAX, 2 * sizeof(double), cudaMemcpyDeviceToDevice,
                            s->stream));
-        if ((rc = take_stages_rk(s, dt, 4, nullptr, q1, q2))) return rc;
+        const bool tk = s->time_kernels;   // the step's stage times stay those of the hybrid stages
+        s->time_kernels = false;
+        rc = take_stages_rk(s, dt, 4, nullptr, q1, q2);
+        s->time_kernels = tk;
+        if (rc) return rc;
         CK(cudaMemsetAsync(s->slots + SLOT_DIFF, 0, 2 * sizeof(double), s->stream));
         const size_t n = size_t(s->p.mx) * s->p.my;
         k_max_diff<<<grid_blocks(n), 256, 0, s->stream>>>(s->q[nxt], s->q[4], s->plane, n, s->slots + SLOT_DIFF);
@@ -839,6 +859,8 @@ int fin_create(const fin_params* p, fin_solver** out)
     if ((e = cudaEventCreate(&s->ev1)) != cudaSuccess) return fail(e, "event");
     for (int k = 0; k < 6; k++)
         if ((e = cudaEventCreate(&s->kev[k])) != cudaSuccess) return fail(e, "event");
+    for (int k = 0; k < 2; k++)
+        if ((e = cudaEventCreate(&s->iev[k])) != cudaSuccess) return fail(e, "event");
     if ((e = cudaMemsetAsync(s->slots, 0, NSLOTS * sizeof(double), s->stream)) != cudaSuccess) return fail(e, "memset");
     for (int b = 0; b < nbuf; b++)
         if ((e = cudaMemsetAsync(s->q[b], 0, MEQN * s->plane * sizeof(double), s->stream)) != cudaSuccess) return fail(e, "memset");
@@ -868,6 +890,8 @@ int fin_destroy(fin_solver* s)
     if (s->ev1) cudaEventDestroy(s->ev1);
     for (int k = 0; k < 6; k++)
         if (s->kev[k]) cudaEventDestroy(s->kev[k]);
+    for (int k = 0; k < 2; k++)
+        if (s->iev[k]) cudaEventDestroy(s->iev[k]);
     if (s->stream) cudaStreamDestroy(s->stream);
     delete s;
     return FIN_OK;
@@ -1241,6 +1265,17 @@ int fin_set_kernel_timing(fin_solver* s, int on)
     s->time_kernels = on != 0;
     s->kernel_ms = 0.0;
     s->kernel_launches = 0;
+    s->ind_ms = 0.0;
+    s->ind_launches = 0;
+    s->ind_timed = false;
+    return FIN_OK;
+}
+
+int fin_indicator_time(fin_solver* s, double* ms, long long* launches)
+{
+    if (!s || !ms || !launches) return set_err(FIN_ERR_ARG, "null argument");
+    *ms = s->ind_ms;
+    *launches = s->ind_launches;
     return FIN_OK;
 }
 

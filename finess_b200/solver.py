@@ -58,6 +58,8 @@ def load_library(path=LIB_PATH):
     lib.fin_advance.argtypes = [vp, C.c_double, _dp, C.c_int, C.POINTER(C.c_int)]
     lib.fin_set_kernel_timing.argtypes = [vp, C.c_int]
     lib.fin_kernel_time.argtypes = [vp, C.POINTER(C.c_double), C.POINTER(C.c_longlong)]
+    lib.fin_indicator_time.argtypes = [vp, C.POINTER(C.c_double), C.POINTER(C.c_longlong)]
+    lib.fin_indicator_time.restype = C.c_int
     lib.fin_fma_peak.argtypes = [C.c_int, C.POINTER(C.c_double)]
     lib.fin_set_indicator.argtypes = [vp, np.ctypeslib.ndpointer(np.float32, flags="C_CONTIGUOUS"), C.c_float,
                                       C.c_int, C.c_double]
@@ -216,6 +218,11 @@ class Solver:
     def kernel_time(self):
         ms, n = C.c_double(), C.c_longlong()
         _check(self.lib.fin_kernel_time(self.h, C.byref(ms), C.byref(n)))
+        return ms.value, n.value
+
+    def indicator_time(self):
+        ms, n = C.c_double(), C.c_longlong()
+        _check(self.lib.fin_indicator_time(self.h, C.byref(ms), C.byref(n)))
         return ms.value, n.value
 
     def step_fixed(self, dt):

@@ -166,6 +166,8 @@ int fin_last_kernel_ms(fin_solver* s, double* ms);
  * since fin_set_kernel_timing was last called. */
 int fin_set_kernel_timing(fin_solver* s, int on);
 int fin_kernel_time(fin_solver* s, double* ms, long long* launches);
+/* The same for the hybrid form's indicator launches. */
+int fin_indicator_time(fin_solver* s, double* ms, long long* launches);
 
 /* Measured FMA throughput of the current device in TFLOP/s (FMA = 2 flops),
  * FP64 (fp64 != 0) or FP32: the denominators of pipe-utilisation figures. */
