@@ -119,14 +119,17 @@ def measured_peaks():
 
 
 def profile_traffic_bytes_per_cell(form):
-    """Per-cell DRAM traffic of one stage launch from the committed ncu summary
-    (profiles/stage_kernel_*.txt, line 'dram_bytes_per_cell_<form>: X')."""
+    """Per-cell DRAM traffic of an average stage launch from the committed ncu
+    summary (profiles/stage_kernel_*.txt, line 'dram_bytes_per_cell_<form>: X A'
+    with X measured on one launch whose algorithmic bytes per cell are A):
+    X scaled to the stage average of 320/3 algorithmic bytes per cell."""
     import glob
     for f in sorted(glob.glob(os.path.join(ROOT, "profiles", "stage_kernel_*.txt"))):
         for line in open(f):
             if line.startswith(f"dram_bytes_per_cell_{form}:"):
                 try:
-                    return float(line.split(":", 1)[1].split()[0])
+                    x, alg = (float(v) for v in line.split(":", 1)[1].split()[:2])
+                    return x * (BYTES_PER_CELL_UPDATE / 3.0) / alg
                 except ValueError:
                     pass
     return None
