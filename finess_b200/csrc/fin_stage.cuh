@@ -106,35 +106,19 @@ struct TileCfg {
     }
     template <class R>
     __host__ __device__ static constexpr size_t smem_bytes() { return red_offset<R>() + 4 * (NT / 32) * sizeof(double); }
-    // Hybrid form, after the reduction scratch: the troubled-face count; the
-    // flag windows of the 3 x 3 dilation as one bit mask per face row (x
-    // faces: rows i0-1 .. i0+TI+1, bit c = column j0-1+c, c < TJ+2; y faces:
-    // rows i0-1 .. i0+TI, c < TJ+3), each already dilated along j; the list
-    // of troubled faces (work-list indices).
+    // Hybrid form (k_stage_hyb): the flag windows of the 3 x 3 dilation as
+    // one bit mask per face row (x faces: rows i0-1 .. i0+TI+1, bit c =
+    // column j0-1+c, c < TJ+2; y faces: rows i0-1 .. i0+TI, c < TJ+3).
     static constexpr int FXR = TI + 3, FXC = TJ + 2, FYR = TI + 2, FYC = TJ + 3;
-    static_assert(FYC <= 32, "flag row masks are 32-bit words");
-    __host__ __device__ static constexpr size_t hyb_bytes()
-    {
-        return (4 + 4 * size_t(FXR + FYR) + 2 * size_t(NFX + NFY) + 15) / 16 * 16;
-    }
-    // Hybrid form, 128-byte aligned after that: the FP64 staging tile of q_in
-    // (rows i0-3 .. i0+TI+2, columns j0-4 .. j0+TJ+3, so the TMA box starts
-    // on a 16-byte boundary), the FP64 tile of the other stage operand, and
-    // the mbarrier of the two copies.
-    // A TMA destination must start on a 128-byte boundary, so each buffer is
-    // padded to a multiple of 128 bytes.
+    static constexpr bool MASKS_FIT = FYC <= 32;   // flag row masks are 32-bit words
+    // The FP64 staging tile of q_in (rows i0-3 .. i0+TI+2, columns j0-4 ..
+    // j0+TJ+3, so the TMA box starts on a 16-byte boundary) and the interior
+    // tile of a stage operand; a TMA destination starts on a 128-byte
+    // boundary, so buffers are padded to multiples of 128 bytes.
     static constexpr int SJ = TJ + 8;
     static constexpr size_t STG_BYTES = size_t(MEQN) * RI * SJ * 8;
     static constexpr size_t ABUF_BYTES = size_t(MEQN) * TI * TJ * 8;
     __host__ __device__ static constexpr size_t pad128(size_t b) { return (b + 127) / 128 * 128; }
-    template <class R>
-    __host__ __device__ static constexpr size_t stg_offset() { return pad128(smem_bytes<R>() + hyb_bytes()); }
-    template <class R>
-    __host__ __device__ static constexpr size_t abuf_offset() { return stg_offset<R>() + pad128(STG_BYTES); }
-    template <class R>
-    __host__ __device__ static constexpr size_t mbar_offset() { return abuf_offset<R>() + pad128(ABUF_BYTES); }
-    template <class R>
-    __host__ __device__ static constexpr size_t hyb_smem_bytes() { return mbar_offset<R>() + 16; }
 };
 
 // Staging of q_in's tile + 3-cell halo (the cross region: rows i0-3 ..
@@ -208,15 +192,8 @@ __device__ __forceinline__ R linear_face(const R* f, int fstr, const R* q, int q
 #ifndef FIN_MINB_F32
 #define FIN_MINB_F32 3
 #endif
-// The hybrid form's faces are mostly the 12-operation linear flux; its full
-// WENO pass runs on few faces, so it trades registers (spills there) for
-// resident blocks.
-#ifndef FIN_MINB_HYB
-#define FIN_MINB_HYB 3
-#endif
-template <class R, bool HYB = false> struct MinBlocks { static constexpr int value = FIN_MINB_F64; };
-template <> struct MinBlocks<float, false> { static constexpr int value = FIN_MINB_F32; };
-template <> struct MinBlocks<float, true> { static constexpr int value = FIN_MINB_HYB; };
+template <class R> struct MinBlocks { static constexpr int value = FIN_MINB_F64; };
+template <> struct MinBlocks<float> { static constexpr int value = FIN_MINB_F32; };
 
 // Scalar parameters read from kernel-parameter space where they are used
 // (keeps them out of the register budget of the face loop).
@@ -277,99 +254,28 @@ __device__ __forceinline__ void right_add(const typename Euler::Eig<R>& e, int k
     }
 }
 
-template <class R, int VER, bool P2, class Cfg, bool FG = false, bool HYB = false>
-__global__ void __launch_bounds__(Cfg::NT, MinBlocks<R, HYB>::value) k_stage(const __grid_constant__ StageArgs a)
+// One tile (rows i0 .., columns j0 ..) of a stage; the whole CTA takes part.
+template <class R, int VER, bool P2, class Cfg, bool FG = false>
+__device__ __forceinline__ void stage_tile(const StageArgs& a, const int i0, const int j0)
 {
     constexpr int TI = Cfg::TI, TJ = Cfg::TJ, NT = Cfg::NT, H = Cfg::H;
     constexpr int RI = Cfg::RI, RJ = Cfg::RJ;
     constexpr int PQ = RI * RJ;                    // plane size of qs and prim
     extern __shared__ __align__(128) unsigned char smem_raw[];
-    // prim holds u, v, p, c per cell: planes [4][RI][RJ], or in the hybrid
-    // form one 16-byte (u, v, p, c) per cell, so a face reads its two cells
-    // with two vector loads
-    R* prim = reinterpret_cast<R*>(smem_raw);      // [4][RI][RJ] | [RI][RJ][4]
+    R* prim = reinterpret_cast<R*>(smem_raw);      // [4][RI][RJ]   u, v, p, c
     R* qs = prim + Cfg::NPRIM * PQ;                // [M][RI][RJ]
     R* fs = qs + MEQN * PQ;                        // [M][RI][TJ]   0.5 * f
     R* gs = fs + MEQN * RI * TJ;                   // [M][TI][RJ]   0.5 * g
     R* Fh = gs + MEQN * TI * RJ;                   // [M][TI+1][TJ]
     R* Gh = Fh + MEQN * (TI + 1) * TJ;             // [M][TI][TJ+1]
-    float4* prim4 = reinterpret_cast<float4*>(smem_raw);
     double* red = reinterpret_cast<double*>(smem_raw + Cfg::template red_offset<R>());
 
     const int tid = threadIdx.x;
-    const int i0 = blockIdx.y * TI, j0 = blockIdx.x * TJ;
     const int mx = a.mx, my = a.my;
 #define gamma (Par<R>::gamma(a))
 
     // ---- phase 0: load the tile + halo, boundary conditions by remap ----
-    unsigned char* hyb = smem_raw + Cfg::template smem_bytes<R>();
-    int* ntrb = reinterpret_cast<int*>(hyb);
-    unsigned* fxm = reinterpret_cast<unsigned*>(hyb + 4);     // [FXR]
-    unsigned* fym = fxm + Cfg::FXR;                          // [FYR]
-    short* tlist = reinterpret_cast<short*>(fym + Cfg::FYR);   // [NFX + NFY]
-    double* stg = reinterpret_cast<double*>(smem_raw + Cfg::template stg_offset<R>());    // [M][RI][SJ]
-    double* abuf = reinterpret_cast<double*>(smem_raw + Cfg::template abuf_offset<R>());  // [M][TI][TJ]
-    uint64_t* mbar = reinterpret_cast<uint64_t*>(smem_raw + Cfg::template mbar_offset<R>());
-    bool a_smem = false;
-    // hybrid: the mask words of the flag windows, loaded first (x rows by
-    // warp 0, y rows by warp 1) so they arrive while the tile is staged
-    unsigned fw_lo = 0, fw_hi = 0;
-    if (HYB) {
-        const int wx = flag_wx(my), wy = flag_wy(my), k = (j0 - 1) >> 5;
-        const unsigned* row = nullptr;
-        int nw = 0;
-        if (tid < Cfg::FXR) {
-            const int a1 = i0 - 1 + tid;
-            if (a1 >= 0 && a1 <= mx) { row = a.flags + size_t(a1) * wx; nw = wx; }
-        } else if (tid >= 32 && tid < 32 + Cfg::FYR) {
-            const int a1 = i0 - 1 + (tid - 32);
-            if (a1 >= 0 && a1 < mx) { row = a.flags + size_t(mx + 1) * wx + size_t(a1) * wy; nw = wy; }
-        }
-        if (row) {
-            if (k >= 0 && k < nw) fw_lo = __ldg(row + k);
-            if (k + 1 < nw) fw_hi = __ldg(row + k + 1);
-        }
-    }
-    if (HYB) {
-        // Tiles whose halo lies inside the domain: one TMA copy of q_in's
-        // tile + halo (and one of the other stage operand's tile), issued
-        // first so they are in flight while the flags arrive.  Other tiles
-        // load with the boundary remap.  Either way q_in lands in FP64 in
-        // the staging tile, whose interior the stage update reads again.
-        // (the destinations' 128-byte alignment is checked too: a violation
-        // is reported in the status word and the tile takes the remap path)
-        const bool aligned = ((tc::smem_addr(stg) | tc::smem_addr(abuf)) & 127u) == 0;
-        if (a.tma && !aligned && tid == 0) atomicOr(a.status, 16u);
-        const bool tma_tile = a.tma && aligned && tma_interior<Cfg>(i0, j0, mx, my);
-        const double* ext = (a.A && a.A != a.qin) ? a.A : ((a.B && a.B != a.qin) ? a.B : nullptr);
-        a_smem = tma_tile && ext != nullptr;
-        if (tma_tile && tid == 0) {
-            tc::mbar_init(mbar, 1);
-            asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
-            tc::mbar_expect_tx(mbar, uint32_t(Cfg::STG_BYTES + (a_smem ? Cfg::ABUF_BYTES : 0)));
-            tc::tma_load_3d(stg, &a.tm_in, j0 - 4, i0 - H, 0, mbar);
-            if (a_smem) tc::tma_load_3d(abuf, &a.tm_A, j0, i0, 0, mbar);
-        }
-        if (!tma_tile) stage_remap<Cfg>(stg, a.qin, a.plane, i0, j0, mx, my, a.bc, tid);
-        // the flag windows of the 3 x 3 dilation as row masks, dilated along
-        // j (faces outside the domain count as smooth)
-        if (tid < Cfg::FXR) {
-            const unsigned msk = row_bits(fw_lo, fw_hi, j0 - 1) & ((1u << Cfg::FXC) - 1u);
-            fxm[tid] = msk | (msk >> 1) | (msk >> 2);
-        } else if (tid >= 32 && tid < 32 + Cfg::FYR) {
-            const unsigned msk = row_bits(fw_lo, fw_hi, j0 - 1) & ((1u << Cfg::FYC) - 1u);
-            fym[tid - 32] = msk | (msk >> 1) | (msk >> 2);
-        }
-        if (tid == 0) *ntrb = 0;
-        __syncthreads();
-        if (tma_tile && !tc::mbar_wait(mbar, 0, 1u << 24)) {
-            // the copy did not land in time: report it, and give it one more
-            // bounded wait before the shared memory is read or released
-            atomicOr(a.status, 8u);
-            tc::mbar_wait(mbar, 0, 1u << 24);
-        }
-        // (the FP64 -> R conversion into qs happens in phase 1, cell by cell)
-    } else {
+    {
         for (int e = tid; e < PQ; e += NT) {
             const int ii = e / RJ, jj = e - ii * RJ;
             const bool xin = ii >= H && ii < H + TI, yin = jj >= H && jj < H + TJ;
@@ -391,21 +297,13 @@ __global__ void __launch_bounds__(Cfg::NT, MinBlocks<R, HYB>::value) k_stage(con
         const bool xin = ii >= H && ii < H + TI, yin = jj >= H && jj < H + TJ;
         if (!xin && !yin) continue;
         R rho, m1, m2, m3, en;
-        if (HYB) {
-            // hybrid: the staged FP64 tile, narrowed here and kept in qs
-            const double* sp = stg + ii * Cfg::SJ + jj + 1;
-            rho = R(sp[0]); m1 = R(sp[RI * Cfg::SJ]); m2 = R(sp[2 * RI * Cfg::SJ]);
-            m3 = R(sp[3 * RI * Cfg::SJ]); en = R(sp[4 * RI * Cfg::SJ]);
-            qs[e] = rho; qs[PQ + e] = m1; qs[2 * PQ + e] = m2; qs[3 * PQ + e] = m3; qs[4 * PQ + e] = en;
-        } else {
+        {
             rho = qs[e]; m1 = qs[PQ + e]; m2 = qs[2 * PQ + e]; m3 = qs[3 * PQ + e]; en = qs[4 * PQ + e];
         }
         const R ir = rcp(rho);
         const R u1 = m1 * ir, u2 = m2 * ir, u3 = m3 * ir;
         const R press = (gamma - R(1)) * (en - R(0.5) * rho * (u1 * u1 + u2 * u2 + u3 * u3));
-        if (HYB) {
-            prim4[e] = make_float4(float(u1), float(u2), float(press), float(fsqrt(fabs(gamma * press * ir))));
-        } else {
+        {
             prim[e] = u1;
             prim[PQ + e] = u2;
             prim[2 * PQ + e] = press;
@@ -458,80 +356,10 @@ __global__ void __launch_bounds__(Cfg::NT, MinBlocks<R, HYB>::value) k_stage(con
     const R ag2 = a.alpha_in ? R(a.alpha_in[1]) : R(0);
     R smax_x = R(0), smax_y = R(0);
     bool neg = false, nonfinite = false;
-    if (HYB) {
-        // Hybrid pass A, every face: the LLF speed (and the CFL / status
-        // bookkeeping), the dilated flag, and for smooth faces the linear
-        // flux.  Troubled faces go to a block-local list for pass B.
-#pragma unroll 1
-        for (int wb = 0; wb < Cfg::NFX + Cfg::NFY; wb += NT) {
-            const int w = wb + tid;
-            bool push = false;
-            if (w < Cfg::NFX + Cfg::NFY) {
-                const bool isx = w < Cfg::NFX;
-                int fi, fj, qbase, qstr, fbase, fstr, fplane;
-                const R* fl;
-                if (isx) {
-                    fi = w / TJ; fj = w - fi * TJ;
-                    qbase = (H + fi) * RJ + (H + fj); qstr = RJ;
-                    fl = fs; fbase = (H + fi) * TJ + fj; fstr = TJ; fplane = RI * TJ;
-                } else {
-                    const int v = w - Cfg::NFX;
-                    fi = v / (TJ + 1); fj = v - fi * (TJ + 1);
-                    qbase = (H + fi) * RJ + (H + fj); qstr = 1;
-                    fl = gs; fbase = fi * RJ + (H + fj); fstr = 1; fplane = TI * RJ;
-                }
-                const int ql = qbase - qstr;
-                const float4 PL = prim4[ql], PR = prim4[qbase];
-                const R unl = isx ? PL.x : PL.y, unr = isx ? PR.x : PR.y;
-                const R pl = PL.z, pr = PR.z;
-                const R cl = PL.w, cr = PR.w;
-                const R rho = R(0.5) * (qs[qbase] + qs[ql]);
-                const R ua = R(0.5) * (unl + unr);
-                const R pa = R(0.5) * (pl + pr);
-                const R ca = fsqrt(fabs(gamma * pa * rcp(rho)));
-                if (pa < R(0) || rho < R(0)) neg = true;
-                const R s1 = Min(unl - cl, ua - ca);
-                const R s2 = Max(unr + cr, ua + ca);
-                const R alpha = Max(isx ? ag1 : ag2, Max(fabs(s1), fabs(s2)));
-                if (!(alpha <= R(1e30))) nonfinite = true;
-                const unsigned* fm = isx ? fxm : fym;
-                const bool trb = (((fm[fi] | fm[fi + 1] | fm[fi + 2]) >> fj) & 1u) != 0;
-                if (isx) {
-                    const int gfi = i0 + fi, gj = j0 + fj;
-                    if (gfi < mx && gj < my && alpha <= R(1e30)) smax_x = Max(smax_x, alpha);
-                    if (a.face_alpha_x && gfi <= mx && gj < my) a.face_alpha_x[size_t(gfi) * my + gj] = double(alpha);
-                } else {
-                    const int gi = i0 + fi, gfj = j0 + fj;
-                    if (gi < mx && gfj < my && alpha <= R(1e30)) smax_y = Max(smax_y, alpha);
-                    if (a.face_alpha_y && gi < mx && gfj <= my) a.face_alpha_y[size_t(gi) * (my + 1) + gfj] = double(alpha);
-                }
-                if (trb) {
-                    push = true;
-                } else {
-                    const R lah = R(0.5) * Par<R>::ascale(a) * alpha;
-                    R* dst = isx ? Fh + fi * TJ + fj : Gh + fi * (TJ + 1) + fj;
-                    const int dplane = isx ? (TI + 1) * TJ : TI * (TJ + 1);
-#pragma unroll
-                    for (int m = 0; m < MEQN; m++)
-                        dst[m * dplane] = linear_face<R>(fl + m * fplane + fbase, fstr, qs + m * PQ + qbase, qstr, lah);
-                }
-            }
-            // warp-aggregated append to the troubled list
-            const unsigned bal = __ballot_sync(0xffffffffu, push);
-            if (bal) {
-                const int lane = tid & 31;
-                int base = 0;
-                if (lane == __ffs(bal) - 1) base = atomicAdd(ntrb, __popc(bal));
-                base = __shfl_sync(0xffffffffu, base, __ffs(bal) - 1);
-                if (push) tlist[base + __popc(bal & ((1u << lane) - 1u))] = short(w);
-            }
-        }
-        __syncthreads();
-    }
-    const int nwork = HYB ? *ntrb : Cfg::NFX + Cfg::NFY;
+    const int nwork = Cfg::NFX + Cfg::NFY;
 #pragma unroll 1
     for (int k = tid; k < nwork; k += NT) {
-        const int w = HYB ? int(tlist[k]) : k;
+        const int w = k;
         const bool isx = w < Cfg::NFX;
         int fi, fj, qbase, qstr, fbase, fstr, fplane;
         const R* fl;
@@ -561,11 +389,7 @@ __global__ void __launch_bounds__(Cfg::NT, MinBlocks<R, HYB>::value) k_stage(con
         {
             const int un = isx ? 0 : 1;
             R unl, unr, pl, pr, cl, cr;
-            if (HYB) {
-                const float4 PL = prim4[ql], PR = prim4[qbase];
-                unl = isx ? PL.x : PL.y; unr = isx ? PR.x : PR.y;
-                pl = PL.z; pr = PR.z; cl = PL.w; cr = PR.w;
-            } else {
+            {
                 unl = prim[un * PQ + ql]; unr = prim[un * PQ + qbase];
                 pl = prim[2 * PQ + ql]; pr = prim[2 * PQ + qbase];
                 cl = prim[3 * PQ + ql]; cr = prim[3 * PQ + qbase];
@@ -719,12 +543,7 @@ __global__ void __launch_bounds__(Cfg::NT, MinBlocks<R, HYB>::value) k_stage(con
             Lr = Lr - (g1 - g0) * R(a.rdy);
             const double L = double(Lr);
             double v = 0.0;
-            if (HYB) {
-                // stage operands from shared memory where they were staged
-                const double qin_c = stg[(m * RI + H + ci) * Cfg::SJ + H + cj + 1];
-                if (a.A) v = a.a1 * (a.A == a.qin ? qin_c : (a_smem ? abuf[(m * TI + ci) * TJ + cj] : a.A[m * a.plane + g]));
-                if (a.B) v = v + a.a2 * (a.B == a.qin ? qin_c : (a_smem ? abuf[(m * TI + ci) * TJ + cj] : a.B[m * a.plane + g]));
-            } else {
+            {
                 if (a.A) v = a.a1 * a.A[m * a.plane + g];
                 if (a.B) v = v + a.a2 * a.B[m * a.plane + g];
             }
@@ -770,6 +589,12 @@ __global__ void __launch_bounds__(Cfg::NT, MinBlocks<R, HYB>::value) k_stage(con
         double* dst = tid < 2 ? a.smax_out : a.alpha_out;
         if (dst) atomic_max_nonneg(dst + (tid & 1), v);
     }
+}
+
+template <class R, int VER, bool P2, class Cfg, bool FG = false>
+__global__ void __launch_bounds__(Cfg::NT, MinBlocks<R>::value) k_stage(const __grid_constant__ StageArgs a)
+{
+    stage_tile<R, VER, P2, Cfg, FG>(a, blockIdx.y * Cfg::TI, blockIdx.x * Cfg::TJ);
 }
 
 // GlobalWaveSpd (lib/2d/GlobalWaveSpd.cpp:52-78) on a state already in HBM:

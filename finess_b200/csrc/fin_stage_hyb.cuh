@@ -123,6 +123,7 @@ __global__ void __launch_bounds__(Cfg::NT, FIN_HYB_CTAS) k_stage_hyb(const __gri
 {
     using R = float;
     using L = HybSmem<Cfg>;
+    static_assert(Cfg::MASKS_FIT, "flag row masks are 32-bit words");
     constexpr int TI = Cfg::TI, TJ = Cfg::TJ, NT = Cfg::NT, H = Cfg::H, RI = Cfg::RI, RJ = Cfg::RJ;
     constexpr int XPL = RI * TJ, YPL = TI * RJ, TT = TI * TJ;   // component planes of fqx, fqy, ebuf
     extern __shared__ __align__(128) unsigned char smem_raw[];

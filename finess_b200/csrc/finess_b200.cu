@@ -262,32 +262,18 @@ int buffer_of(const fin_solver* s, const double* ptr)
     return -1;
 }
 
-template <class R, int VER, bool P2, bool FG = false, bool HYB = false>
+template <class R, int VER, bool P2, bool FG = false>
 int launch_stage_t(fin_solver* s, const StageArgs& a)
 {
-    const size_t smem = HYB ? Cfg::template hyb_smem_bytes<R>() : Cfg::template smem_bytes<R>();
-    auto kern = k_stage<R, VER, P2, Cfg, FG, HYB>;
+    const size_t smem = Cfg::template smem_bytes<R>();
+    auto kern = k_stage<R, VER, P2, Cfg, FG>;
     static bool configured = false;   // per instantiation; attribute is per device function
     if (!configured) {
         CK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
         configured = true;
     }
     dim3 grid((a.my + Cfg::TJ - 1) / Cfg::TJ, (a.mx + Cfg::TI - 1) / Cfg::TI);
-    if (HYB) {
-        // the tensor maps of q_in and of the operand that is not q_in
-        StageArgs b = a;
-        b.tma = 0;
-        const double* ext = (a.A && a.A != a.qin) ? a.A : ((a.B && a.B != a.qin) ? a.B : nullptr);
-        const int iq = buffer_of(s, a.qin), ie = buffer_of(s, ext);
-        if (s->tma_ok && iq >= 0 && (!ext || ie >= 0)) {
-            b.tma = 1;
-            b.tm_in = s->tm_q[iq];
-            if (ext) b.tm_A = s->tm_a[ie];
-        }
-        kern<<<grid, Cfg::NT, smem, s->stream>>>(b);
-    } else {
-        kern<<<grid, Cfg::NT, smem, s->stream>>>(a);
-    }
+    kern<<<grid, Cfg::NT, smem, s->stream>>>(a);
     s->launches++;
     CK(cudaGetLastError());
     return FIN_OK;
@@ -355,7 +341,7 @@ int launch_stage_hyb(fin_solver* s, const StageArgs& a)
     switch (s->p.weno_version) {
     case FIN_WENO_JS: return p2 ? launch_stage_hyb_t<FIN_WENO_JS, true>(s, a) : launch_stage_hyb_t<FIN_WENO_JS, false>(s, a);
     case FIN_WENO_Z: return p2 ? launch_stage_hyb_t<FIN_WENO_Z, true>(s, a) : launch_stage_hyb_t<FIN_WENO_Z, false>(s, a);
-    case FIN_WENO_FD: return launch_stage_t<float, FIN_WENO_FD, true, false, false>(s, a);
+    case FIN_WENO_FD: return launch_stage_t<float, FIN_WENO_FD, true, false>(s, a);
     }
     return set_err(FIN_ERR_ARG, "weno_version");
 }

@@ -232,6 +232,33 @@ int fin_hybrid_stats(fin_solver* s, long long* troubled_faces, long long* faces,
 int fin_face_samples(fin_solver* s, long long offset, long long stride, long long max_n, float* X_host,
                      unsigned char* y_host, long long* n_out);
 
+/* ---- batches of independent problems ---------------------------------- */
+/* No single counterpart in the reference (an application would run
+ * FinSolveRK, lib/2d/FinSolveRK.cpp:13, once per problem).  A batch holds
+ * nprob independent 2D Euler problems of any grid sizes (params[k]: grid,
+ * domain, boundaries, CFL numbers and nv per problem; precision (FP64 or
+ * FP32), WENO version, power, epsilon, gamma, alpha_scaling and global_alpha
+ * shared; SSP-RK3) and advances all of them to one end time, each with its
+ * own adaptive dt: per problem the arithmetic and the step control are
+ * fin_solve's, so the results agree with separate runs to rounding; the
+ * stages of all problems run as one launch each, from a work queue of tiles.  States are passed in
+ * the reference's ghosted layout of each problem, as fin_set_state. */
+typedef struct fin_batch fin_batch;
+int fin_batch_create(const fin_params* params, int nprob, fin_batch** out);
+int fin_batch_destroy(fin_batch* b);
+int fin_batch_set_state(fin_batch* b, int k, const double* q_host, double t);
+int fin_batch_get_state(fin_batch* b, int k, double* q_host, double* t);
+/* dtv1[k]: problem k's dt on entry and on exit (dtv[1] of RunFinpack.cpp:62);
+ * steps[k] (may be NULL): its accepted steps.  Fails with the first failing
+ * problem's code (FIN_ERR_NSTEPS, FIN_ERR_DT_BOUNDS, FIN_ERR_CFL_BOUNDS,
+ * FIN_ERR_NONFINITE). */
+int fin_batch_solve(fin_batch* b, double tend, double* dtv1, int* steps);
+/* Device time of the last solve, graph replays (each one step of every
+ * active problem), the tile shape the autotuner chose (0: 15x16, 1: 7x32)
+ * and its stage-1 times for both (tune_ms[2]). */
+int fin_batch_stats(fin_batch* b, double* device_ms, long long* replays, int* tile_cfg, double* tune_ms);
+const char* fin_batch_last_error(void);
+
 /* ---- for callers that cannot allocate device memory ------------------- */
 /* No counterpart in the reference.  For callers that must not call
  * cudaMalloc (an application whose own allocator owns the device, or a loop

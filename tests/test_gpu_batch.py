@@ -1,0 +1,70 @@
+"""The batched solver against separate single-problem runs: per problem the
+batch runs the same stage arithmetic and step control, so it must take the
+same number of steps and agree with the separate run to rounding (the plain
+FP64 form's 1e-12 bar; FP32 to FP32 rounding)."""
+import numpy as np
+import pytest
+
+from conftest import interior, rel_linf
+from finess_b200 import problems as P
+from finess_b200._abi import FIN_PREC_FP32, FIN_PREC_FP64, FIN_WENO_Z
+
+pytestmark = pytest.mark.gpu
+
+
+def _problems(precision):
+    rng = np.random.default_rng(3)
+    params, states = [], []
+    for n in (20, 33, 48, 17, 40):
+        p = P.riemann_params(n=n, weno=FIN_WENO_Z)
+        p.precision = precision
+        params.append(p)
+        states.append(P.random_riemann_state(p, rng))
+    p = P.riemann_params(n=30, weno=FIN_WENO_Z)
+    p.my = 25
+    p.precision = precision
+    params.append(p)
+    states.append(P.random_riemann_state(p, rng))
+    p = P.vortex_params(n=36, weno=FIN_WENO_Z)   # periodic, on another domain
+    p.precision = precision
+    params.append(p)
+    states.append(P.vortex_exact(p))
+    return params, states
+
+
+@pytest.mark.parametrize("precision", [FIN_PREC_FP64, FIN_PREC_FP32])
+def test_batch_equals_separate_runs(oracle, precision):
+    from finess_b200.batch import Batch, first_dt
+    from finess_b200.solver import Solver
+    params, states = _problems(precision)
+    states = [oracle.set_bnd(p, q) for p, q in zip(params, states)]
+    tend = 0.05
+    dts = np.array([first_dt(p, q) for p, q in zip(params, states)])
+    with Batch(params) as b:
+        for k, q in enumerate(states):
+            b.set_state(k, q)
+        dt_out, steps = b.solve(tend, dts)
+        got = [b.get_state(k) for k in range(len(params))]
+        st = b.stats()
+    assert st["replays"] >= steps.max()
+    for k, (p, q) in enumerate(zip(params, states)):
+        with Solver(p) as s:
+            s.set_state(q)
+            dtv, n = s.FinSolveRK(tend, np.array([0.0, dts[k], p.max_dt]))
+            qs, ts = s.get_state()
+        qb, tb = got[k]
+        tol = 1e-12 if precision == FIN_PREC_FP64 else 1e-5
+        assert steps[k] == n, (k, steps[k], n)
+        assert abs(dt_out[k] - dtv[1]) <= tol * dtv[1], (k, dt_out[k], dtv[1])
+        assert abs(tb - ts) <= 1e-14 * max(1.0, abs(ts))
+        assert rel_linf(interior(p, qb), interior(p, qs)) <= tol, k
+
+
+def test_batch_rejects_mixed_forms():
+    from finess_b200.batch import Batch
+    from finess_b200.solver import FinError
+    a = P.riemann_params(n=16)
+    b = P.riemann_params(n=16)
+    b.precision = FIN_PREC_FP32
+    with pytest.raises(FinError):
+        Batch([a, b])
