@@ -16,6 +16,7 @@ FIN_WENO_FD, FIN_WENO_JS, FIN_WENO_Z = 0, 1, 2
 FIN_TS_RK, FIN_TS_LXW, FIN_TS_MD = 0, 2, 3
 FIN_BC_PERIODIC, FIN_BC_TRANSMISSIVE = 0, 1
 FIN_PHYS_EULER = 0
+FIN_PHYS_MHD = 1
 FIN_PREC_FP64, FIN_PREC_FP32, FIN_PREC_HYBRID = 0, 1, 2
 
 WENO_NAMES = {"FD": FIN_WENO_FD, "JS": FIN_WENO_JS, "Z": FIN_WENO_Z}
@@ -41,6 +42,7 @@ class FinParams(C.Structure):
         ("precision", C.c_int),
         ("tfinal", C.c_double),
         ("nout", C.c_int),
+        ("constrained_transport", C.c_int),
     ]
 
     def copy(self):
@@ -71,6 +73,7 @@ def default_params(**overrides):
     p.physics = FIN_PHYS_EULER
     p.precision = FIN_PREC_FP64
     p.tfinal, p.nout = 0.0, 1
+    p.constrained_transport = 1
     for k, v in overrides.items():
         if not hasattr(p, k):
             raise AttributeError(f"fin_params has no field {k!r}")
@@ -81,6 +84,11 @@ def default_params(**overrides):
 def ghosted_shape(p):
     """numpy shape of a reference dTensorBC3(mx, my, meqn, mbc): (i, j, m)."""
     return (p.mx + 2 * p.mbc, p.my + 2 * p.mbc, p.meqn)
+
+
+def aux_shape(p):
+    """numpy shape of the auxiliary dTensorBC3(mx, my, maux, mbc)."""
+    return (p.mx + 2 * p.mbc, p.my + 2 * p.mbc, p.maux)
 
 
 def smax_shape(p):

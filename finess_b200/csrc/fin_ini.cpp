@@ -1,7 +1,7 @@
 // parameters.ini reader: the same file an unmodified FINESS application
 // ships.  Keys, defaults, enumerations and checks follow the reference's
 // parameter specs (python/finess/params/finess.py, dim2.py, weno.py,
-// euler.py), which its build turns into the IniParams class
+// euler.py, mhd.py), which its build turns into the IniParams class
 // (python/finess/params/params.py:358-497) read by lib/sys/IniParser.h.
 // Booleans parse as true/false like stringToAny<bool> (lib/sys/util.h:9).
 //
@@ -125,6 +125,7 @@ extern "C" int fin_params_from_ini(const char* path, fin_params* p)
         {"grid.ylow", &p->ylow, true}, {"grid.yhigh", &p->yhigh, true},
         {"weno.power_param", &p->power_param, false}, {"weno.alpha_scaling", &p->alpha_scaling, false},
         {"weno.epsilon", &p->epsilon, false}, {"euler.gamma", &p->gamma, false},
+        {"mhd.gamma", &p->gamma, false},
     };
     for (const auto& k : ints) {
         if (!ini.has(k.k)) {
@@ -157,6 +158,13 @@ extern "C" int fin_params_from_ini(const char* path, fin_params* p)
         else if (m == "Multiderivative") p->time_stepping_method = FIN_TS_MD;
         else if (m == "SDC" || m == "User-Defined") return fail("time_stepping_method " + m + " is not built here");
         else return fail("unknown time_stepping_method " + m);
+    }
+    // [mhd] (python/finess/params/mhd.py): its presence selects the MHD callbacks
+    if (ini.has("mhd.gamma")) {
+        p->physics = FIN_PHYS_MHD;
+        if (ini.has("mhd.constrained_transport") &&
+            !parse_bool(ini.get("mhd.constrained_transport"), &p->constrained_transport))
+            return fail("not a bool: mhd.constrained_transport");
     }
     if (ini.has("weno.weno_version")) {
         const std::string v = ini.get("weno.weno_version");

@@ -780,6 +780,7 @@ void fin_params_default(fin_params* p)
     p->precision = FIN_PREC_FP64;
     p->tfinal = 0.0;
     p->nout = 1;
+    p->constrained_transport = 1;
 }
 
 const char* fin_last_error(void) { return g_err.c_str(); }

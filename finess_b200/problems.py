@@ -11,7 +11,7 @@ import math
 
 import numpy as np
 
-from ._abi import (FIN_BC_PERIODIC, FIN_BC_TRANSMISSIVE, FIN_TS_MD, FIN_TS_RK, FIN_WENO_JS,
+from ._abi import (FIN_BC_PERIODIC, FIN_BC_TRANSMISSIVE, FIN_PHYS_MHD, FIN_TS_MD, FIN_TS_RK, FIN_WENO_JS,
                    FIN_WENO_Z, default_params)
 
 
@@ -125,6 +125,70 @@ def shock_entropy_init(p):
     v = np.zeros_like(x)
     pr = np.where(left, 10.33333, 1.0)
     return primitive_to_conserved(p.gamma, rho, u, v, pr)
+
+
+# --------------------------------------------------------------------------
+# 5. Ideal MHD Orszag-Tang vortex on [0,2pi]^2, periodic (apps/2d/mhd/orszag_tang).
+# --------------------------------------------------------------------------
+def orszag_tang_params(n=2048, weno=FIN_WENO_JS, **kw):
+    """apps/2d/mhd/orszag_tang/parameters.ini (meqn 8, maux 1, mbc 7,
+    gamma 5/3, domain [0, 6.2831853071795865]^2, global_alpha default false)
+    with SSP-RK3 at CFL 0.4 (max 0.45) and n x n cells."""
+    p = default_params(mx=n, my=n, mbc=7, meqn=8, maux=1, xlow=0.0, xhigh=6.2831853071795865, ylow=0.0,
+                       yhigh=6.2831853071795865, weno_version=weno, global_alpha=0, desired_cfl=0.4,
+                       max_cfl=0.45, time_stepping_method=FIN_TS_RK, time_order=3, gamma=1.6666666666666667,
+                       physics=FIN_PHYS_MHD, constrained_transport=1, initial_dt=0.001)
+    for k, v in kw.items():
+        setattr(p, k, v)
+    return p
+
+
+def orszag_tang_init(p):
+    """(q, aux): QinitFunc (apps/2d/mhd/orszag_tang/QinitFunc.cpp:10-52) at
+    the cell centres, rho = gamma^2, p = gamma, u = (-sin y, sin x, 0),
+    B = (-sin y, sin 2x, 0); aux = A3 = 0.5 cos 2x + cos y (AfterQinit.cpp:
+    10-35, whose curl is B).  Ghost cells hold the periodic images."""
+    x, y = cell_centres(p)
+    g = p.gamma
+    rho = np.full_like(x, g * g)
+    u1, u2 = -np.sin(y), np.sin(x)
+    B1, B2 = -np.sin(y), np.sin(2.0 * x)
+    q = np.zeros(x.shape + (8,))
+    q[..., 0] = rho
+    q[..., 1] = rho * u1
+    q[..., 2] = rho * u2
+    q[..., 4] = g / (g - 1.0) + 0.5 * rho * (u1 * u1 + u2 * u2) + 0.5 * (B1 * B1 + B2 * B2)
+    q[..., 5] = B1
+    q[..., 6] = B2
+    aux = (0.5 * np.cos(2.0 * x) + np.cos(y))[..., None]
+    return q, aux
+
+
+def mhd_random_state(p, rng, amp=0.3):
+    """A smooth periodic MHD state with every component nonzero (u3, B3
+    included) and (q, aux) consistent: B1, B2 the 4th-order central curl of
+    the periodic potential aux, as constrained transport leaves them."""
+    x, y = cell_centres(p)
+    Lx, Ly = p.xhigh - p.xlow, p.yhigh - p.ylow
+    kx, ky = 2.0 * math.pi / Lx, 2.0 * math.pi / Ly
+    ph = rng.uniform(0, 2 * math.pi, size=10)
+    rho = 1.0 + amp * np.sin(kx * x + ph[0]) * np.cos(ky * y + ph[1])
+    u1 = 0.4 + amp * np.sin(kx * x + ph[2] + ky * y)
+    u2 = -0.3 + amp * np.cos(ky * y + ph[3] - kx * x)
+    u3 = 0.2 * np.sin(kx * x + ph[4])
+    pr = 1.0 + amp * np.cos(kx * x + ph[5]) * np.sin(ky * y + ph[6])
+    A = 0.6 * np.cos(kx * x + ph[7]) + 0.5 * np.sin(ky * y + ph[8]) + 0.2 * np.sin(kx * x + ky * y + ph[9])
+    dx, dy = Lx / p.mx, Ly / p.my
+    B1 = (np.roll(A, 2, 1) - 8 * np.roll(A, 1, 1) + 8 * np.roll(A, -1, 1) - np.roll(A, -2, 1)) / (12 * dy)
+    B2 = -(np.roll(A, 2, 0) - 8 * np.roll(A, 1, 0) + 8 * np.roll(A, -1, 0) - np.roll(A, -2, 0)) / (12 * dx)
+    B3 = 0.3 + 0.1 * np.cos(ky * y + ph[0])
+    g = p.gamma
+    q = np.zeros(x.shape + (8,))
+    q[..., 0] = rho
+    q[..., 1], q[..., 2], q[..., 3] = rho * u1, rho * u2, rho * u3
+    q[..., 4] = pr / (g - 1.0) + 0.5 * rho * (u1 * u1 + u2 * u2 + u3 * u3) + 0.5 * (B1 * B1 + B2 * B2 + B3 * B3)
+    q[..., 5], q[..., 6], q[..., 7] = B1, B2, B3
+    return q, A[..., None]
 
 
 # --------------------------------------------------------------------------

@@ -46,7 +46,7 @@ enum {
 enum fin_weno_version { FIN_WENO_FD = 0, FIN_WENO_JS = 1, FIN_WENO_Z = 2 };
 enum fin_time_stepping { FIN_TS_RK = 0, FIN_TS_LXW = 2, FIN_TS_MD = 3 };
 enum fin_bc { FIN_BC_PERIODIC = 0, FIN_BC_TRANSMISSIVE = 1 };
-enum fin_physics { FIN_PHYS_EULER = 0 };
+enum fin_physics { FIN_PHYS_EULER = 0, FIN_PHYS_MHD = 1 };
 enum fin_precision {
     FIN_PREC_FP64 = 0,     /* plain method, FP64 everywhere (the parity form) */
     FIN_PREC_FP32 = 1,     /* FP32 reconstruction/splitting/projection, FP64 state */
@@ -79,9 +79,12 @@ typedef struct fin_params {
     /* frame loop of RunFinpack (lib/2d/RunFinpack.cpp:95-130) */
     double tfinal;
     int nout;
+    /* [mhd] (python/finess/params/mhd.py:20-26): rebuild B1, B2 from the
+     * potential A3 after every stage (apps/2d/mhd/lib/AfterStep.cpp:31-56) */
+    int constrained_transport;
 } fin_params;
 
-/* Defaults of python/finess/params/finess.py, weno.py and euler.py. */
+/* Defaults of python/finess/params/finess.py, weno.py, euler.py and mhd.py. */
 void fin_params_default(fin_params* p);
 
 /* Reads an application's parameters.ini (sections [finess], [grid], [weno],

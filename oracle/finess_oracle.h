@@ -59,6 +59,25 @@ void oracle_conservation_totals(const fin_params* p, const double* q, double* to
  * x faces then y faces (the device kernel's enumeration). */
 void oracle_face_samples(const fin_params* p, const double* q, double* X, unsigned char* y);
 
+/* ---- ideal MHD (mhd_oracle.c): q ghosted (mx,my,8), aux ghosted (mx,my,1) ---- */
+/* Doubly periodic SetBndValues of apps/2d/mhd/orszag_tang (aux may be NULL). */
+void oracle_mhd_set_bnd(const fin_params* p, double* q, double* aux);
+void oracle_mhd_global_wave_spd(const fin_params* p, const double* q, double* alpha1, double* alpha2);
+/* ConstructL with the MHD callbacks; L interior written, smax max-accumulated. */
+int oracle_mhd_construct_l(const fin_params* p, const double* q, double* L, double* smax);
+/* ConstructHJ_L_Order1 (apps/2d/mhd/lib/ConstructHJ_L.cpp:29-113); needs mbc >= 5. */
+int oracle_mhd_construct_hj_l(const fin_params* p, const double* q, const double* aux, double* Laux);
+/* AfterStep (apps/2d/mhd/lib/AfterStep.cpp:13-60): B1, B2 from aux when
+ * p->constrained_transport is set. */
+void oracle_mhd_after_step(const fin_params* p, double* q, const double* aux);
+/* One SSP-RK3 step of exactly dt (no CFL control); *cfl: the MHD GetCFL. */
+int oracle_mhd_step_fixed(const fin_params* p, double* q, double* aux, double dt, double* cfl);
+/* apps/2d/mhd/lib/FinSolveRK.cpp:17-395 (time_order 3) from *t to tend. */
+int oracle_mhd_finsolve(const fin_params* p, double* q, double* aux, double* t, double tend, double* dtv,
+                        int* nsteps);
+/* Orszag-Tang initial state (QinitFunc + AfterQinit), ghosts filled. */
+void oracle_orszag_tang(const fin_params* p, double* q, double* aux);
+
 #ifdef __cplusplus
 }
 #endif

@@ -5,6 +5,9 @@
 * ``RefLib``: oracle/_ref/libfinref.so, the reference's own sources
   (lib/2d/ConstructL.cpp, lib/WenoReconstruct.cpp, lib/2d/FinSolveRK.cpp, ...)
   compiled in place by oracle/Makefile with the harness in ref_harness/.
+* ``MhdRefLib``: oracle/_ref/libfinref_mhd.so, the same for the ideal-MHD
+  path (lib/2d/ConstructL.cpp with apps/2d/mhd/lib and the Orszag-Tang case).
+  The MHD arrays are q (mx+2mbc, my+2mbc, 8) and aux (mx+2mbc, my+2mbc, 1).
 
 Both take and return numpy arrays in the reference's ghosted dTensorBC3 layout
 (lib/tensors.h:267-273), shape (mx+2mbc, my+2mbc, meqn).  Only tests/,
@@ -22,19 +25,20 @@ ROOT = os.path.dirname(HERE)
 if ROOT not in sys.path:
     sys.path.insert(0, ROOT)
 
-from finess_b200._abi import FinParams, ghosted_shape, smax_shape  # noqa: E402
+from finess_b200._abi import FinParams, aux_shape, ghosted_shape, smax_shape  # noqa: E402
 
 _dp = np.ctypeslib.ndpointer(dtype=np.float64, flags="C_CONTIGUOUS")
 ORACLE_SO = os.path.join(HERE, "liboracle.so")
 REF_SO = os.path.join(HERE, "_ref", "libfinref.so")
 # the same reference objects relinked against libfinb200.so through the shim
 REF_SHIM_SO = os.path.join(HERE, "_ref", "libfinref_shim.so")
+REF_MHD_SO = os.path.join(HERE, "_ref", "libfinref_mhd.so")
 
 
 def build_oracle():
     """Compile liboracle.so (seconds, gcc only) if it is missing or stale."""
-    src = os.path.join(HERE, "finess_oracle.c")
-    if not os.path.exists(ORACLE_SO) or os.path.getmtime(ORACLE_SO) < os.path.getmtime(src):
+    srcs = [os.path.join(HERE, f) for f in ("finess_oracle.c", "mhd_oracle.c", "finess_oracle.h")]
+    if not os.path.exists(ORACLE_SO) or os.path.getmtime(ORACLE_SO) < max(os.path.getmtime(f) for f in srcs):
         subprocess.check_call(["make", "-s", "-C", HERE], stdout=subprocess.DEVNULL)
 
 
@@ -60,6 +64,19 @@ class Oracle:
         lib.oracle_step_fixed.restype = C.c_int
         lib.oracle_conservation_totals.argtypes = [P, _dp, _dp]
         lib.oracle_face_samples.argtypes = [P, _dp, _dp, np.ctypeslib.ndpointer(np.uint8, flags="C_CONTIGUOUS")]
+        lib.oracle_mhd_set_bnd.argtypes = [P, _dp, _dp]
+        lib.oracle_mhd_global_wave_spd.argtypes = [P, _dp, C.POINTER(C.c_double), C.POINTER(C.c_double)]
+        lib.oracle_mhd_construct_l.argtypes = [P, _dp, _dp, _dp]
+        lib.oracle_mhd_construct_l.restype = C.c_int
+        lib.oracle_mhd_construct_hj_l.argtypes = [P, _dp, _dp, _dp]
+        lib.oracle_mhd_construct_hj_l.restype = C.c_int
+        lib.oracle_mhd_after_step.argtypes = [P, _dp, _dp]
+        lib.oracle_mhd_step_fixed.argtypes = [P, _dp, _dp, C.c_double, C.POINTER(C.c_double)]
+        lib.oracle_mhd_step_fixed.restype = C.c_int
+        lib.oracle_mhd_finsolve.argtypes = [P, _dp, _dp, C.POINTER(C.c_double), C.c_double, _dp,
+                                            C.POINTER(C.c_int)]
+        lib.oracle_mhd_finsolve.restype = C.c_int
+        lib.oracle_orszag_tang.argtypes = [P, _dp, _dp]
         self.lib = lib
 
     def set_bnd(self, p, q):
@@ -133,6 +150,62 @@ class Oracle:
         self.lib.oracle_conservation_totals(C.byref(p), np.ascontiguousarray(q), out)
         return out
 
+    # ---- ideal MHD (mhd_oracle.c) ----
+    def mhd_set_bnd(self, p, q, aux):
+        q = np.ascontiguousarray(q, dtype=np.float64).copy()
+        aux = np.ascontiguousarray(aux, dtype=np.float64).copy()
+        self.lib.oracle_mhd_set_bnd(C.byref(p), q, aux)
+        return q, aux
+
+    def mhd_global_wave_spd(self, p, q):
+        a1, a2 = C.c_double(), C.c_double()
+        self.lib.oracle_mhd_global_wave_spd(C.byref(p), np.ascontiguousarray(q), C.byref(a1), C.byref(a2))
+        return a1.value, a2.value
+
+    def mhd_construct_l(self, p, q, smax=None):
+        L = np.zeros(ghosted_shape(p))
+        sm = np.zeros(smax_shape(p)) if smax is None else np.ascontiguousarray(smax).copy()
+        rc = self.lib.oracle_mhd_construct_l(C.byref(p), np.ascontiguousarray(q), L, sm)
+        if rc:
+            raise ValueError(f"oracle_mhd_construct_l failed: {rc}")
+        return L, sm
+
+    def mhd_construct_hj_l(self, p, q, aux):
+        La = np.zeros(aux_shape(p))
+        rc = self.lib.oracle_mhd_construct_hj_l(C.byref(p), np.ascontiguousarray(q), np.ascontiguousarray(aux), La)
+        if rc:
+            raise ValueError(f"oracle_mhd_construct_hj_l failed: {rc}")
+        return La
+
+    def mhd_after_step(self, p, q, aux):
+        q = np.ascontiguousarray(q, dtype=np.float64).copy()
+        self.lib.oracle_mhd_after_step(C.byref(p), q, np.ascontiguousarray(aux))
+        return q
+
+    def mhd_step_fixed(self, p, q, aux, dt):
+        q = np.ascontiguousarray(q, dtype=np.float64).copy()
+        aux = np.ascontiguousarray(aux, dtype=np.float64).copy()
+        cfl = C.c_double(0.0)
+        rc = self.lib.oracle_mhd_step_fixed(C.byref(p), q, aux, dt, C.byref(cfl))
+        if rc:
+            raise ValueError(f"oracle_mhd_step_fixed failed: {rc}")
+        return q, aux, cfl.value
+
+    def mhd_finsolve(self, p, q, aux, t, tend, dt):
+        q = np.ascontiguousarray(q, dtype=np.float64).copy()
+        aux = np.ascontiguousarray(aux, dtype=np.float64).copy()
+        tt = C.c_double(t)
+        dtv = np.array([0.0, dt, p.max_dt])
+        n = C.c_int(0)
+        rc = self.lib.oracle_mhd_finsolve(C.byref(p), q, aux, C.byref(tt), tend, dtv, C.byref(n))
+        return rc, q, aux, tt.value, dtv[1], n.value
+
+    def orszag_tang(self, p):
+        q = np.zeros(ghosted_shape(p))
+        aux = np.zeros(aux_shape(p))
+        self.lib.oracle_orszag_tang(C.byref(p), q, aux)
+        return q, aux
+
 
 class RefLib:
     """The reference's own compiled sources; available where oracle/_ref was built."""
@@ -192,3 +265,78 @@ class RefLib:
         dtv = np.array([0.0, dt, p.max_dt])
         rc = self.lib.ref_finsolve(p.time_stepping_method, q, C.byref(tt), tend, dtv)
         return rc, q, tt.value, dtv[1]
+
+
+class MhdRefLib:
+    """The reference's own ideal-MHD sources; available where oracle/_ref was built."""
+
+    @staticmethod
+    def available(path=REF_MHD_SO):
+        return os.path.exists(path)
+
+    def __init__(self, path=REF_MHD_SO):
+        lib = C.CDLL(path)
+        lib.ref_mhd_setup.argtypes = [C.POINTER(FinParams)]
+        lib.ref_mhd_qinit.argtypes = [_dp, _dp]
+        lib.ref_mhd_set_bnd.argtypes = [_dp, _dp]
+        lib.ref_mhd_construct_l.argtypes = [_dp, _dp, _dp, _dp]
+        lib.ref_mhd_construct_l.restype = C.c_int
+        lib.ref_mhd_global_wave_spd.argtypes = [_dp, _dp, _dp]
+        lib.ref_mhd_construct_hj_l.argtypes = [_dp, _dp, _dp]
+        lib.ref_mhd_after_step.argtypes = [_dp, _dp]
+        lib.ref_mhd_finsolve.argtypes = [_dp, _dp, C.POINTER(C.c_double), C.c_double, _dp]
+        lib.ref_mhd_finsolve.restype = C.c_int
+        self.lib = lib
+
+    def setup(self, p):
+        self.lib.ref_mhd_setup(C.byref(p))
+
+    def qinit(self, p):
+        self.setup(p)
+        q = np.zeros(ghosted_shape(p))
+        aux = np.zeros(aux_shape(p))
+        self.lib.ref_mhd_qinit(q, aux)
+        return q, aux
+
+    def set_bnd(self, p, q, aux):
+        self.setup(p)
+        q = np.ascontiguousarray(q, dtype=np.float64).copy()
+        aux = np.ascontiguousarray(aux, dtype=np.float64).copy()
+        self.lib.ref_mhd_set_bnd(q, aux)
+        return q, aux
+
+    def global_wave_spd(self, p, q, aux):
+        self.setup(p)
+        out = np.zeros(2)
+        self.lib.ref_mhd_global_wave_spd(np.ascontiguousarray(q), np.ascontiguousarray(aux), out)
+        return out[0], out[1]
+
+    def construct_l(self, p, q, aux, smax=None):
+        self.setup(p)
+        L = np.zeros(ghosted_shape(p))
+        sm = np.zeros(smax_shape(p)) if smax is None else np.ascontiguousarray(smax).copy()
+        rc = self.lib.ref_mhd_construct_l(np.ascontiguousarray(q), np.ascontiguousarray(aux), L, sm)
+        if rc:
+            raise ValueError(f"ref_mhd_construct_l failed: {rc}")
+        return L, sm
+
+    def construct_hj_l(self, p, q, aux):
+        self.setup(p)
+        La = np.zeros(aux_shape(p))
+        self.lib.ref_mhd_construct_hj_l(np.ascontiguousarray(q), np.ascontiguousarray(aux), La)
+        return La
+
+    def after_step(self, p, q, aux):
+        self.setup(p)
+        q = np.ascontiguousarray(q, dtype=np.float64).copy()
+        self.lib.ref_mhd_after_step(q, np.ascontiguousarray(aux))
+        return q
+
+    def finsolve(self, p, q, aux, t, tend, dt):
+        self.setup(p)
+        q = np.ascontiguousarray(q, dtype=np.float64).copy()
+        aux = np.ascontiguousarray(aux, dtype=np.float64).copy()
+        tt = C.c_double(t)
+        dtv = np.array([0.0, dt, p.max_dt])
+        rc = self.lib.ref_mhd_finsolve(q, aux, C.byref(tt), tend, dtv)
+        return rc, q, aux, tt.value, dtv[1]

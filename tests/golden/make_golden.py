@@ -1,11 +1,12 @@
 """Generates the golden fixtures in this directory by running the reference's
-own sources (oracle/_ref/libfinref.so, built by ``make -C oracle ref`` from
-the reference checkout) on small seeded inputs.
+own sources (oracle/_ref/libfinref.so and libfinref_mhd.so, built by
+``make -C oracle ref ref_mhd`` from the reference checkout) on small seeded
+inputs.
 
 The reference repository stores no golden vectors for this path, so these
 files pin its behaviour: each .npz holds the inputs (ghosted q after the BC
 remap, parameters) and the reference's outputs.  Re-run with
-``python tests/golden/make_golden.py`` after ``make -C oracle ref``.
+``python tests/golden/make_golden.py`` after ``make -C oracle ref ref_mhd``.
 """
 import json
 import os
@@ -18,7 +19,7 @@ ROOT = os.path.dirname(os.path.dirname(HERE))
 sys.path.insert(0, ROOT)
 sys.path.insert(0, os.path.join(ROOT, "oracle"))
 
-from oracle import RefLib  # noqa: E402
+from oracle import MhdRefLib, RefLib  # noqa: E402
 from finess_b200 import problems as P  # noqa: E402
 from finess_b200._abi import (FIN_BC_TRANSMISSIVE, FIN_TS_LXW, FIN_TS_MD, FIN_TS_RK, FIN_WENO_FD,  # noqa: E402
                               FIN_WENO_JS, FIN_WENO_Z)
@@ -99,7 +100,48 @@ def main():
         np.savez_compressed(os.path.join(HERE, name + ".npz"), params=params_json(p), q0=q0, q1=q1,
                             t0=t0, t1=t1, tend=tend, dt0=dt, dt1=dt1)
         print("wrote", name, t1, dt1)
+    mhd_main()
+
+
+def mhd_main():
+    """Ideal MHD (apps/2d/mhd/lib with the Orszag-Tang case): ConstructL with
+    the MHD callbacks, ConstructHJ_L_Order1, AfterStep's constrained
+    transport, and whole FinSolveRK frames."""
+    ref = MhdRefLib()
+    rng = np.random.default_rng(20261204)
+    cases = []
+    p = P.orszag_tang_params(n=24, weno=FIN_WENO_JS)
+    cases.append(("mhd_constructl_js_ot24_local", p, ref.qinit(p)))
+    p = P.orszag_tang_params(n=20, weno=FIN_WENO_Z, global_alpha=1)
+    p.my = 18
+    p.yhigh = 2.0
+    cases.append(("mhd_constructl_z_random20x18_global", p, P.mhd_random_state(p, rng)))
+    for name, p, (q, aux) in cases:
+        q, aux = ref.set_bnd(p, q, aux)
+        L, smax = ref.construct_l(p, q, aux)
+        La = ref.construct_hj_l(p, q, aux)
+        qct = ref.after_step(p, q, aux)
+        a1, a2 = ref.global_wave_spd(p, q, aux)
+        np.savez_compressed(os.path.join(HERE, name + ".npz"), params=params_json(p), q=q, aux=aux, L=L,
+                            smax=smax, Laux=La, qct=qct, alpha=np.array([a1, a2]))
+        print("wrote", name)
+    runs = []
+    p = P.orszag_tang_params(n=24, weno=FIN_WENO_JS)
+    runs.append(("mhd_finsolverk_js_ot24", p, 0.0, 0.08, 1e-3))
+    # a large initial dt forces step rejections (FinSolveRK.cpp:343-357 of the MHD app)
+    p = P.orszag_tang_params(n=20, weno=FIN_WENO_Z)
+    runs.append(("mhd_finsolverk_z_ot20_reject", p, 0.0, 0.05, 0.2))
+    for name, p, t0, tend, dt in runs:
+        q0, aux0 = ref.set_bnd(p, *ref.qinit(p))
+        rc, q1, aux1, t1, dt1 = ref.finsolve(p, q0, aux0, t0, tend, dt)
+        assert rc == 0
+        np.savez_compressed(os.path.join(HERE, name + ".npz"), params=params_json(p), q0=q0, aux0=aux0, q1=q1,
+                            aux1=aux1, t0=t0, t1=t1, tend=tend, dt0=dt, dt1=dt1)
+        print("wrote", name, t1, dt1)
 
 
 if __name__ == "__main__":
-    main()
+    if sys.argv[1:] == ["mhd"]:
+        mhd_main()
+    else:
+        main()
