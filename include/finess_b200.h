@@ -282,6 +282,54 @@ const char* fin_batch_last_error(void);
  *     describe them); non-finite speeds are not reported. */
 int fin_construct_l_noalloc(const fin_params* p, const double* q_dev, double* L_dev, void* stream);
 
+/* ---- ideal MHD (physics FIN_PHYS_MHD) ---------------------------------- */
+/* The reference's apps/2d/mhd application path: lib/2d's ConstructL with the
+ * MHD callbacks (apps/2d/mhd/lib/FluxFunc.cpp, SetWaveSpd.cpp,
+ * ProjectLeftEig.cpp, ProjectRightEig.cpp), the potential A3 advanced by the
+ * Hamilton-Jacobi step (ConstructHJ_L.cpp:29-113), constrained transport
+ * (AfterStep.cpp:13-60) and the application's FinSolveRK (SSP-RK3,
+ * FinSolveRK.cpp:17-395) with its CFL number (GetCFL.cpp:31-73); doubly
+ * periodic boundaries (apps/2d/mhd/orszag_tang/SetBndValues.cpp).
+ * fin_params: physics FIN_PHYS_MHD, meqn 8, maux 1, mbc >= 5, time_order 3,
+ * precision FIN_PREC_FP64 or FIN_PREC_FP32.  q arrays are the ghosted
+ * (mx, my, 8) layout above, aux arrays the ghosted (mx, my, 1) layout.
+ * Errors: fin_mhd_last_error(). */
+typedef struct fin_mhd fin_mhd;
+const char* fin_mhd_last_error(void);
+int fin_mhd_create(const fin_params* p, fin_mhd** out);
+int fin_mhd_destroy(fin_mhd* s);
+/* State (interior read; ghosts come from the periodic remap) and its time. */
+int fin_mhd_set_state(fin_mhd* s, const double* q_host, const double* aux_host, double t);
+/* aux_host may be NULL; ghosts are written with the periodic images. */
+int fin_mhd_get_state(fin_mhd* s, double* q_host, double* aux_host, double* t);
+/* ConstructL (lib/2d/ConstructL.cpp:13-408 with the MHD callbacks) on a host
+ * state: L interior written, ghosts untouched; smax_host optional, ghosted
+ * (mx+1, my+1, 2), max-accumulated. */
+int fin_mhd_construct_l(fin_mhd* s, const double* q_host, const double* aux_host, double* L_host,
+                        double* smax_host);
+/* ConstructHJ_L_Order1 (ConstructHJ_L.cpp:29-113): Laux interior written. */
+int fin_mhd_construct_hj_l(fin_mhd* s, const double* q_host, const double* aux_host, double* Laux_host);
+/* AfterStep (AfterStep.cpp:13-60): B1, B2 of q_host rebuilt from aux_host. */
+int fin_mhd_after_step(fin_mhd* s, double* q_host, const double* aux_host);
+/* FinSolveRK of the MHD application from the state's t to tend; dtv as
+ * fin_solve's.  fin_mhd_advance stops after max_steps accepted steps. */
+int fin_mhd_solve(fin_mhd* s, double tend, double* dtv, int* nsteps_out);
+int fin_mhd_advance(fin_mhd* s, double tend, double* dtv, int max_steps, int* nsteps_out);
+/* One step of exactly dt with no CFL control; cfl_out receives GetCFL's value. */
+int fin_mhd_step_fixed(fin_mhd* s, double dt, double* cfl_out);
+/* max over interior cells of |D_x B1 + D_y B2|, D the 4th-order central
+ * difference of the constrained transport (zero to rounding when B is the
+ * transport's curl of A3). */
+int fin_mhd_div_b(fin_mhd* s, double* max_div);
+/* Device time of the last solve/advance/step_fixed call (ms); stage-kernel
+ * times when timing is on; launches since creation; the device state (9
+ * planes: q then A3) and its plane stride. */
+int fin_mhd_last_kernel_ms(fin_mhd* s, double* ms);
+int fin_mhd_set_kernel_timing(fin_mhd* s, int on);
+int fin_mhd_kernel_time(fin_mhd* s, double* ms, long long* launches);
+int fin_mhd_launch_count(fin_mhd* s, long long* launches);
+int fin_mhd_device_state(fin_mhd* s, double** q_dev, size_t* plane_stride);
+
 #ifdef __cplusplus
 }
 #endif

@@ -54,3 +54,15 @@ def test_create_fails_cleanly_without_gpu_or_with_bad_args(lib):
     rc = lib.fin_create(C.byref(bad), C.byref(h))
     assert rc != 0 and not h.value
     assert b"mbc" in lib.fin_last_error()
+
+
+def test_mhd_create_validates_without_gpu(lib):
+    from finess_b200 import problems as P
+    h = C.c_void_p()
+    lib.fin_mhd_last_error.restype = C.c_char_p
+    bad = P.orszag_tang_params(n=16, meqn=5)
+    assert lib.fin_mhd_create(C.byref(bad), C.byref(h)) == 1 and not h.value
+    assert b"meqn 8" in lib.fin_mhd_last_error()
+    bad = P.orszag_tang_params(n=16, mbc=3)
+    assert lib.fin_mhd_create(C.byref(bad), C.byref(h)) == 1
+    assert b"mbc" in lib.fin_mhd_last_error()
