@@ -37,8 +37,19 @@ int merr(int code, const std::string& msg)
             return merr(FIN_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_));    \
     } while (0)
 
-// Tile of the stage kernel: 15 x 16 cells, 511 faces, one per thread.
-using MCfg = MhdCfg<15, 16, 512>;
+// Tile of the stage kernel: 15 x 16 cells, 511 faces.  Threads per block,
+// measured on B200 at 2048^2 (stage ms, fast and slow pairs merged): FP64
+// 256 threads with up to 255 registers and no spills 2.58, 512 threads at
+// 128 registers (~500 B spilled, missing L1 beside 160 KB of shared memory)
+// 2.71; FP32 512 threads 1.50, 256 threads 1.74.
+#ifndef FIN_MHD_NT64
+#define FIN_MHD_NT64 256
+#endif
+#ifndef FIN_MHD_NT32
+#define FIN_MHD_NT32 512
+#endif
+template <class R> struct MCfgOf { using T = MhdCfg<15, 16, FIN_MHD_NT64>; };
+template <> struct MCfgOf<float> { using T = MhdCfg<15, 16, FIN_MHD_NT32>; };
 
 // Reduction slots (doubles): face-speed maxima of the step, then per state
 // buffer its GlobalWaveSpd maxima and its HJ speeds, the status word, and the
@@ -241,7 +252,8 @@ MhdArgs base_args(fin_mhd* s)
 template <class R, int VER, bool P2>
 int launch_t(fin_mhd* s, const MhdArgs& a)
 {
-    constexpr size_t smem = MCfg::smem_bytes<R>();
+    using MCfg = typename MCfgOf<R>::T;
+    constexpr size_t smem = MCfg::template smem_bytes<R>();
     static bool attr = false;
     if (!attr) {
         MCK(cudaFuncSetAttribute(k_mhd_stage<R, VER, P2, MCfg>, cudaFuncAttributeMaxDynamicSharedMemorySize,
