@@ -307,6 +307,75 @@ __device__ __forceinline__ void mhd_left_ent(const MhdFace<R>& f, const R* v, R&
     w4 = v[5];
 }
 
+// The stencil of one face in shared memory: q and the half flux of the six
+// points (normal-frame component order through perm).
+template <class R>
+struct MhdStencil {
+    const R* qs;
+    const R* fl;
+    const int* perm;
+    int qbase, qstr, fbase, fstr, fplane, PQ;
+    R lah;
+};
+
+// One sweep over the stencil: K characteristic values of v+ = 0.5 f + lah q
+// at points 0..4 into p, and of v- = 0.5 f - lah q at points 5..1 into m
+// (reversed), as ConstructL.cpp:179-185 orders them.
+template <class R, int K, class Left>
+__device__ __forceinline__ void mhd_sweep(const MhdStencil<R>& st, const Left& left, R (&p)[K][5], R (&m)[K][5])
+{
+#pragma unroll
+    for (int s = 0; s < 6; s++) {
+        // keep the compiler from hoisting every point's loads ahead of the arithmetic
+        asm volatile("" ::: "memory");
+        const int oq = st.qbase + (s - 3) * st.qstr, of = st.fbase + (s - 3) * st.fstr;
+        R q[MHD_NQ], fh[MHD_NQ];
+#pragma unroll
+        for (int c = 0; c < MHD_NQ; c++) {
+            q[c] = st.qs[st.perm[c] * st.PQ + oq];
+            fh[c] = st.fl[st.perm[c] * st.fplane + of];
+        }
+        if (s < 5) {
+            R v[MHD_NQ], w[K];
+#pragma unroll
+            for (int c = 0; c < MHD_NQ; c++) v[c] = fh[c] + st.lah * q[c];
+            left(v, w);
+#pragma unroll
+            for (int k = 0; k < K; k++) p[k][s] = w[k];
+        }
+        if (s > 0) {
+            R v[MHD_NQ], w[K];
+#pragma unroll
+            for (int c = 0; c < MHD_NQ; c++) v[c] = fh[c] - st.lah * q[c];
+            left(v, w);
+#pragma unroll
+            for (int k = 0; k < K; k++) m[k][5 - s] = w[k];
+        }
+    }
+}
+
+// ghat_k = WENO(p_k) + WENO(m_k) (ConstructL.cpp:191-199) for K fields,
+// FIN_MHD_WGROUP fields at a time between scheduling fences.
+#ifndef FIN_MHD_WGROUP
+#define FIN_MHD_WGROUP 1
+#endif
+template <class R, int VER, bool P2, int K>
+__device__ __forceinline__ void mhd_weno_fields(R (&p)[K][5], R (&m)[K][5], R eps, R pw, R* g)
+{
+    constexpr int G = FIN_MHD_WGROUP < K ? FIN_MHD_WGROUP : K;
+#pragma unroll
+    for (int k0 = 0; k0 < K; k0 += G) {
+#pragma unroll
+        for (int k = k0; k < k0 + G; k++)
+#pragma unroll
+            for (int t = 0; t < 5; t++) { wfence(p[k][t]); wfence(m[k][t]); }
+#pragma unroll
+        for (int k = k0; k < k0 + G; k++) g[k] = weno5<R, VER, P2>(p[k], eps, pw) + weno5<R, VER, P2>(m[k], eps, pw);
+#pragma unroll
+        for (int k = k0; k < k0 + G; k++) wfence(g[k]);
+    }
+}
+
 template <int TI_, int TJ_, int NT_>
 struct MhdCfg {
     static constexpr int TI = TI_, TJ = TJ_, NT = NT_;
@@ -332,11 +401,16 @@ struct MhdCfg {
     }
 };
 
-// The fast and slow pairs share dn, S_u, P and S_b; projecting both in one
-// sweep (40 live values) measured 2.58 / 1.50 ms per FP64 / FP32 stage at
-// 2048^2 against 2.98 / 1.78 for separate sweeps.
-#ifndef FIN_MHD_MERGE_FS
-#define FIN_MHD_MERGE_FS 1
+// Sweeps over the stencil per face: the fast and slow pairs share dn, S_u, P
+// and S_b and take one sweep (40 live values); with FIN_MHD_SWEEPS = 2 the
+// Alfven, entropy and divergence rows take a second (3: one sweep each for
+// the Alfven pair and the entropy/divergence pair).  Stage ms on B200 at
+// 2048^2, FP64 / FP32: a sweep per pair 2.98 / 1.78, three sweeps 2.63 /
+// 1.49, two sweeps 2.36 / 1.26 (FP64 then spills ~130 B to L1, still faster).
+// Evaluating the WENO pairs of two or four fields between one pair of
+// scheduling fences (FIN_MHD_WGROUP) changed nothing measurable.
+#ifndef FIN_MHD_SWEEPS
+#define FIN_MHD_SWEEPS 2
 #endif
 template <class R> struct MhdMinBlocks { static constexpr int value = 1; };
 
@@ -539,77 +613,43 @@ __global__ void __launch_bounds__(Cfg::NT, MhdMinBlocks<R>::value) k_mhd_stage(c
         // lah q at points 0..4, gm from v- = 0.5 f - lah q at points 5..1
         // (ConstructL.cpp:179-199); ghat[k] for the eight waves.
         R ghat[MHD_NQ];
-#if FIN_MHD_MERGE_FS
+        const MhdStencil<R> st{qs, fl, perm, qbase, qstr, fbase, fstr, fplane, PQ, lah};
         {
-            // fast and slow pairs in one sweep over the stencil (40 values)
-            R a0[5], a7[5], a2[5], a5[5], b0[5], b7[5], b2[5], b5[5];
-#pragma unroll
-            for (int s = 0; s < 6; s++) {
-                asm volatile("" ::: "memory");
-                const int oq = qbase + (s - 3) * qstr, of = fbase + (s - 3) * fstr;
-                R q[MHD_NQ], fh[MHD_NQ];
-#pragma unroll
-                for (int m = 0; m < MHD_NQ; m++) {
-                    q[m] = qs[perm[m] * PQ + oq];
-                    fh[m] = fl[perm[m] * fplane + of];
-                }
-                if (s < 5) {
-                    R v[MHD_NQ];
-#pragma unroll
-                    for (int m = 0; m < MHD_NQ; m++) v[m] = fh[m] + lah * q[m];
-                    mhd_left_fs4<R>(f, v, a0[s], a7[s], a2[s], a5[s]);
-                }
-                if (s > 0) {
-                    R v[MHD_NQ];
-#pragma unroll
-                    for (int m = 0; m < MHD_NQ; m++) v[m] = fh[m] - lah * q[m];
-                    mhd_left_fs4<R>(f, v, b0[5 - s], b7[5 - s], b2[5 - s], b5[5 - s]);
-                }
-            }
-            ghat[0] = weno_pair_f<R, VER, P2>(a0, b0, eps, pw);
-            ghat[7] = weno_pair_f<R, VER, P2>(a7, b7, eps, pw);
-            ghat[2] = weno_pair_f<R, VER, P2>(a2, b2, eps, pw);
-            ghat[5] = weno_pair_f<R, VER, P2>(a5, b5, eps, pw);
+            // fast and slow pairs (rows 0, 7, 2, 5) in one sweep
+            R p[4][5], m[4][5];
+            mhd_sweep<R, 4>(st, [&](const R* v, R* w) { mhd_left_fs4<R>(f, v, w[0], w[1], w[2], w[3]); }, p, m);
+            R g[4];
+            mhd_weno_fields<R, VER, P2, 4>(p, m, eps, pw, g);
+            ghat[0] = g[0]; ghat[7] = g[1]; ghat[2] = g[2]; ghat[5] = g[3];
         }
-        constexpr int PASS0 = 2;
+#if FIN_MHD_SWEEPS == 2
+        {
+            // Alfven, entropy and divergence rows (1, 6, 3, 4) in one sweep
+            R p[4][5], m[4][5];
+            mhd_sweep<R, 4>(st, [&](const R* v, R* w) {
+                mhd_left_alf<R>(f, v, w[0], w[1]);
+                mhd_left_ent<R>(f, v, w[2], w[3]);
+            }, p, m);
+            R g[4];
+            mhd_weno_fields<R, VER, P2, 4>(p, m, eps, pw, g);
+            ghat[1] = g[0]; ghat[6] = g[1]; ghat[3] = g[2]; ghat[4] = g[3];
+        }
 #else
-        constexpr int PASS0 = 0;
-#endif
+        // the Alfven pair, then the entropy and divergence rows: one loop
+        // body for both sweeps
 #pragma unroll 1
-        for (int pass = PASS0; pass < 4; pass++) {
-            R pm[5], pp[5], mm[5], mp[5];
-#pragma unroll
-            for (int s = 0; s < 6; s++) {
-                asm volatile("" ::: "memory");
-                const int oq = qbase + (s - 3) * qstr, of = fbase + (s - 3) * fstr;
-                R q[MHD_NQ], fh[MHD_NQ];
-#pragma unroll
-                for (int m = 0; m < MHD_NQ; m++) {
-                    q[m] = qs[perm[m] * PQ + oq];
-                    fh[m] = fl[perm[m] * fplane + of];
-                }
-#pragma unroll
-                for (int sg = 0; sg < 2; sg++) {
-                    if ((sg == 0 && s == 5) || (sg == 1 && s == 0)) continue;
-                    R v[MHD_NQ];
-#pragma unroll
-                    for (int m = 0; m < MHD_NQ; m++) v[m] = sg == 0 ? fh[m] + lah * q[m] : fh[m] - lah * q[m];
-                    R w0, w1;
-                    if (pass < 2) mhd_left_fs<R>(f, pass, v, w0, w1);
-                    else if (pass == 2) mhd_left_alf<R>(f, v, w0, w1);
-                    else mhd_left_ent<R>(f, v, w0, w1);
-                    if (sg == 0) { pm[s] = w0; pp[s] = w1; }
-                    else { mm[5 - s] = w0; mp[5 - s] = w1; }
-                }
-            }
-            const R g0 = weno_pair_f<R, VER, P2>(pm, mm, eps, pw);
-            const R g1 = weno_pair_f<R, VER, P2>(pp, mp, eps, pw);
-            // wave numbering of ProjectLeftEig.cpp:92-174
-            if (pass == 0) { ghat[0] = g0; ghat[7] = g1; }
-            else if (pass == 1) { ghat[2] = g0; ghat[5] = g1; }
-            else if (pass == 2) { ghat[1] = g0; ghat[6] = g1; }
-            else { ghat[3] = g0; ghat[4] = g1; }
+        for (int pass = 0; pass < 2; pass++) {
+            R p[2][5], m[2][5];
+            mhd_sweep<R, 2>(st, [&](const R* v, R* w) {
+                if (pass == 0) mhd_left_alf<R>(f, v, w[0], w[1]);
+                else mhd_left_ent<R>(f, v, w[0], w[1]);
+            }, p, m);
+            R g[2];
+            mhd_weno_fields<R, VER, P2, 2>(p, m, eps, pw, g);
+            if (pass == 0) { ghat[1] = g[0]; ghat[6] = g[1]; }
+            else { ghat[3] = g[0]; ghat[4] = g[1]; }
         }
+#endif
 
         // Right projection (ProjectRightEig.cpp:89-203) in the normal frame.
         R Fo[MHD_NQ];
