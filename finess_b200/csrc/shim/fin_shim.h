@@ -17,6 +17,11 @@
 // SetBndValues (see fin_shim_common.cpp).
 fin_solver* fin_shim_solver();
 
+// The fin_params fields held by global_ini_params, and the boundary
+// conditions read off the application's SetBndValues.
+void fin_shim_params(fin_params* out);
+void fin_shim_probe_bc(int mx, int my, int mbc, int meqn, int maux, int* bc);
+
 // dTensorBC3 <-> contiguous ghosted buffer in the same (i, j, m) order.
 void fin_shim_pack(const dTensorBC3& t, std::vector<double>& buf);
 void fin_shim_unpack_interior(const std::vector<double>& buf, dTensorBC3& t);

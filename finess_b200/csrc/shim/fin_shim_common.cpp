@@ -47,7 +47,31 @@ void fin_shim_check(int rc, const char* where)
     exit(1);
 }
 
-fin_solver* fin_shim_solver()
+// Reads every side's boundary condition off the application's SetBndValues
+// (probe state of meqn components, maux aux components).  Returns 0, or
+// prints and exits as the reference's terminate paths do.
+void fin_shim_probe_bc(int mx, int my, int mbc, int meqn, int maux, int* bc)
+{
+    StateVars probe(0.0, mx, my, meqn, (maux > 0 ? maux : 1), mbc);
+    dTensorBC3& q = probe.ref_q();
+    const double sy = my + 2 * mbc;
+    for (int i = 1; i <= mx; i++)
+        for (int j = 1; j <= my; j++)
+            for (int m = 1; m <= meqn; m++) q.set(i, j, m, i * sy + j);
+    SetBndValues(probe);
+    for (int side = 0; side < 4; side++) {
+        const int k = classify(q, side, mx, my, mbc);
+        if (k < 0) {
+            printf(" Error: SetBndValues side %d is neither periodic nor zeroth-order extrapolation;"
+                   " this library remaps only those two\n", side);
+            exit(1);
+        }
+        bc[side] = k;
+    }
+}
+
+// The fields of fin_params the application's global_ini_params holds.
+void fin_shim_params(fin_params* out)
 {
     const IniParams& g = global_ini_params;
     fin_params p;
@@ -67,29 +91,19 @@ fin_solver* fin_shim_solver()
     else p.weno_version = FIN_WENO_FD;
     p.epsilon = g.get_epsilon(); p.power_param = g.get_power_param(); p.alpha_scaling = g.get_alpha_scaling();
     p.gamma = g.get_gamma();
+    *out = p;
+}
+
+fin_solver* fin_shim_solver()
+{
+    fin_params p;
+    fin_shim_params(&p);
     // The solver is kept while the grid and method stay the same.
     if (g_solver && memcmp(&p, &g_key, sizeof(p)) == 0) return g_solver;
     g_key = p;
-    // Probe the application's SetBndValues.
-    {
-        StateVars probe(0.0, p.mx, p.my, p.meqn, (p.maux > 0 ? p.maux : 1), p.mbc);
-        dTensorBC3& q = probe.ref_q();
-        const double sy = p.my + 2 * p.mbc;
-        for (int i = 1; i <= p.mx; i++)
-            for (int j = 1; j <= p.my; j++)
-                for (int m = 1; m <= p.meqn; m++) q.set(i, j, m, i * sy + j);
-        SetBndValues(probe);
-        int* bc[4] = {&p.bc_xlow, &p.bc_xhigh, &p.bc_ylow, &p.bc_yhigh};
-        for (int side = 0; side < 4; side++) {
-            const int k = classify(q, side, p.mx, p.my, p.mbc);
-            if (k < 0) {
-                printf(" Error: SetBndValues side %d is neither periodic nor zeroth-order extrapolation;"
-                       " this library remaps only those two\n", side);
-                exit(1);
-            }
-            *bc[side] = k;
-        }
-    }
+    int bc[4];
+    fin_shim_probe_bc(p.mx, p.my, p.mbc, p.meqn, p.maux, bc);
+    p.bc_xlow = bc[0]; p.bc_xhigh = bc[1]; p.bc_ylow = bc[2]; p.bc_yhigh = bc[3];
     if (g_solver) fin_destroy(g_solver);
     g_solver = nullptr;
     fin_shim_check(fin_create(&p, &g_solver), "fin_create");

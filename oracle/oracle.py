@@ -33,6 +33,8 @@ REF_SO = os.path.join(HERE, "_ref", "libfinref.so")
 # the same reference objects relinked against libfinb200.so through the shim
 REF_SHIM_SO = os.path.join(HERE, "_ref", "libfinref_shim.so")
 REF_MHD_SO = os.path.join(HERE, "_ref", "libfinref_mhd.so")
+# the MHD application's objects relinked against libfinb200.so (its FinSolveRK replaced)
+REF_MHD_SHIM_SO = os.path.join(HERE, "_ref", "libfinref_mhd_shim.so")
 
 
 def build_oracle():

@@ -1,8 +1,10 @@
 """The drop-in boundary end to end: the reference's own driver objects (the
 same objects as oracle/_ref/libfinref.so) relinked against libfinb200.so
 through the relink shim, which replaces ConstructL.o, GlobalWaveSpd.o and
-FinSolveRK.o by name as an application Makefile would.  Its results must
-match the golden fixtures the unmodified reference produced."""
+FinSolveRK.o by name as an application Makefile would; likewise the MHD
+application's objects (oracle/_ref/libfinref_mhd.so) with its FinSolveRK.o
+replaced.  Their results must match the golden fixtures the unmodified
+reference produced."""
 import os
 
 import numpy as np
@@ -39,5 +41,26 @@ def test_relinked_finsolve_rk(shimlib, path):
     rc, q1, t1, dt1 = shimlib.finsolve(p, g["q0"], float(g["t0"]), float(g["tend"]), float(g["dt0"]))
     assert rc == 0
     assert rel_linf(interior(p, q1), interior(p, g["q1"])) <= 1e-11
+    assert abs(t1 - float(g["t1"])) <= 1e-14 * abs(float(g["t1"]))
+    assert abs(dt1 - float(g["dt1"])) <= 1e-10 * float(g["dt1"])
+
+
+@pytest.fixture(scope="module")
+def mhdshim():
+    from oracle import REF_MHD_SHIM_SO, MhdRefLib
+    if not MhdRefLib.available(REF_MHD_SHIM_SO):
+        pytest.skip("oracle/_ref/libfinref_mhd_shim.so not built (needs the reference checkout)")
+    return MhdRefLib(REF_MHD_SHIM_SO)
+
+
+@pytest.mark.parametrize("path", golden_cases("mhd_finsolverk_"))
+def test_relinked_mhd_finsolve_rk(mhdshim, path):
+    g = load_golden(path)
+    p = g["p"]
+    rc, q1, aux1, t1, dt1 = mhdshim.finsolve(p, g["q0"], g["aux0"], float(g["t0"]), float(g["tend"]),
+                                             float(g["dt0"]))
+    assert rc == 0
+    assert rel_linf(interior(p, q1), interior(p, g["q1"])) <= 1e-11
+    assert rel_linf(interior(p, aux1), interior(p, g["aux1"])) <= 1e-11
     assert abs(t1 - float(g["t1"])) <= 1e-14 * abs(float(g["t1"]))
     assert abs(dt1 - float(g["dt1"])) <= 1e-10 * float(g["dt1"])
