@@ -1,6 +1,6 @@
-// Kernels of the hybrid form: the per-step troubled-face indicator (features
-// -> network on tcgen05 tensor cores -> one flag byte per face), the
-// training-sample extractor, and the judge step's state comparison.
+// The hybrid form's per-step troubled-face indicator: features -> network on
+// tcgen05 tensor cores -> a bit mask of troubled faces.  (The training-sample
+// extractor and the judge step's state comparison are in finess_b200.cu.)
 #pragma once
 #include "fin_indicator.cuh"
 #include "fin_mlp.cuh"
@@ -269,58 +269,6 @@ __global__ void __launch_bounds__(Cfg::NT, 3) k_indicator(const __grid_constant_
     }
     tc::fence_after_sync();
     if (warp == 0) tc::tmem_free(tmem, 128);
-}
-
-// Training samples: features and labels of faces f0, f0 + stride, ...
-__global__ void k_face_samples(const double* q, size_t plane, int mx, int my, int bc0, int bc1, int bc2, int bc3,
-                               double gamma, double eps, double pw, double ascale, const double* alpha_g,
-                               long long f0, long long stride, long long n, float* X, unsigned char* y)
-{
-    const int bc[4] = {bc0, bc1, bc2, bc3};
-    for (long long s = blockIdx.x * (long long)blockDim.x + threadIdx.x; s < n; s += (long long)gridDim.x * blockDim.x) {
-        const long long f = f0 + s * stride;
-        bool isx;
-        int i, j;
-        ind::face_of(f, mx, my, isx, i, j);
-        float x[ind::NFEAT];
-        ind::face_features<float>(q, plane, mx, my, bc, float(gamma), isx, i, j, x);
-#pragma unroll
-        for (int k = 0; k < ind::NFEAT; k++) X[s * ind::NFEAT + k] = x[k];
-        const double ag = alpha_g ? alpha_g[isx ? 0 : 1] : 0.0;
-        y[s] = ind::face_label(q, plane, mx, my, bc, gamma, eps, pw, ascale, ag, isx, i, j);
-    }
-}
-
-// max |a - b| and max |b| over all planes' interior values (judge step).
-__global__ void k_max_diff(const double* a, const double* b, size_t plane, size_t n, double* out)
-{
-    __shared__ double red[2][32];
-    double d = 0.0, m = 0.0;
-    for (size_t g = blockIdx.x * size_t(blockDim.x) + threadIdx.x; g < n; g += size_t(gridDim.x) * blockDim.x) {
-#pragma unroll
-        for (int c = 0; c < MEQN; c++) {
-            const double va = a[c * plane + g], vb = b[c * plane + g];
-            const double dd = fabs(va - vb);
-            d = dd > d || dd != dd ? dd : d;     // NaN wins
-            m = Max(m, fabs(vb));
-        }
-    }
-    for (int o = 16; o > 0; o >>= 1) {
-        const double od = __shfl_xor_sync(0xffffffffu, d, o);
-        d = od > d || od != od ? od : d;
-        m = Max(m, __shfl_xor_sync(0xffffffffu, m, o));
-    }
-    const int w = threadIdx.x >> 5, nw = blockDim.x >> 5;
-    if ((threadIdx.x & 31) == 0) { red[0][w] = d; red[1][w] = m; }
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        for (int k = 0; k < nw; k++) {
-            d = red[0][k] > d || red[0][k] != red[0][k] ? red[0][k] : d;
-            m = Max(m, red[1][k]);
-        }
-        atomic_max_nonneg(out, d != d ? __longlong_as_double(0x7ff0000000000000ll) : d);
-        atomic_max_nonneg(out + 1, m);
-    }
 }
 
 }  // namespace fin

@@ -13,10 +13,12 @@
 #include <cstdio>
 #include <cstring>
 #include <string>
+#include <utility>
 #include <vector>
 #include "finess_b200.h"
 #include "fin_weno_face.cuh"
 #include "fin_mhd.cuh"
+#include "fin_mhd_hyb.cuh"
 
 using namespace fin;
 
@@ -54,8 +56,13 @@ template <> struct MCfgOf<float> { using T = MhdCfg<15, 16, FIN_MHD_NT32>; };
 // Reduction slots (doubles): face-speed maxima of the step, then per state
 // buffer its GlobalWaveSpd maxima and its HJ speeds, the status word, and the
 // divergence diagnostic.
-enum { MNBUF = 4, MS_SMAX = 0, MS_ALPHA = 2, MS_HJ = MS_ALPHA + 2 * MNBUF, MS_STATUS = MS_HJ + 2 * MNBUF,
-       MS_DIV = MS_STATUS + 1, MS_N = MS_DIV + 1 };
+// Buffer 4 is the hybrid form's judge buffer.  SMAX_ALT keeps the hybrid
+// attempt's face-speed maxima while a judge step recomputes with full WENO;
+// DIFF receives the judge's max |q_hybrid - q_full| and max |q_full|.
+enum { MNBUF = 5, MS_SMAX = 0, MS_ALPHA = 2, MS_HJ = MS_ALPHA + 2 * MNBUF, MS_STATUS = MS_HJ + 2 * MNBUF,
+       MS_DIV = MS_STATUS + 1, MS_SMAX_ALT = MS_DIV + 1, MS_DIFF = MS_SMAX_ALT + 2, MS_N = MS_DIFF + 2 };
+// The indicator's tile (the stage kernel's 15 x 16, 256 threads).
+using ICfg = MhdCfg<15, 16, 256>;
 
 int grid_blocks(size_t n)
 {
@@ -88,6 +95,20 @@ struct fin_mhd {
     double t;
     bool max_valid;         // slots hold the maxima of q[cur]
     long long launches;
+    // hybrid form
+    float* mlpP;            // network parameters on the device
+    unsigned* flags;        // troubled-face bit masks of the current indicator pass
+    unsigned long long* ind_count;
+    float zthr;
+    int judge_every;
+    double judge_tol;
+    int ind_every, ind_since, hyb_off;
+    bool judge_pending;
+    long long hstep, judges, reverts, troubled_last, faces;
+    cudaEvent_t iev[2];
+    bool ind_timed;
+    double ind_ms;
+    long long ind_launches;
 };
 
 namespace fin {
@@ -178,6 +199,38 @@ __global__ void k_mhd_div_b(const double* q, int mx, int my, size_t plane, doubl
     }
 }
 
+// max |a - b| and max |b| over the 9 planes (judge step); a NaN difference wins.
+__global__ void k_mhd_max_diff(const double* a, const double* b, size_t plane, size_t n, double* out)
+{
+    __shared__ double red[2][32];
+    double d = 0.0, m = 0.0;
+    for (size_t g = blockIdx.x * size_t(blockDim.x) + threadIdx.x; g < n; g += size_t(gridDim.x) * blockDim.x) {
+#pragma unroll
+        for (int c = 0; c < MHD_NP; c++) {
+            const double va = a[c * plane + g], vb = b[c * plane + g];
+            const double dd = fabs(va - vb);
+            d = dd > d || dd != dd ? dd : d;
+            m = Max(m, fabs(vb));
+        }
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+        const double od = __shfl_xor_sync(0xffffffffu, d, o);
+        d = od > d || od != od ? od : d;
+        m = Max(m, __shfl_xor_sync(0xffffffffu, m, o));
+    }
+    const int w = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    if ((threadIdx.x & 31) == 0) { red[0][w] = d; red[1][w] = m; }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        for (int k = 0; k < nw; k++) {
+            d = red[0][k] > d || red[0][k] != red[0][k] ? red[0][k] : d;
+            m = Max(m, red[1][k]);
+        }
+        atomic_max_nonneg(out, d != d ? __longlong_as_double(0x7ff0000000000000ll) : d);
+        atomic_max_nonneg(out + 1, m);
+    }
+}
+
 // Reference ghosted AoS q (8 components) and aux (1) -> the 9 interior planes.
 __global__ void k_mhd_aos_to_planes(const double* q, const double* aux, double* planes, int mx, int my, int mbc,
                                     size_t plane)
@@ -249,39 +302,46 @@ MhdArgs base_args(fin_mhd* s)
     return a;
 }
 
-template <class R, int VER, bool P2>
+template <class R, int VER, bool P2, bool HYB>
 int launch_t(fin_mhd* s, const MhdArgs& a)
 {
     using MCfg = typename MCfgOf<R>::T;
-    constexpr size_t smem = MCfg::template smem_bytes<R>();
+    constexpr size_t smem = HYB ? MCfg::template smem_bytes_hyb<R>() : MCfg::template smem_bytes<R>();
     static bool attr = false;
     if (!attr) {
-        MCK(cudaFuncSetAttribute(k_mhd_stage<R, VER, P2, MCfg>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+        MCK(cudaFuncSetAttribute(k_mhd_stage<R, VER, P2, MCfg, HYB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  int(smem)));
         attr = true;
     }
     dim3 grid((s->p.my + MCfg::TJ - 1) / MCfg::TJ, (s->p.mx + MCfg::TI - 1) / MCfg::TI);
-    k_mhd_stage<R, VER, P2, MCfg><<<grid, MCfg::NT, smem, s->stream>>>(a);
+    k_mhd_stage<R, VER, P2, MCfg, HYB><<<grid, MCfg::NT, smem, s->stream>>>(a);
     s->launches++;
     MCK(cudaGetLastError());
     return FIN_OK;
 }
 
-template <class R>
+template <class R, bool HYB>
 int launch_r(fin_mhd* s, const MhdArgs& a)
 {
     const bool p2 = s->p.power_param == 2.0;
     switch (s->p.weno_version) {
-        case FIN_WENO_JS: return p2 ? launch_t<R, FIN_WENO_JS, true>(s, a) : launch_t<R, FIN_WENO_JS, false>(s, a);
-        case FIN_WENO_Z: return p2 ? launch_t<R, FIN_WENO_Z, true>(s, a) : launch_t<R, FIN_WENO_Z, false>(s, a);
-        default: return launch_t<R, FIN_WENO_FD, true>(s, a);
+        case FIN_WENO_JS:
+            return p2 ? launch_t<R, FIN_WENO_JS, true, HYB>(s, a) : launch_t<R, FIN_WENO_JS, false, HYB>(s, a);
+        case FIN_WENO_Z:
+            return p2 ? launch_t<R, FIN_WENO_Z, true, HYB>(s, a) : launch_t<R, FIN_WENO_Z, false, HYB>(s, a);
+        default: return launch_t<R, FIN_WENO_FD, true, HYB>(s, a);
     }
 }
 
+// A stage in the solver's form: FP64, FP32, or (hybrid) FP32 with the
+// per-face choice when a.flags is set and full FP32 WENO otherwise.
 int launch_stage(fin_mhd* s, const MhdArgs& a, int k)
 {
     if (s->time_kernels) MCK(cudaEventRecord(s->kev[2 * k], s->stream));
-    const int rc = s->p.precision == FIN_PREC_FP32 ? launch_r<float>(s, a) : launch_r<double>(s, a);
+    int rc;
+    if (s->p.precision == FIN_PREC_FP64) rc = launch_r<double, false>(s, a);
+    else if (a.flags) rc = launch_r<float, true>(s, a);
+    else rc = launch_r<float, false>(s, a);
     if (rc) return rc;
     if (s->time_kernels) MCK(cudaEventRecord(s->kev[2 * k + 1], s->stream));
     return FIN_OK;
@@ -289,6 +349,14 @@ int launch_stage(fin_mhd* s, const MhdArgs& a, int k)
 
 int collect_times(fin_mhd* s, int nk)
 {
+    if (s->ind_timed) {
+        float ms = 0.f;
+        MCK(cudaEventSynchronize(s->iev[1]));
+        MCK(cudaEventElapsedTime(&ms, s->iev[0], s->iev[1]));
+        s->ind_ms += ms;
+        s->ind_launches++;
+        s->ind_timed = false;
+    }
     if (!s->time_kernels) return FIN_OK;
     MCK(cudaEventSynchronize(s->kev[2 * nk - 1]));
     for (int k = 0; k < nk; k++) {
@@ -356,14 +424,15 @@ int upload(fin_mhd* s, const double* q_host, const double* aux_host, int buf)
     return FIN_OK;
 }
 
-// The three stages of one step of size dt from q[cur] into q[nxt]
-// (FinSolveRK.cpp:176-219 of the MHD application with SetRKinfo.cpp:50-64).
-int take_stages(fin_mhd* s, double dt, int nxt)
+// The three stages of one step of size dt from q[cur] into q[out] through
+// the stage registers q1, q2 (FinSolveRK.cpp:176-219 of the MHD application
+// with SetRKinfo.cpp:50-64); flags: the hybrid form's troubled-face masks
+// (nullptr: full WENO).
+int stages(fin_mhd* s, double dt, int q1, int q2, int out, const unsigned* flags)
 {
-    const int qn = s->cur, q1 = (s->cur + 1) % 4, q2 = (s->cur + 2) % 4;
+    const int qn = s->cur;
     MCK(cudaMemsetAsync(s->slots + MS_SMAX, 0, 2 * sizeof(double), s->stream));
-    MCK(cudaMemsetAsync(s->slots + MS_STATUS, 0, sizeof(double), s->stream));
-    for (int b : {q1, q2, nxt}) {
+    for (int b : {q1, q2, out}) {
         MCK(cudaMemsetAsync(alpha_slot(s, b), 0, 2 * sizeof(double), s->stream));
         MCK(cudaMemsetAsync(hj_slot(s, b), 0, 2 * sizeof(double), s->stream));
     }
@@ -371,6 +440,7 @@ int take_stages(fin_mhd* s, double dt, int nxt)
     int rc;
     MhdArgs a = base_args(s);
     a.smax_out = s->slots + MS_SMAX;
+    a.flags = flags;
     // stage 1: Qstar = 1*Qnew + 0*Qstar + (1*dt) (L, Laux)(Qnew), then AfterStep
     a.qin = s->q[qn]; a.A = s->q[qn]; a.B = nullptr; a.qout = s->q[q1];
     a.a1 = 1.0; a.a2 = 0.0; a.bdt = 1.0 * dt;
@@ -384,11 +454,111 @@ int take_stages(fin_mhd* s, double dt, int nxt)
     a.alpha_out = alpha_slot(s, q2); a.hj_out = hj_slot(s, q2);
     if ((rc = launch_stage(s, a, 1))) return rc;
     // stage 3: Qnew = (2/3) Qstar + (1/3) Qnew + ((2/3) dt) (L, Laux)(Qstar)
-    a.qin = s->q[q2]; a.A = s->q[q2]; a.B = s->q[qn]; a.qout = s->q[nxt];
+    a.qin = s->q[q2]; a.A = s->q[q2]; a.B = s->q[qn]; a.qout = s->q[out];
     a.a1 = 2.0e0 / 3.0e0; a.a2 = 1.0e0 / 3.0e0; a.bdt = (2.0e0 / 3.0e0) * dt;
     a.alpha_in = ga ? alpha_slot(s, q2) : nullptr; a.hj_in = hj_slot(s, q2);
-    a.alpha_out = alpha_slot(s, nxt); a.hj_out = hj_slot(s, nxt);
+    a.alpha_out = alpha_slot(s, out); a.hj_out = hj_slot(s, out);
     return launch_stage(s, a, 2);
+}
+
+// Troubled-face flags of q[buf] (fin_mhd_hyb.cuh).
+int launch_indicator(fin_mhd* s, int buf)
+{
+    MhdIndArgs ia;
+    memset(&ia, 0, sizeof(ia));
+    ia.m = base_args(s);
+    ia.m.qin = s->q[buf];
+    ia.P = s->mlpP;
+    ia.zthr = s->zthr;
+    ia.flags = s->flags;
+    ia.count = s->ind_count;
+    static bool configured = false;
+    const size_t smem = sizeof(MhdIndTile<ICfg>);
+    if (!configured) {
+        MCK(cudaFuncSetAttribute(k_mhd_indicator<ICfg>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
+        configured = true;
+    }
+    MCK(cudaMemsetAsync(s->ind_count, 0, sizeof(unsigned long long), s->stream));
+    MCK(cudaMemsetAsync(s->flags, 0, flag_words(s->p.mx, s->p.my) * sizeof(unsigned), s->stream));
+    const long long tiles = (long long)((s->p.mx + ICfg::TI - 1) / ICfg::TI) * ((s->p.my + ICfg::TJ - 1) / ICfg::TJ);
+    const int grid = int(tiles < 148 * 2 ? tiles : 148 * 2);
+    k_mhd_indicator<ICfg><<<grid, ICfg::NT, smem, s->stream>>>(ia);
+    s->launches++;
+    s->faces = (long long)(s->p.mx + 1) * s->p.my + (long long)s->p.mx * (s->p.my + 1);
+    MCK(cudaGetLastError());
+    return FIN_OK;
+}
+
+// One step from q[cur] into q[nxt].  Hybrid form with a network: flags from
+// the indicator on q^n when due, FP32 stages with the per-face choice; every
+// judge_every-th such step also the full-WENO FP32 step from the same q^n
+// into q[4], compared on the device (settled by settle_judge).
+int take_stages(fin_mhd* s, double dt, int nxt)
+{
+    const int q1 = (s->cur + 1) % 4, q2 = (s->cur + 2) % 4;
+    s->judge_pending = false;
+    MCK(cudaMemsetAsync(s->slots + MS_STATUS, 0, sizeof(double), s->stream));
+    if (s->p.precision != FIN_PREC_HYBRID || !s->mlpP) return stages(s, dt, q1, q2, nxt, nullptr);
+    if (s->hyb_off > 0) {
+        s->hyb_off--;
+        return stages(s, dt, q1, q2, nxt, nullptr);
+    }
+    int rc;
+    if (s->ind_since < 0 || s->ind_since >= s->ind_every) {
+        if (s->time_kernels) MCK(cudaEventRecord(s->iev[0], s->stream));
+        if ((rc = launch_indicator(s, s->cur))) return rc;
+        if (s->time_kernels) {
+            MCK(cudaEventRecord(s->iev[1], s->stream));
+            s->ind_timed = true;
+        }
+        s->ind_since = 0;
+    }
+    if ((rc = stages(s, dt, q1, q2, nxt, s->flags))) return rc;
+    s->hstep++;
+    if (s->judge_every > 0 && s->hstep % s->judge_every == 0) {
+        MCK(cudaMemcpyAsync(s->slots + MS_SMAX_ALT, s->slots + MS_SMAX, 2 * sizeof(double), cudaMemcpyDeviceToDevice,
+                            s->stream));
+        const bool tk = s->time_kernels;   // the step's stage times stay those of the hybrid stages
+        s->time_kernels = false;
+        rc = stages(s, dt, q1, q2, 4, nullptr);
+        s->time_kernels = tk;
+        if (rc) return rc;
+        MCK(cudaMemsetAsync(s->slots + MS_DIFF, 0, 2 * sizeof(double), s->stream));
+        const size_t n = size_t(s->p.mx) * s->p.my;
+        k_mhd_max_diff<<<grid_blocks(n), 256, 0, s->stream>>>(s->q[nxt], s->q[4], s->plane, n, s->slots + MS_DIFF);
+        s->launches++;
+        MCK(cudaGetLastError());
+        s->judge_pending = true;
+    }
+    return FIN_OK;
+}
+
+// After get_cfl brought the slots to the host: settle a judge step.  The
+// hybrid result stays (with its face-speed maxima) unless it differs from
+// the full-WENO result by more than judge_tol (relative L-infinity); then
+// the full result takes its place, its maxima give the CFL, and the
+// indicator stays off for judge_every steps.
+void settle_judge(fin_mhd* s, int nxt, double dt, double* cfl)
+{
+    if (!s->judge_pending) return;
+    s->judges++;
+    const double d = s->h_slots[MS_DIFF], m = s->h_slots[MS_DIFF + 1];
+    const bool revert = !(d <= s->judge_tol * (m > 0 ? m : 1.0));
+    double sm;
+    if (revert) {
+        s->reverts++;
+        s->hyb_off = s->judge_every;
+        s->ind_since = -1;
+        std::swap(s->q[4], s->q[nxt]);
+        cudaMemcpyAsync(alpha_slot(s, nxt), alpha_slot(s, 4), 2 * sizeof(double), cudaMemcpyDeviceToDevice, s->stream);
+        cudaMemcpyAsync(hj_slot(s, nxt), hj_slot(s, 4), 2 * sizeof(double), cudaMemcpyDeviceToDevice, s->stream);
+        sm = Max(s->h_slots[MS_SMAX], s->h_slots[MS_SMAX + 1]);
+    } else {
+        sm = Max(s->h_slots[MS_SMAX_ALT], s->h_slots[MS_SMAX_ALT + 1]);
+    }
+    double c = -100.0;
+    c = Max(c, dt * sm * (1.0 / s->dx + 1.0 / s->dy));
+    *cfl = c;
 }
 
 // GetCFL of the MHD application (GetCFL.cpp:31-73): the largest
@@ -400,6 +570,7 @@ int get_cfl(fin_mhd* s, double dt, double dtmax, double* cfl, bool* nonfinite)
     int rc = read_status(s, &st);
     if (rc) return rc;
     *nonfinite = (st & 1u) != 0;
+    if (st & 4u) return merr(FIN_ERR_CUDA, "a bounded tensor-core wait of the indicator ran out");
     if (dt > dtmax) return merr(FIN_ERR_DT_BOUNDS, "dt is out of bounds");
     const double sm = Max(s->h_slots[MS_SMAX], s->h_slots[MS_SMAX + 1]);
     double c = -100.0;
@@ -426,8 +597,8 @@ int validate(const fin_params* p)
         if (b != FIN_BC_PERIODIC) return merr(FIN_ERR_UNSUPPORTED, "the MHD path has doubly periodic boundaries");
     if (p->source_term) return merr(FIN_ERR_UNSUPPORTED, "source terms are not built");
     if (!(p->xhigh > p->xlow) || !(p->yhigh > p->ylow)) return merr(FIN_ERR_ARG, "empty domain");
-    if (p->precision != FIN_PREC_FP64 && p->precision != FIN_PREC_FP32)
-        return merr(FIN_ERR_UNSUPPORTED, "the MHD path has the FP64 and FP32 forms");
+    if (p->precision != FIN_PREC_FP64 && p->precision != FIN_PREC_FP32 && p->precision != FIN_PREC_HYBRID)
+        return merr(FIN_ERR_ARG, "unknown precision form");
     return FIN_OK;
 }
 
@@ -446,11 +617,16 @@ int fin_mhd_destroy(fin_mhd* s)
     cudaFree(s->d_aos);
     cudaFree(s->d_face_x);
     cudaFree(s->d_face_y);
+    cudaFree(s->mlpP);
+    cudaFree(s->flags);
+    cudaFree(s->ind_count);
     if (s->h_slots) cudaFreeHost(s->h_slots);
     if (s->ev0) cudaEventDestroy(s->ev0);
     if (s->ev1) cudaEventDestroy(s->ev1);
     for (int k = 0; k < 6; k++)
         if (s->kev[k]) cudaEventDestroy(s->kev[k]);
+    for (int k = 0; k < 2; k++)
+        if (s->iev[k]) cudaEventDestroy(s->iev[k]);
     if (s->stream) cudaStreamDestroy(s->stream);
     delete s;
     return FIN_OK;
@@ -479,9 +655,20 @@ int fin_mhd_create(const fin_params* p, fin_mhd** out)
         return merr(FIN_ERR_CUDA, std::string(what) + ": " + cudaGetErrorString(e));
     };
     cudaError_t e;
-    for (int b = 0; b < MNBUF; b++)
+    const int nbuf = p->precision == FIN_PREC_HYBRID ? 5 : 4;
+    for (int b = 0; b < nbuf; b++)
         if ((e = cudaMalloc(&s->q[b], MHD_NP * s->plane * sizeof(double))) != cudaSuccess)
             return fail(e, "cudaMalloc state");
+    if (p->precision == FIN_PREC_HYBRID) {
+        if ((e = cudaMalloc(&s->flags, flag_words(p->mx, p->my) * sizeof(unsigned))) != cudaSuccess)
+            return fail(e, "cudaMalloc flags");
+        if ((e = cudaMalloc(&s->ind_count, 16)) != cudaSuccess) return fail(e, "cudaMalloc counter");
+        if ((e = cudaMemset(s->ind_count, 0, 16)) != cudaSuccess) return fail(e, "memset");
+        s->judge_every = 50;
+        s->judge_tol = 1e-3;
+        s->ind_every = 1;
+        s->ind_since = -1;
+    }
     if ((e = cudaMalloc(&s->slots, MS_N * sizeof(double))) != cudaSuccess) return fail(e, "cudaMalloc slots");
     s->status = reinterpret_cast<unsigned int*>(s->slots + MS_STATUS);
     if ((e = cudaMallocHost(&s->h_slots, MS_N * sizeof(double))) != cudaSuccess) return fail(e, "cudaMallocHost");
@@ -490,8 +677,10 @@ int fin_mhd_create(const fin_params* p, fin_mhd** out)
     if ((e = cudaEventCreate(&s->ev1)) != cudaSuccess) return fail(e, "event");
     for (int k = 0; k < 6; k++)
         if ((e = cudaEventCreate(&s->kev[k])) != cudaSuccess) return fail(e, "event");
+    for (int k = 0; k < 2; k++)
+        if ((e = cudaEventCreate(&s->iev[k])) != cudaSuccess) return fail(e, "event");
     if ((e = cudaMemsetAsync(s->slots, 0, MS_N * sizeof(double), s->stream)) != cudaSuccess) return fail(e, "memset");
-    for (int b = 0; b < MNBUF; b++)
+    for (int b = 0; b < nbuf; b++)
         if ((e = cudaMemsetAsync(s->q[b], 0, MHD_NP * s->plane * sizeof(double), s->stream)) != cudaSuccess)
             return fail(e, "memset");
     if ((e = cudaStreamSynchronize(s->stream)) != cudaSuccess) return fail(e, "sync");
@@ -647,11 +836,13 @@ int fin_mhd_step_fixed(fin_mhd* s, double dt, double* cfl_out)
     bool nonfinite = false;
     if ((rc = get_cfl(s, dt, 1e300, &cfl, &nonfinite))) return rc;
     if ((rc = collect_times(s, 3))) return rc;
+    settle_judge(s, nxt, dt, &cfl);
     if (nonfinite) return merr(FIN_ERR_NONFINITE, "non-finite wave speed or state");
     float ms = 0.f;
     MCK(cudaEventElapsedTime(&ms, s->ev0, s->ev1));
     s->last_ms = ms;
     s->cur = nxt;
+    if (s->ind_since >= 0) s->ind_since++;
     s->max_valid = true;
     s->t = s->t + dt;
     if (cfl_out) *cfl_out = cfl;
@@ -685,6 +876,7 @@ int fin_mhd_advance(fin_mhd* s, double tend, double* dtv, int max_steps, int* ns
             bool nonfinite = false;
             if ((rc = get_cfl(s, dt, dtv[2], &cfl, &nonfinite))) goto done;
             if ((rc = collect_times(s, 3))) goto done;
+            settle_judge(s, nxt, dt, &cfl);
             // Qnew.t after the stages (UpdateSoln.cpp:27 of the MHD application)
             t_star = 1.0 * s->t + 0.0 * t_star + 1.0 * dt;
             t_star = 0.75 * s->t + 0.25 * t_star + 0.25 * dt;
@@ -700,6 +892,7 @@ int fin_mhd_advance(fin_mhd* s, double tend, double* dtv, int max_steps, int* ns
             if (cfl <= CFL_max) {
                 m_accept = 1;
                 s->cur = nxt;
+                if (s->ind_since >= 0) s->ind_since++;
                 s->t = t_new;
             } else {
                 t = told;
@@ -737,6 +930,85 @@ int fin_mhd_div_b(fin_mhd* s, double* max_div)
     s->launches++;
     MCK(cudaGetLastError());
     MCK(cudaMemcpyAsync(max_div, s->slots + MS_DIV, sizeof(double), cudaMemcpyDeviceToHost, s->stream));
+    MCK(cudaStreamSynchronize(s->stream));
+    return FIN_OK;
+}
+
+int fin_mhd_set_indicator(fin_mhd* s, const float* params, float z_threshold, int judge_every, double judge_tol)
+{
+    if (!s || !params) return merr(FIN_ERR_ARG, "null argument");
+    if (s->p.precision != FIN_PREC_HYBRID) return merr(FIN_ERR_ARG, "the solver was not created in the hybrid form");
+    if (judge_every < 0) return merr(FIN_ERR_ARG, "judge_every must be >= 0");
+    if (!s->mlpP) MCK(cudaMalloc(&s->mlpP, mlp::NPARAM * sizeof(float)));
+    MCK(cudaMemcpyAsync(s->mlpP, params, mlp::NPARAM * sizeof(float), cudaMemcpyHostToDevice, s->stream));
+    MCK(cudaStreamSynchronize(s->stream));
+    s->zthr = z_threshold;
+    s->judge_every = judge_every;
+    s->judge_tol = judge_tol;
+    s->hyb_off = 0;
+    s->ind_since = -1;
+    return FIN_OK;
+}
+
+int fin_mhd_set_indicator_every(fin_mhd* s, int every)
+{
+    if (!s) return merr(FIN_ERR_ARG, "null argument");
+    if (every < 1) return merr(FIN_ERR_ARG, "the indicator period must be at least one step");
+    s->ind_every = every;
+    s->ind_since = -1;
+    return FIN_OK;
+}
+
+int fin_mhd_hybrid_stats(fin_mhd* s, long long* troubled_faces, long long* faces, long long* judges,
+                         long long* reverts)
+{
+    if (!s) return merr(FIN_ERR_ARG, "null solver");
+    if (s->ind_count) {
+        unsigned long long c = 0;
+        MCK(cudaMemcpyAsync(&c, s->ind_count, sizeof(c), cudaMemcpyDeviceToHost, s->stream));
+        MCK(cudaStreamSynchronize(s->stream));
+        s->troubled_last = (long long)c;
+    }
+    if (troubled_faces) *troubled_faces = s->troubled_last;
+    if (faces) *faces = s->faces;
+    if (judges) *judges = s->judges;
+    if (reverts) *reverts = s->reverts;
+    return FIN_OK;
+}
+
+int fin_mhd_indicator_time(fin_mhd* s, double* ms, long long* launches)
+{
+    if (!s || !ms || !launches) return merr(FIN_ERR_ARG, "null argument");
+    *ms = s->ind_ms;
+    *launches = s->ind_launches;
+    return FIN_OK;
+}
+
+int fin_mhd_face_samples(fin_mhd* s, long long offset, long long stride, long long max_n, float* X_host,
+                         unsigned char* y_host, long long* n_out)
+{
+    if (!s || !X_host || !y_host || !n_out || stride < 1 || offset < 0) return merr(FIN_ERR_ARG, "bad argument");
+    const fin_params& p = s->p;
+    const long long nf = (long long)(p.mx + 1) * p.my + (long long)p.mx * (p.my + 1);
+    long long n = offset < nf ? (nf - offset + stride - 1) / stride : 0;
+    if (n > max_n) n = max_n;
+    *n_out = n;
+    if (n == 0) return FIN_OK;
+    int rc;
+    if (!s->max_valid && (rc = compute_max(s, s->cur))) return rc;
+    float* dX = nullptr;
+    unsigned char* dy = nullptr;
+    MCK(cudaMallocAsync(&dX, size_t(n) * ind::NFEAT * sizeof(float), s->stream));
+    MCK(cudaMallocAsync(&dy, size_t(n), s->stream));
+    const MhdArgs a = base_args(s);
+    k_mhd_face_samples<<<grid_blocks(size_t(n)), 256, 0, s->stream>>>(
+        a, s->q[s->cur], p.global_alpha ? alpha_slot(s, s->cur) : nullptr, offset, stride, n, dX, dy);
+    s->launches++;
+    MCK(cudaGetLastError());
+    MCK(cudaMemcpyAsync(X_host, dX, size_t(n) * ind::NFEAT * sizeof(float), cudaMemcpyDeviceToHost, s->stream));
+    MCK(cudaMemcpyAsync(y_host, dy, size_t(n), cudaMemcpyDeviceToHost, s->stream));
+    MCK(cudaFreeAsync(dX, s->stream));
+    MCK(cudaFreeAsync(dy, s->stream));
     MCK(cudaStreamSynchronize(s->stream));
     return FIN_OK;
 }

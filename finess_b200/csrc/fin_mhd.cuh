@@ -35,6 +35,7 @@
 // evaluated with the reference's own rounding (see mhd_eig_scalars).
 #pragma once
 #include "fin_device.cuh"
+#include "fin_stage.cuh"   // flag masks (flag_wx, row_bits) and linear_face
 
 namespace fin {
 
@@ -63,7 +64,9 @@ struct MhdArgs {
     double* smax_out;          // [2] max face speed over GetCFL's faces
     double* face_alpha_x;      // optional per-face alpha, (mx+1) x my, i-major
     double* face_alpha_y;      // optional per-face alpha, mx x (my+1)
-    unsigned int* status;      // bit 0: non-finite speed, bit 1: negative p or rho
+    unsigned int* status;      // bit 0: non-finite speed, bit 1: negative p or rho, bit 2: a tensor-core
+                               // wait ran out (indicator)
+    const unsigned* flags;     // hybrid form: troubled-face bit masks (flag_wx / flag_wy layout of fin_stage.cuh)
 };
 
 template <class R> struct MPar;
@@ -233,6 +236,7 @@ __device__ __forceinline__ void mhd_face_setup(const MhdArgs& a, R gamma, const 
     f.ra = rs2 * ir;
     f.rb = rs2 * rcp(rsq);
     f.ie = gm1 * ia2;
+    if (!rec) return;
     rec[MR_RHO * rstride] = rho;
     rec[MR_AF * rstride] = af;
     rec[MR_AS * rstride] = as;
@@ -399,7 +403,43 @@ struct MhdCfg {
     {
         return dbl_offset<R>() + sizeof(double) * (size_t(AI) * AJ + size_t(NI) * NJ + 6 * (NT / 32));
     }
+    // Hybrid form, after the above: per-face speeds falpha [NF] (R), the
+    // troubled-face list [NF] (short), its count, and the flag windows of the
+    // 3 x 3 dilation as row masks (x faces: rows i0-1 .. i0+TI+1, bit c =
+    // column j0-1+c, c < TJ+2; y faces: rows i0-1 .. i0+TI, c < TJ+3).
+    static constexpr int NF = NFX + NFY;
+    static constexpr int FXR = TI + 3, FXC = TJ + 2, FYR = TI + 2, FYC = TJ + 3;
+    static_assert(FYC <= 32 && FXR <= 32 && FYR <= 32, "flag row masks are 32-bit words read by one warp each");
+    template <class R>
+    __host__ __device__ static constexpr size_t hyb_ntrb_offset() { return (NF * sizeof(R) + NF * 2 + 15) / 16 * 16; }
+    template <class R>
+    __host__ __device__ static constexpr size_t hyb_mask_offset() { return hyb_ntrb_offset<R>() + 16; }
+    template <class R>
+    __host__ __device__ static constexpr size_t smem_bytes_hyb()
+    {
+        return smem_bytes<R>() + hyb_mask_offset<R>() + 4 * (FXR + FYR);
+    }
 };
+
+// Bits of columns c0 .. c0+nb-1 (nb <= 32) of one flag-mask row of nw words,
+// columns taken modulo the period (periodic boundaries; the flag arrays hold
+// columns 0 .. period-1, y faces also column period, equal to column 0).
+__device__ __forceinline__ unsigned mask_row_wrapped(const unsigned* row, int nw, int c0, int nb, int period)
+{
+    if (c0 >= 0 && c0 + nb <= period) {
+        const int k = c0 >> 5;
+        const unsigned lo = __ldg(row + k), hi = k + 1 < nw ? __ldg(row + k + 1) : 0u;
+        return row_bits(lo, hi, c0) & (nb >= 32 ? 0xffffffffu : ((1u << nb) - 1u));
+    }
+    unsigned m = 0;
+    for (int b = 0; b < nb; b++) {
+        int c = c0 + b;
+        if (c < 0) c += period;
+        else if (c >= period) c -= period;
+        m |= ((__ldg(row + (c >> 5)) >> (c & 31)) & 1u) << b;
+    }
+    return m;
+}
 
 // Sweeps over the stencil per face: the fast and slow pairs share dn, S_u, P
 // and S_b and take one sweep (40 live values); with FIN_MHD_SWEEPS = 2 the
@@ -414,7 +454,7 @@ struct MhdCfg {
 #endif
 template <class R> struct MhdMinBlocks { static constexpr int value = 1; };
 
-template <class R, int VER, bool P2, class Cfg>
+template <class R, int VER, bool P2, class Cfg, bool HYB = false>
 __global__ void __launch_bounds__(Cfg::NT, MhdMinBlocks<R>::value) k_mhd_stage(const __grid_constant__ MhdArgs a)
 {
     constexpr int TI = Cfg::TI, TJ = Cfg::TJ, NT = Cfg::NT, H = Cfg::H;
@@ -433,6 +473,9 @@ __global__ void __launch_bounds__(Cfg::NT, MhdMinBlocks<R>::value) k_mhd_stage(c
     double* as = reinterpret_cast<double*>(smem_raw + Cfg::template dbl_offset<R>());   // [AI][AJ]
     double* an = as + Cfg::AI * AJ;                  // [NI][NJ]
     double* red = an + Cfg::NI * NJ;                 // [NT/32][6]
+    unsigned char* hyb_base = smem_raw + Cfg::template smem_bytes<R>();
+    unsigned* fxm = reinterpret_cast<unsigned*>(hyb_base + Cfg::template hyb_mask_offset<R>());
+    unsigned* fym = fxm + Cfg::FXR;
 
     const int tid = threadIdx.x;
     const int mx = a.mx, my = a.my;
@@ -457,6 +500,26 @@ __global__ void __launch_bounds__(Cfg::NT, MhdMinBlocks<R>::value) k_mhd_stage(c
         const int gi = bc_remap(i0 + ii - HA, mx, FIN_BC_PERIODIC, FIN_BC_PERIODIC);
         const int gj = bc_remap(j0 + jj - HA, my, FIN_BC_PERIODIC, FIN_BC_PERIODIC);
         as[e] = __ldg(a.qin + 8 * a.plane + size_t(gi) * my + gj);
+    }
+    if (HYB) {
+        // the flag windows, rows and columns wrapped (doubly periodic), each
+        // row dilated over 3 columns
+        const int wx = flag_wx(my), wy = flag_wy(my);
+        if (tid < Cfg::FXR) {
+            int r = i0 - 1 + tid;   // x-face row (faces 0 .. mx, face mx = face 0)
+            if (r < 0) r += mx;
+            else if (r > mx) r -= mx;
+            const unsigned m = mask_row_wrapped(a.flags + size_t(r) * wx, wx, j0 - 1, Cfg::FXC, my);
+            fxm[tid] = m | (m >> 1) | (m >> 2);
+        } else if (tid >= 32 && tid < 32 + Cfg::FYR) {
+            int r = i0 - 1 + (tid - 32);   // y-face row (cell rows 0 .. mx-1)
+            if (r < 0) r += mx;
+            else if (r >= mx) r -= mx;
+            const unsigned m =
+                mask_row_wrapped(a.flags + size_t(mx + 1) * wx + size_t(r) * wy, wy, j0 - 1, Cfg::FYC, my);
+            fym[tid - 32] = m | (m >> 1) | (m >> 2);
+        }
+        if (tid == 0) *reinterpret_cast<int*>(hyb_base + Cfg::template hyb_ntrb_offset<R>()) = 0;
     }
     __syncthreads();
 
@@ -554,58 +617,95 @@ __global__ void __launch_bounds__(Cfg::NT, MhdMinBlocks<R>::value) k_mhd_stage(c
     }
     __syncthreads();
 
-    // ---- phase 2: one thread per face (x faces then y faces) ----
+    // ---- phase 2: the faces (x faces then y faces).  Plain form: one thread
+    // per face, the full characteristic WENO flux.  Hybrid form: pass A gives
+    // every face its speed and the smooth faces (no troubled flag in the 3 x 3
+    // window of same-direction faces) the linear FD5 flux, component by
+    // component (linear_face, fin_stage.cuh); the troubled faces go to a list
+    // that pass B works through with the full flux ----
     const R ag1 = a.alpha_in ? R(a.alpha_in[0]) : R(0);
     const R ag2 = a.alpha_in ? R(a.alpha_in[1]) : R(0);
     const R eps = MPar<R>::eps(a), pw = MPar<R>::pw(a);
     R smax_x = R(0), smax_y = R(0);
     const int nwork = Cfg::NFX + Cfg::NFY;
-#pragma unroll 1
-    for (int w = tid; w < nwork; w += NT) {
-        const bool isx = w < Cfg::NFX;
+    struct Geom {
+        bool isx;
         int fi, fj, qbase, qstr, fbase, fstr, fplane, pbase, pstr;
         const R* fl;
-        if (isx) {
-            fi = w / TJ; fj = w - fi * TJ;               // between tile rows fi-1 and fi
-            qbase = (H + fi) * RJ + (H + fj); qstr = RJ;
-            fl = fs; fbase = (H + fi) * TJ + fj; fstr = TJ; fplane = RI * TJ;
-            pbase = (fi + 1) * PJ + (fj + 1); pstr = PJ;
+        int perm[MHD_NQ];
+    };
+    auto geom = [&](int w) {
+        Geom g;
+        g.isx = w < Cfg::NFX;
+        if (g.isx) {
+            g.fi = w / TJ; g.fj = w - g.fi * TJ;                  // between tile rows fi-1 and fi
+            g.qbase = (H + g.fi) * RJ + (H + g.fj); g.qstr = RJ;
+            g.fl = fs; g.fbase = (H + g.fi) * TJ + g.fj; g.fstr = TJ; g.fplane = RI * TJ;
+            g.pbase = (g.fi + 1) * PJ + (g.fj + 1); g.pstr = PJ;
         } else {
             const int v = w - Cfg::NFX;
-            fi = v / (TJ + 1); fj = v - fi * (TJ + 1);   // between tile columns fj-1 and fj
-            qbase = (H + fi) * RJ + (H + fj); qstr = 1;
-            fl = gs; fbase = fi * RJ + (H + fj); fstr = 1; fplane = TI * RJ;
-            pbase = (fi + 1) * PJ + (fj + 1); pstr = 1;
+            g.fi = v / (TJ + 1); g.fj = v - g.fi * (TJ + 1);      // between tile columns fj-1 and fj
+            g.qbase = (H + g.fi) * RJ + (H + g.fj); g.qstr = 1;
+            g.fl = gs; g.fbase = g.fi * RJ + (H + g.fj); g.fstr = 1; g.fplane = TI * RJ;
+            g.pbase = (g.fi + 1) * PJ + (g.fj + 1); g.pstr = 1;
         }
         // normal-frame component order: rho, m_n, m_t, m_w, E, B_n, B_t, B_w
-        const int cn = isx ? 1 : 2, ct = isx ? 2 : 1, bn = isx ? 5 : 6, bt = isx ? 6 : 5;
-        const int perm[MHD_NQ] = {0, cn, ct, 3, 4, bn, bt, 7};
-        const int ql = qbase - qstr;
+        g.perm[0] = 0; g.perm[1] = g.isx ? 1 : 2; g.perm[2] = g.isx ? 2 : 1; g.perm[3] = 3; g.perm[4] = 4;
+        g.perm[5] = g.isx ? 5 : 6; g.perm[6] = g.isx ? 6 : 5; g.perm[7] = 7;
+        return g;
+    };
+    // SetWaveSpd.cpp:39-88 (nmag = 1; the fast speeds use B1, the x
+    // component, for either normal), the LLF alpha of ConstructL.cpp:172-174,
+    // and the face-speed maxima GetCFL reads.
+    auto speed = [&](const Geom& g) -> R {
+        const int pl = g.pbase - g.pstr, un = g.isx ? 0 : 1;
+        const int ql = g.qbase - g.qstr;
+        const R unl = pc[un * PP + pl], unr = pc[un * PP + g.pbase];
+        const R pa = R(0.5) * (pc[2 * PP + pl] + pc[2 * PP + g.pbase]);
+        const R rho = R(0.5) * (qs[g.qbase] + qs[ql]);
+        const R b5 = R(0.5) * (qs[5 * PQ + g.qbase] + qs[5 * PQ + ql]);
+        const R b6 = R(0.5) * (qs[6 * PQ + g.qbase] + qs[6 * PQ + ql]);
+        const R b7 = R(0.5) * (qs[7 * PQ + g.qbase] + qs[7 * PQ + ql]);
+        const R Bm2 = b5 * b5 + b6 * b6 + b7 * b7;
+        const R ir = rcp(rho);
+        const R a2 = fabs(gamma * pa * ir);
+        const R t = a2 + Bm2 * ir;
+        const R cf = fsqrt(R(0.5) * (t + fsqrt(fabs(t * t - R(4) * a2 * (b5 * b5) * ir))));
+        const R ua = R(0.5) * (unl + unr);
+        const R s1 = Min(unl - pc[3 * PP + pl], ua - cf);
+        const R s2 = Max(unr + pc[3 * PP + g.pbase], ua + cf);
+        const R alpha = Max(g.isx ? ag1 : ag2, Max(fabs(s1), fabs(s2)));
+        if (!(alpha <= R(1e30))) nonfinite = true;
+        if (g.isx) {
+            const int gfi = i0 + g.fi, gj = j0 + g.fj;
+            if (gfi < mx && gj < my && alpha <= R(1e30)) smax_x = Max(smax_x, alpha);
+            if (a.face_alpha_x && gfi <= mx && gj < my) a.face_alpha_x[size_t(gfi) * my + gj] = double(alpha);
+        } else {
+            const int gi = i0 + g.fi, gfj = j0 + g.fj;
+            if (gi < mx && gfj < my && alpha <= R(1e30)) smax_y = Max(smax_y, alpha);
+            if (a.face_alpha_y && gi < mx && gfj <= my) a.face_alpha_y[size_t(gi) * (my + 1) + gfj] = double(alpha);
+        }
+        return alpha;
+    };
+    auto store_face = [&](const Geom& g, const R* Fo) {
+        if (g.isx) {
+#pragma unroll
+            for (int m = 0; m < MHD_NQ; m++) Fh[g.perm[m] * Cfg::NFX + g.fi * TJ + g.fj] = Fo[m];
+        } else {
+#pragma unroll
+            for (int m = 0; m < MHD_NQ; m++) Gh[g.perm[m] * Cfg::NFY + g.fi * (TJ + 1) + g.fj] = Fo[m];
+        }
+    };
+    // The full characteristic WENO flux of one face (ConstructL.cpp:72-206 /
+    // 224-356 with the MHD projections).
+    auto full_face = [&](const Geom& g, R alpha) {
+        const int* perm = g.perm;
+        const int qbase = g.qbase, ql = g.qbase - g.qstr;
         R Qa[MHD_NQ];
 #pragma unroll
         for (int m = 0; m < MHD_NQ; m++) Qa[m] = R(0.5) * (qs[perm[m] * PQ + qbase] + qs[perm[m] * PQ + ql]);
-
-        // SetWaveSpd.cpp:39-88 (nmag = 1; the fast speeds use B1, the x
-        // component, for either normal) and the LLF alpha of ConstructL.cpp:172-174.
-        R alpha;
-        {
-            const int pl = pbase - pstr, un = isx ? 0 : 1;
-            const R unl = pc[un * PP + pl], unr = pc[un * PP + pbase];
-            const R pa = R(0.5) * (pc[2 * PP + pl] + pc[2 * PP + pbase]);
-            const R rho = Qa[0];
-            const R B1x = isx ? Qa[5] : Qa[6];
-            const R Bm2 = Qa[5] * Qa[5] + Qa[6] * Qa[6] + Qa[7] * Qa[7];
-            const R ir = rcp(rho);
-            const R a2 = fabs(gamma * pa * ir);
-            const R t = a2 + Bm2 * ir;
-            const R cf = fsqrt(R(0.5) * (t + fsqrt(fabs(t * t - R(4) * a2 * (B1x * B1x) * ir))));
-            const R ua = R(0.5) * (unl + unr);
-            const R s1 = Min(unl - pc[3 * PP + pl], ua - cf);
-            const R s2 = Max(unr + pc[3 * PP + pbase], ua + cf);
-            alpha = Max(isx ? ag1 : ag2, Max(fabs(s1), fabs(s2)));
-        }
-        if (!(alpha <= R(1e30))) nonfinite = true;
         const R lah = R(0.5) * MPar<R>::ascale(a) * alpha;
+        const MhdStencil<R> st{qs, g.fl, perm, qbase, g.qstr, g.fbase, g.fstr, g.fplane, PQ, lah};
         MhdFace<R> f;
         mhd_face_setup<R>(a, gamma, Qa, f, rec + tid, NT, neg);
 
@@ -613,14 +713,13 @@ __global__ void __launch_bounds__(Cfg::NT, MhdMinBlocks<R>::value) k_mhd_stage(c
         // lah q at points 0..4, gm from v- = 0.5 f - lah q at points 5..1
         // (ConstructL.cpp:179-199); ghat[k] for the eight waves.
         R ghat[MHD_NQ];
-        const MhdStencil<R> st{qs, fl, perm, qbase, qstr, fbase, fstr, fplane, PQ, lah};
         {
             // fast and slow pairs (rows 0, 7, 2, 5) in one sweep
             R p[4][5], m[4][5];
             mhd_sweep<R, 4>(st, [&](const R* v, R* w) { mhd_left_fs4<R>(f, v, w[0], w[1], w[2], w[3]); }, p, m);
-            R g[4];
-            mhd_weno_fields<R, VER, P2, 4>(p, m, eps, pw, g);
-            ghat[0] = g[0]; ghat[7] = g[1]; ghat[2] = g[2]; ghat[5] = g[3];
+            R gg[4];
+            mhd_weno_fields<R, VER, P2, 4>(p, m, eps, pw, gg);
+            ghat[0] = gg[0]; ghat[7] = gg[1]; ghat[2] = gg[2]; ghat[5] = gg[3];
         }
 #if FIN_MHD_SWEEPS == 2
         {
@@ -630,9 +729,9 @@ __global__ void __launch_bounds__(Cfg::NT, MhdMinBlocks<R>::value) k_mhd_stage(c
                 mhd_left_alf<R>(f, v, w[0], w[1]);
                 mhd_left_ent<R>(f, v, w[2], w[3]);
             }, p, m);
-            R g[4];
-            mhd_weno_fields<R, VER, P2, 4>(p, m, eps, pw, g);
-            ghat[1] = g[0]; ghat[6] = g[1]; ghat[3] = g[2]; ghat[4] = g[3];
+            R gg[4];
+            mhd_weno_fields<R, VER, P2, 4>(p, m, eps, pw, gg);
+            ghat[1] = gg[0]; ghat[6] = gg[1]; ghat[3] = gg[2]; ghat[4] = gg[3];
         }
 #else
         // the Alfven pair, then the entropy and divergence rows: one loop
@@ -644,10 +743,10 @@ __global__ void __launch_bounds__(Cfg::NT, MhdMinBlocks<R>::value) k_mhd_stage(c
                 if (pass == 0) mhd_left_alf<R>(f, v, w[0], w[1]);
                 else mhd_left_ent<R>(f, v, w[0], w[1]);
             }, p, m);
-            R g[2];
-            mhd_weno_fields<R, VER, P2, 2>(p, m, eps, pw, g);
-            if (pass == 0) { ghat[1] = g[0]; ghat[6] = g[1]; }
-            else { ghat[3] = g[0]; ghat[4] = g[1]; }
+            R gg[2];
+            mhd_weno_fields<R, VER, P2, 2>(p, m, eps, pw, gg);
+            if (pass == 0) { ghat[1] = gg[0]; ghat[6] = gg[1]; }
+            else { ghat[3] = gg[0]; ghat[4] = gg[1]; }
         }
 #endif
 
@@ -683,18 +782,53 @@ __global__ void __launch_bounds__(Cfg::NT, MhdMinBlocks<R>::value) k_mhd_stage(c
             Fo[6] = dbt;
             Fo[7] = dbw;
         }
-        if (isx) {
+        store_face(g, Fo);
+    };
+    if (HYB) {
+        R* falpha = reinterpret_cast<R*>(hyb_base);                            // [NFX + NFY]
+        short* tlist = reinterpret_cast<short*>(falpha + nwork);               // [NFX + NFY]
+        int* ntrb = reinterpret_cast<int*>(hyb_base + Cfg::template hyb_ntrb_offset<R>());
+#pragma unroll 1
+        for (int wb = 0; wb < nwork; wb += NT) {
+            const int w = wb + tid;
+            bool push = false;
+            if (w < nwork) {
+                const Geom g = geom(w);
+                const R alpha = speed(g);
+                falpha[w] = alpha;
+                const unsigned* fm = g.isx ? fxm : fym;
+                push = (((fm[g.fi] | fm[g.fi + 1] | fm[g.fi + 2]) >> g.fj) & 1u) != 0;
+                if (!push) {
+                    const R lah = R(0.5) * MPar<R>::ascale(a) * alpha;
+                    R Fo[MHD_NQ];
 #pragma unroll
-            for (int m = 0; m < MHD_NQ; m++) Fh[perm[m] * Cfg::NFX + fi * TJ + fj] = Fo[m];
-            const int gfi = i0 + fi, gj = j0 + fj;
-            if (gfi < mx && gj < my && alpha <= R(1e30)) smax_x = Max(smax_x, alpha);
-            if (a.face_alpha_x && gfi <= mx && gj < my) a.face_alpha_x[size_t(gfi) * my + gj] = double(alpha);
-        } else {
-#pragma unroll
-            for (int m = 0; m < MHD_NQ; m++) Gh[perm[m] * Cfg::NFY + fi * (TJ + 1) + fj] = Fo[m];
-            const int gi = i0 + fi, gfj = j0 + fj;
-            if (gi < mx && gfj < my && alpha <= R(1e30)) smax_y = Max(smax_y, alpha);
-            if (a.face_alpha_y && gi < mx && gfj <= my) a.face_alpha_y[size_t(gi) * (my + 1) + gfj] = double(alpha);
+                    for (int m = 0; m < MHD_NQ; m++)
+                        Fo[m] = linear_face<R>(g.fl + g.perm[m] * g.fplane + g.fbase, g.fstr,
+                                               qs + g.perm[m] * PQ + g.qbase, g.qstr, lah);
+                    store_face(g, Fo);
+                }
+            }
+            const unsigned bal = __ballot_sync(0xffffffffu, push);
+            if (bal) {
+                int base = 0;
+                const int lead = __ffs(bal) - 1;
+                if ((tid & 31) == lead) base = atomicAdd(ntrb, __popc(bal));
+                base = __shfl_sync(0xffffffffu, base, lead);
+                if (push) tlist[base + __popc(bal & ((1u << (tid & 31)) - 1u))] = short(w);
+            }
+        }
+        __syncthreads();
+        const int nt = *ntrb;
+#pragma unroll 1
+        for (int k = tid; k < nt; k += NT) {
+            const int w = tlist[k];
+            full_face(geom(w), falpha[w]);
+        }
+    } else {
+#pragma unroll 1
+        for (int w = tid; w < nwork; w += NT) {
+            const Geom g = geom(w);
+            full_face(g, speed(g));
         }
     }
     __syncthreads();

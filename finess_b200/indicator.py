@@ -17,6 +17,8 @@ from .solver import FinError, load_library
 NIN = 20
 _HERE = os.path.dirname(os.path.abspath(__file__))
 DEFAULT_WEIGHTS = os.path.join(_HERE, "data", "indicator_weights.npz")
+# the same network trained on ideal-MHD faces (finess_b200/mhd.py's hybrid form)
+DEFAULT_MHD_WEIGHTS = os.path.join(_HERE, "data", "indicator_mhd_weights.npz")
 
 
 def _lib():

@@ -291,7 +291,7 @@ int fin_construct_l_noalloc(const fin_params* p, const double* q_dev, double* L_
  * FinSolveRK.cpp:17-395) with its CFL number (GetCFL.cpp:31-73); doubly
  * periodic boundaries (apps/2d/mhd/orszag_tang/SetBndValues.cpp).
  * fin_params: physics FIN_PHYS_MHD, meqn 8, maux 1, mbc >= 5, time_order 3,
- * precision FIN_PREC_FP64 or FIN_PREC_FP32.  q arrays are the ghosted
+ * precision FIN_PREC_FP64, FIN_PREC_FP32 or FIN_PREC_HYBRID.  q arrays are the ghosted
  * (mx, my, 8) layout above, aux arrays the ghosted (mx, my, 1) layout.
  * Errors: fin_mhd_last_error(). */
 typedef struct fin_mhd fin_mhd;
@@ -329,6 +329,25 @@ int fin_mhd_set_kernel_timing(fin_mhd* s, int on);
 int fin_mhd_kernel_time(fin_mhd* s, double* ms, long long* launches);
 int fin_mhd_launch_count(fin_mhd* s, long long* launches);
 int fin_mhd_device_state(fin_mhd* s, double** q_dev, size_t* plane_stride);
+/* Hybrid form (precision FIN_PREC_HYBRID): the troubled-face network
+ * (fin_mlp_nparam() floats; trained on MHD labels: the WENO5-JS weights of
+ * any of the eight characteristic fields departing from the linear weights
+ * by more than 10 %), its logit threshold, and the judge step (every
+ * judge_every-th hybrid step is recomputed with full WENO from the same
+ * state; a relative L-infinity difference above judge_tol takes the full
+ * result and switches the indicator off for judge_every steps).  Faces with a
+ * troubled flag in their 3 x 3 same-direction window take the full
+ * characteristic WENO flux, all others the linear FD5 weights.  Without this
+ * call the hybrid form runs full WENO in FP32. */
+int fin_mhd_set_indicator(fin_mhd* s, const float* params, float z_threshold, int judge_every, double judge_tol);
+int fin_mhd_set_indicator_every(fin_mhd* s, int every);
+int fin_mhd_hybrid_stats(fin_mhd* s, long long* troubled_faces, long long* faces, long long* judges,
+                         long long* reverts);
+int fin_mhd_indicator_time(fin_mhd* s, double* ms, long long* launches);
+/* Training samples of the current state: 20 features and a label per face
+ * for faces offset, offset + stride, ... (x faces, then y faces), at most max_n. */
+int fin_mhd_face_samples(fin_mhd* s, long long offset, long long stride, long long max_n, float* X_host,
+                         unsigned char* y_host, long long* n_out);
 
 #ifdef __cplusplus
 }

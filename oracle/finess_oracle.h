@@ -75,6 +75,9 @@ int oracle_mhd_step_fixed(const fin_params* p, double* q, double* aux, double dt
 /* apps/2d/mhd/lib/FinSolveRK.cpp:17-395 (time_order 3) from *t to tend. */
 int oracle_mhd_finsolve(const fin_params* p, double* q, double* aux, double* t, double tend, double* dtv,
                         int* nsteps);
+/* Features (20 per face) and labels of the MHD troubled-face indicator,
+ * x faces then y faces (the device kernel's enumeration). */
+void oracle_mhd_face_samples(const fin_params* p, const double* q, double* X, unsigned char* y);
 /* Orszag-Tang initial state (QinitFunc + AfterQinit), ghosts filled. */
 void oracle_orszag_tang(const fin_params* p, double* q, double* aux);
 

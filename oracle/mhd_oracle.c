@@ -660,3 +660,80 @@ void oracle_orszag_tang(const fin_params* p, double* q, double* aux)
         }
     oracle_mhd_set_bnd(p, q, aux);
 }
+
+/* ---------------------------------------------------------------------- */
+/* Troubled-face samples of the MHD learned indicator                      */
+/* ---------------------------------------------------------------------- */
+
+/* Features and labels of every face (x faces, then y faces; (i, j) with j
+ * fastest), for the face between cells i-1 and i (1-based i = f_i + 1) with
+ * the 6-point stencil i-3 .. i+2:
+ *   w = Lmat q at the six points, Lmat the left eigenvectors at the face
+ *   average (ProjectLeftEig.cpp:179-192); for each wave pair (fast 0/7,
+ *   slow 2/5, Alfven 1/6, entropy/divergence 3/4) the member with the larger
+ *   undivided difference max_s |w(s+1) - w(s)| gives 5 features, its
+ *   differences divided by max(that maximum, 1e-3): 20 features;
+ *   label: 1 when the WENO5-JS weights of gp or gm (ConstructL.cpp:179-192)
+ *   of any of the eight fields depart from (0.1, 0.6, 0.3) by more than 10 %
+ *   (lib/WenoReconstruct.cpp:104, 131-134). */
+void oracle_mhd_face_samples(const fin_params* p, const double* q, double* X, unsigned char* y)
+{
+    const mgrid_t g = mgrid(p, p->mx, p->my, MQ);
+    double alpha1 = 0., alpha2 = 0.;
+    if (p->global_alpha) oracle_mhd_global_wave_spd(p, q, &alpha1, &alpha2);
+    static const int pairs[4][2] = {{0, 7}, {2, 5}, {1, 6}, {3, 4}};
+    static const double dl[3] = {0.1, 0.6, 0.3};
+    long long f = 0;
+    for (int ixy = 1; ixy <= 2; ixy++) {
+        const int ni = ixy == 1 ? g.mx + 1 : g.mx, nj = ixy == 1 ? g.my : g.my + 1;
+        const int di = ixy == 1 ? 1 : 0, dj = ixy == 1 ? 0 : 1;
+        for (int i = 0; i < ni; i++)
+            for (int j = 0; j < nj; j++, f++) {
+                double Qs[6][MQ], Fs[6][MQ];
+                for (int s = 0; s < 6; s++) {
+                    const double* Qp = q + MI(&g, i + 1 + di * (s - 3), j + 1 + dj * (s - 3), 1);
+                    double fx[MQ], fy[MQ];
+                    mhd_flux(p->gamma, Qp, fx, fy);
+                    for (int m = 0; m < MQ; m++) {
+                        Qs[s][m] = Qp[m];
+                        Fs[s][m] = ixy == 1 ? fx[m] : fy[m];
+                    }
+                }
+                double Qavg[MQ], Lm[MQ][MQ], Rm[MQ][MQ], W[6][MQ], G[6][MQ];
+                for (int m = 0; m < MQ; m++) Qavg[m] = 0.5 * (Qs[3][m] + Qs[2][m]);
+                mhd_eig(ixy, p->gamma, Qavg, Lm, Rm);
+                for (int s = 0; s < 6; s++) {
+                    matvec8(Lm, Qs[s], W[s]);
+                    matvec8(Lm, Fs[s], G[s]);
+                }
+                for (int t = 0; t < 4; t++) {
+                    double d[2][5], mm[2] = {0.0, 0.0};
+                    for (int c = 0; c < 2; c++)
+                        for (int s = 0; s < 5; s++) {
+                            d[c][s] = W[s + 1][pairs[t][c]] - W[s][pairs[t][c]];
+                            if (fabs(d[c][s]) > mm[c]) mm[c] = fabs(d[c][s]);
+                        }
+                    const int c = mm[0] >= mm[1] ? 0 : 1;
+                    const double den = mm[c] > 1e-3 ? mm[c] : 1e-3;
+                    for (int s = 0; s < 5; s++) X[f * 20 + t * 5 + s] = d[c][s] / den;
+                }
+                double s1, s2;
+                mhd_wave_spd(p->gamma, ixy == 1 ? 1.0 : 0.0, ixy == 1 ? 0.0 : 1.0, Qs[2], Qs[3], &s1, &s2);
+                const double alpha = Max(ixy == 1 ? alpha1 : alpha2, Max(fabs(s1), fabs(s2)));
+                const double la = p->alpha_scaling * alpha;
+                double dep = 0.0;
+                for (int k = 0; k < MQ; k++) {
+                    double gp[5], gm[5], w[3];
+                    for (int s = 0; s < 5; s++) {
+                        gp[s] = 0.5 * (G[s][k] + la * W[s][k]);
+                        gm[s] = 0.5 * (G[5 - s][k] - la * W[5 - s][k]);
+                    }
+                    oracle_weno_js5_weights(p->epsilon, p->power_param, gp, w);
+                    for (int r = 0; r < 3; r++) dep = Max(dep, fabs(w[r] - dl[r]) / dl[r]);
+                    oracle_weno_js5_weights(p->epsilon, p->power_param, gm, w);
+                    for (int r = 0; r < 3; r++) dep = Max(dep, fabs(w[r] - dl[r]) / dl[r]);
+                }
+                y[f] = dep > 0.1 ? 1 : 0;
+            }
+    }
+}

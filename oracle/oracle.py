@@ -79,6 +79,7 @@ class Oracle:
                                             C.POINTER(C.c_int)]
         lib.oracle_mhd_finsolve.restype = C.c_int
         lib.oracle_orszag_tang.argtypes = [P, _dp, _dp]
+        lib.oracle_mhd_face_samples.argtypes = [P, _dp, _dp, np.ctypeslib.ndpointer(np.uint8, flags="C_CONTIGUOUS")]
         self.lib = lib
 
     def set_bnd(self, p, q):
@@ -201,6 +202,13 @@ class Oracle:
         n = C.c_int(0)
         rc = self.lib.oracle_mhd_finsolve(C.byref(p), q, aux, C.byref(tt), tend, dtv, C.byref(n))
         return rc, q, aux, tt.value, dtv[1], n.value
+
+    def mhd_face_samples(self, p, q):
+        nf = (p.mx + 1) * p.my + p.mx * (p.my + 1)
+        X = np.zeros((nf, 20))
+        y = np.zeros(nf, dtype=np.uint8)
+        self.lib.oracle_mhd_face_samples(C.byref(p), np.ascontiguousarray(q), X, y)
+        return X, y
 
     def orszag_tang(self, p):
         q = np.zeros(ghosted_shape(p))
