@@ -43,15 +43,28 @@ int merr(int code, const std::string& msg)
 // measured on B200 at 2048^2 (stage ms, fast and slow pairs merged): FP64
 // 256 threads with up to 255 registers and no spills 2.58, 512 threads at
 // 128 registers (~500 B spilled, missing L1 beside 160 KB of shared memory)
-// 2.71; FP32 512 threads 1.50, 256 threads 1.74.
+// 2.71.  FP32 and the hybrid form: 256 threads at 128 registers, two blocks
+// per SM, so that one block's loads and barriers overlap the other's
+// arithmetic (1024^2, stage ms: FP32 0.268 against 0.323 for one 512-thread
+// block per SM; hybrid with no troubled face 0.186 against 0.246).
 #ifndef FIN_MHD_NT64
 #define FIN_MHD_NT64 256
 #endif
 #ifndef FIN_MHD_NT32
-#define FIN_MHD_NT32 512
+#define FIN_MHD_NT32 256
 #endif
-template <class R> struct MCfgOf { using T = MhdCfg<15, 16, FIN_MHD_NT64>; };
-template <> struct MCfgOf<float> { using T = MhdCfg<15, 16, FIN_MHD_NT32>; };
+#ifndef FIN_MHD_MINB32
+#define FIN_MHD_MINB32 2
+#endif
+#ifndef FIN_MHD_NTH
+#define FIN_MHD_NTH 256
+#endif
+#ifndef FIN_MHD_MINBH
+#define FIN_MHD_MINBH 2
+#endif
+template <class R, bool HYB> struct MCfgOf { using T = MhdCfg<15, 16, FIN_MHD_NT64>; };
+template <> struct MCfgOf<float, false> { using T = MhdCfg<15, 16, FIN_MHD_NT32, FIN_MHD_MINB32>; };
+template <> struct MCfgOf<float, true> { using T = MhdCfg<15, 16, FIN_MHD_NTH, FIN_MHD_MINBH>; };
 
 // Reduction slots (doubles): face-speed maxima of the step, then per state
 // buffer its GlobalWaveSpd maxima and its HJ speeds, the status word, and the
@@ -305,7 +318,7 @@ MhdArgs base_args(fin_mhd* s)
 template <class R, int VER, bool P2, bool HYB>
 int launch_t(fin_mhd* s, const MhdArgs& a)
 {
-    using MCfg = typename MCfgOf<R>::T;
+    using MCfg = typename MCfgOf<R, HYB>::T;
     constexpr size_t smem = HYB ? MCfg::template smem_bytes_hyb<R>() : MCfg::template smem_bytes<R>();
     static bool attr = false;
     if (!attr) {

@@ -69,6 +69,17 @@ struct MhdArgs {
     const unsigned* flags;     // hybrid form: troubled-face bit masks (flag_wx / flag_wy layout of fin_stage.cuh)
 };
 
+// Periodic index wrap: one add or subtract for the indices a tile reaches
+// (at most one period outside), the general remap otherwise (grids smaller
+// than a tile and its halo).
+__device__ __forceinline__ int pwrap(int k, int n)
+{
+    if (k < 0) k += n;
+    else if (k >= n) k -= n;
+    if (unsigned(k) >= unsigned(n)) k = bc_remap(k, n, FIN_BC_PERIODIC, FIN_BC_PERIODIC);
+    return k;
+}
+
 template <class R> struct MPar;
 template <> struct MPar<double> {
     __device__ static double gamma(const MhdArgs& a) { return a.gamma; }
@@ -380,9 +391,10 @@ __device__ __forceinline__ void mhd_weno_fields(R (&p)[K][5], R (&m)[K][5], R ep
     }
 }
 
-template <int TI_, int TJ_, int NT_>
+template <int TI_, int TJ_, int NT_, int MINB_ = 1>
 struct MhdCfg {
     static constexpr int TI = TI_, TJ = TJ_, NT = NT_;
+    static constexpr int MINB = MINB_;   // resident blocks per SM the registers are sized for
     static constexpr int H = 3;              // q halo of the WENO stencils
     static constexpr int HA = 5;             // A3 halo (HJ stencils of the 2-cell CT halo)
     static constexpr int HN = 2;             // CT halo of the updated A3
@@ -452,10 +464,9 @@ __device__ __forceinline__ unsigned mask_row_wrapped(const unsigned* row, int nw
 #ifndef FIN_MHD_SWEEPS
 #define FIN_MHD_SWEEPS 2
 #endif
-template <class R> struct MhdMinBlocks { static constexpr int value = 1; };
 
 template <class R, int VER, bool P2, class Cfg, bool HYB = false>
-__global__ void __launch_bounds__(Cfg::NT, MhdMinBlocks<R>::value) k_mhd_stage(const __grid_constant__ MhdArgs a)
+__global__ void __launch_bounds__(Cfg::NT, Cfg::MINB) k_mhd_stage(const __grid_constant__ MhdArgs a)
 {
     constexpr int TI = Cfg::TI, TJ = Cfg::TJ, NT = Cfg::NT, H = Cfg::H;
     constexpr int RI = Cfg::RI, RJ = Cfg::RJ, PQ = RI * RJ;
@@ -489,16 +500,16 @@ __global__ void __launch_bounds__(Cfg::NT, MhdMinBlocks<R>::value) k_mhd_stage(c
         const int ii = e / RJ, jj = e - ii * RJ;
         const bool xin = ii >= H && ii < H + TI, yin = jj >= H && jj < H + TJ;
         if (!xin && !yin) continue;
-        const int gi = bc_remap(i0 + ii - H, mx, FIN_BC_PERIODIC, FIN_BC_PERIODIC);
-        const int gj = bc_remap(j0 + jj - H, my, FIN_BC_PERIODIC, FIN_BC_PERIODIC);
+        const int gi = pwrap(i0 + ii - H, mx);
+        const int gj = pwrap(j0 + jj - H, my);
         const size_t g = size_t(gi) * my + gj;
 #pragma unroll
         for (int m = 0; m < MHD_NQ; m++) qs[m * PQ + e] = R(__ldg(a.qin + m * a.plane + g));
     }
     for (int e = tid; e < Cfg::AI * AJ; e += NT) {
         const int ii = e / AJ, jj = e - ii * AJ;
-        const int gi = bc_remap(i0 + ii - HA, mx, FIN_BC_PERIODIC, FIN_BC_PERIODIC);
-        const int gj = bc_remap(j0 + jj - HA, my, FIN_BC_PERIODIC, FIN_BC_PERIODIC);
+        const int gi = pwrap(i0 + ii - HA, mx);
+        const int gj = pwrap(j0 + jj - HA, my);
         as[e] = __ldg(a.qin + 8 * a.plane + size_t(gi) * my + gj);
     }
     if (HYB) {
@@ -606,8 +617,8 @@ __global__ void __launch_bounds__(Cfg::NT, MhdMinBlocks<R>::value) k_mhd_stage(c
             const R u1 = qs[PQ + qe] * ir, u2 = qs[2 * PQ + qe] * ir;
             const double La = double(-u1 * R(0.5) * (xm + xp) - u2 * R(0.5) * (ym + yp)) +
                               (msx * 0.5 * double(xp - xm) + msy * 0.5 * double(yp - ym));
-            const int gi = bc_remap(i0 + ci, mx, FIN_BC_PERIODIC, FIN_BC_PERIODIC);
-            const int gj = bc_remap(j0 + cj, my, FIN_BC_PERIODIC, FIN_BC_PERIODIC);
+            const int gi = pwrap(i0 + ci, mx);
+            const int gj = pwrap(j0 + cj, my);
             const size_t g = 8 * a.plane + size_t(gi) * my + gj;
             double v = 0.0;
             if (a.A) v = a.a1 * __ldg(a.A + g);
@@ -866,7 +877,7 @@ __global__ void __launch_bounds__(Cfg::NT, MhdMinBlocks<R>::value) k_mhd_stage(c
         a.qout[8 * a.plane + g] = N[0];
         // next stage's maxima: GlobalWaveSpd.cpp:71-76 with Ql = Qr (each
         // direction's speed is |u_n| + the cell's fast speed) and the HJ speeds
-        const double ir = 1.0 / qn[0];
+        const double ir = rcp(qn[0]);
         const double u1 = qn[1] * ir, u2 = qn[2] * ir, u3 = qn[3] * ir;
         if (a.alpha_out) {
             const R Bsq = R(qn[5] * qn[5] + qn[6] * qn[6] + qn[7] * qn[7]);

@@ -7,12 +7,14 @@
 // the 6-point WENO stencil i-3 .. i+2 and the left eigenvectors at the face
 // average (ProjectLeftEig.cpp:179-192, in the structured form of
 // fin_mhd.cuh):
-//   features: w = L q at the six points; for each wave pair (fast 0/7, slow
-//     2/5, Alfven 1/6, entropy/divergence 3/4) the member with the larger
-//     undivided difference max_s |w(s+1) - w(s)| gives its 5 differences
-//     divided by max(that maximum, 1e-3): 20 values.  A pair's two members
-//     see different discontinuities (a pure fast-plus jump is orthogonal to
-//     the fast-minus row), hence the choice by activity;
+//   features: w = L q at the six points; for each of the eight fields k,
+//     with D_s = w_k(s+1) - w_k(s) and M = max_s |D_s|: the relative second
+//     difference max_s |D_(s+1) - D_s| / max(M, 1e-3) (in [0, 2]; large where
+//     the field is not smooth on the stencil) and the magnitude M / (M + 1e-3)
+//     (small where the field varies too little to move the WENO weights, beta
+//     ~ D^2 against epsilon = 1e-6); 16 values, the last 4 inputs zero.  One
+//     number pair per field keeps every field visible to the network, which
+//     the labels need: any of the eight can trigger;
 //   label: 1 when the WENO5-JS weights of gp or gm (ConstructL.cpp:179-192)
 //     of any of the eight fields depart from the linear weights (0.1, 0.6,
 //     0.3) by more than 10 % (lib/WenoReconstruct.cpp:104, 131-134).
@@ -47,30 +49,29 @@ __device__ __forceinline__ void features(const MhdArgs& a, R gamma, const R (&Qn
         w[0][s] = r0; w[7][s] = r7; w[2][s] = r2; w[5][s] = r5;
         w[1][s] = r1; w[6][s] = r6; w[3][s] = r3; w[4][s] = r4;
     }
-    constexpr int pa[4] = {0, 2, 1, 3}, pb[4] = {7, 5, 6, 4};
 #pragma unroll
-    for (int t = 0; t < 4; t++) {
-        R da[5], db[5], ma = R(0), mb = R(0);
+    for (int k = 0; k < MHD_NQ; k++) {
+        R d[5], M = R(0), S = R(0);
 #pragma unroll
         for (int s = 0; s < 5; s++) {
-            da[s] = w[pa[t]][s + 1] - w[pa[t]][s];
-            db[s] = w[pb[t]][s + 1] - w[pb[t]][s];
-            ma = Max(ma, R(fabs(da[s])));
-            mb = Max(mb, R(fabs(db[s])));
+            d[s] = w[k][s + 1] - w[k][s];
+            M = Max(M, R(fabs(d[s])));
         }
-        const bool useA = ma >= mb;
-        const R inv = R(1) / Max(useA ? ma : mb, R(FEAT_FLOOR));
 #pragma unroll
-        for (int s = 0; s < 5; s++) x[t * 5 + s] = float((useA ? da[s] : db[s]) * inv);
+        for (int s = 0; s < 4; s++) S = Max(S, R(fabs(d[s + 1] - d[s])));
+        x[2 * k] = float(S / Max(M, R(FEAT_FLOOR)));
+        x[2 * k + 1] = float(M / (M + R(FEAT_FLOOR)));
     }
+#pragma unroll
+    for (int k = 2 * MHD_NQ; k < ind::NFEAT; k++) x[k] = 0.0f;
 }
 
 // Stencil cell s (0..5) of face (isx, i, j) under the periodic remap.
 __device__ __forceinline__ size_t stencil_cell(bool isx, int i, int j, int s, int mx, int my)
 {
     const int ci = isx ? i + s - 3 : i, cj = isx ? j : j + s - 3;
-    return size_t(bc_remap(ci, mx, FIN_BC_PERIODIC, FIN_BC_PERIODIC)) * my +
-           bc_remap(cj, my, FIN_BC_PERIODIC, FIN_BC_PERIODIC);
+    return size_t(pwrap(ci, mx)) * my +
+           pwrap(cj, my);
 }
 
 // Label of one face (FP64): the reference's split (SetWaveSpd with the two
@@ -250,8 +251,8 @@ __global__ void __launch_bounds__(Cfg::NT, 2) k_mhd_indicator(const __grid_const
             const int ii = e / RJ, jj = e - ii * RJ;
             const bool xin = ii >= H && ii < H + TI, yin = jj >= H && jj < H + TJ;
             if (!xin && !yin) continue;
-            const int gi = bc_remap(i0 + ii - H, mx, FIN_BC_PERIODIC, FIN_BC_PERIODIC);
-            const int gj = bc_remap(j0 + jj - H, my, FIN_BC_PERIODIC, FIN_BC_PERIODIC);
+            const int gi = pwrap(i0 + ii - H, mx);
+            const int gj = pwrap(j0 + jj - H, my);
             const size_t g = size_t(gi) * my + gj;
 #pragma unroll
             for (int m = 0; m < MHD_NQ; m++) S.qs[m * PQ + e] = float(__ldg(a.qin + m * a.plane + g));

@@ -13,8 +13,8 @@ of the troubled faces are flagged.
     python -m finess_b200.train_indicator --physics mhd [--out PATH] [--samples 2000000]
 
 The MHD network (--physics mhd) is trained the same way on faces of ideal-MHD
-runs -- the Orszag-Tang vortex at 512^2 and 1024^2 through t = pi and smooth
-random periodic MHD states at 512^2 -- with the MHD features and labels
+runs -- the Orszag-Tang vortex at 512^2, 1024^2 and 2048^2 through t = pi
+and smooth random periodic MHD states at 512^2 -- with the MHD features and labels
 (fin_mhd_face_samples: the WENO5-JS weights of any of the eight
 characteristic fields).
 """
@@ -103,20 +103,26 @@ def _mhd_snapshots(p, q0, aux0, times, rng, per_snapshot):
 
 
 def generate_mhd(total=2_000_000, seed=0, verbose=True):
+    from ._abi import FIN_PREC_FP32
     rng = np.random.default_rng(seed)
     runs = []
-    for n, times in ((512, [0.0, 0.5, 1.0, 1.5, 2.0, 2.5, 3.0]), (1024, [0.5, 1.0, 1.5, 2.0, 2.5, math.pi])):
+    # (grid, times, form): 2048^2 runs in the FP32 form (the labels are
+    # computed in FP64 from the state either way)
+    for n, times, prec in ((512, [0.0, 0.5, 1.0, 1.5, 2.0, 2.5, 3.0], FIN_PREC_FP64),
+                           (1024, [0.5, 1.0, 1.5, 2.0, 2.5, math.pi], FIN_PREC_FP64),
+                           (2048, [0.5, 1.0, 1.5, 2.0, 2.5, math.pi], FIN_PREC_FP32)):
         p = P.orszag_tang_params(n=n)
+        p.precision = prec
         q, aux = P.orszag_tang_init(p)
         runs.append((p, q, aux, times))
     for k in range(4):
         p = P.orszag_tang_params(n=512)
+        p.precision = FIN_PREC_FP64
         q, aux = P.mhd_random_state(p, rng, amp=0.3)
         runs.append((p, q, aux, [0.0, 0.3, 0.8]))
     per = total // sum(len(r[3]) for r in runs) + 1
     Xs, ys = [], []
     for p, q0, aux0, times in runs:
-        p.precision = FIN_PREC_FP64
         t0 = time.time()
         X, y = _mhd_snapshots(p, q0, aux0, times, rng, per)
         Xs += X

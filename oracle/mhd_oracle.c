@@ -669,10 +669,9 @@ void oracle_orszag_tang(const fin_params* p, double* q, double* aux)
  * fastest), for the face between cells i-1 and i (1-based i = f_i + 1) with
  * the 6-point stencil i-3 .. i+2:
  *   w = Lmat q at the six points, Lmat the left eigenvectors at the face
- *   average (ProjectLeftEig.cpp:179-192); for each wave pair (fast 0/7,
- *   slow 2/5, Alfven 1/6, entropy/divergence 3/4) the member with the larger
- *   undivided difference max_s |w(s+1) - w(s)| gives 5 features, its
- *   differences divided by max(that maximum, 1e-3): 20 features;
+ *   average (ProjectLeftEig.cpp:179-192); for each of the eight fields, with
+ *   D_s = w(s+1) - w(s) and M = max |D_s|: max |D_(s+1) - D_s| / max(M, 1e-3)
+ *   and M / (M + 1e-3); 16 features, the last 4 of 20 zero;
  *   label: 1 when the WENO5-JS weights of gp or gm (ConstructL.cpp:179-192)
  *   of any of the eight fields depart from (0.1, 0.6, 0.3) by more than 10 %
  *   (lib/WenoReconstruct.cpp:104, 131-134). */
@@ -681,7 +680,6 @@ void oracle_mhd_face_samples(const fin_params* p, const double* q, double* X, un
     const mgrid_t g = mgrid(p, p->mx, p->my, MQ);
     double alpha1 = 0., alpha2 = 0.;
     if (p->global_alpha) oracle_mhd_global_wave_spd(p, q, &alpha1, &alpha2);
-    static const int pairs[4][2] = {{0, 7}, {2, 5}, {1, 6}, {3, 4}};
     static const double dl[3] = {0.1, 0.6, 0.3};
     long long f = 0;
     for (int ixy = 1; ixy <= 2; ixy++) {
@@ -706,17 +704,18 @@ void oracle_mhd_face_samples(const fin_params* p, const double* q, double* X, un
                     matvec8(Lm, Qs[s], W[s]);
                     matvec8(Lm, Fs[s], G[s]);
                 }
-                for (int t = 0; t < 4; t++) {
-                    double d[2][5], mm[2] = {0.0, 0.0};
-                    for (int c = 0; c < 2; c++)
-                        for (int s = 0; s < 5; s++) {
-                            d[c][s] = W[s + 1][pairs[t][c]] - W[s][pairs[t][c]];
-                            if (fabs(d[c][s]) > mm[c]) mm[c] = fabs(d[c][s]);
-                        }
-                    const int c = mm[0] >= mm[1] ? 0 : 1;
-                    const double den = mm[c] > 1e-3 ? mm[c] : 1e-3;
-                    for (int s = 0; s < 5; s++) X[f * 20 + t * 5 + s] = d[c][s] / den;
+                for (int k = 0; k < MQ; k++) {
+                    double d[5], M = 0.0, S = 0.0;
+                    for (int s = 0; s < 5; s++) {
+                        d[s] = W[s + 1][k] - W[s][k];
+                        if (fabs(d[s]) > M) M = fabs(d[s]);
+                    }
+                    for (int s = 0; s < 4; s++)
+                        if (fabs(d[s + 1] - d[s]) > S) S = fabs(d[s + 1] - d[s]);
+                    X[f * 20 + 2 * k] = S / (M > 1e-3 ? M : 1e-3);
+                    X[f * 20 + 2 * k + 1] = M / (M + 1e-3);
                 }
+                for (int k = 16; k < 20; k++) X[f * 20 + k] = 0.0;
                 double s1, s2;
                 mhd_wave_spd(p->gamma, ixy == 1 ? 1.0 : 0.0, ixy == 1 ? 0.0 : 1.0, Qs[2], Qs[3], &s1, &s2);
                 const double alpha = Max(ixy == 1 ? alpha1 : alpha2, Max(fabs(s1), fabs(s2)));
