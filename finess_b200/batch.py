@@ -8,7 +8,7 @@ log-uniform in [64, 1024]; quadrant states rho ~ U[0.1, 2], u, v ~
 U[-1.5, 1.5], p ~ U[0.02, 2]; interface ~ U[0.3, 0.7]^2; transmissive
 boundaries; CFL 0.4) from a seed.
 
-    python -m finess_b200.batch [--n 1024] [--tend 0.25] [--seed 0] [--precision fp32] [--separate]
+    python -m finess_b200.batch [--n 1024] [--tend 0.25] [--seed 0] [--precision fp32|fp64|hybrid] [--separate]
 """
 import argparse
 import ctypes as C
@@ -18,7 +18,7 @@ import math
 import numpy as np
 
 from . import problems as P
-from ._abi import FIN_OK, FIN_PREC_FP32, FIN_PREC_FP64, FIN_WENO_Z, FinParams, ghosted_shape
+from ._abi import FIN_OK, FIN_PREC_FP32, FIN_PREC_FP64, FIN_PREC_HYBRID, FIN_WENO_Z, FinParams, ghosted_shape
 from .solver import FinError, Solver, load_library
 
 _dp = np.ctypeslib.ndpointer(dtype=np.float64, flags="C_CONTIGUOUS")
@@ -35,9 +35,14 @@ def _lib():
         lib.fin_batch_solve.argtypes = [vp, C.c_double, _dp, np.ctypeslib.ndpointer(np.int32, flags="C_CONTIGUOUS")]
         lib.fin_batch_stats.argtypes = [vp, C.POINTER(C.c_double), C.POINTER(C.c_longlong), C.POINTER(C.c_int),
                                         np.ctypeslib.ndpointer(np.float64, flags="C_CONTIGUOUS")]
+        lib.fin_batch_set_indicator.argtypes = [vp, np.ctypeslib.ndpointer(np.float32, flags="C_CONTIGUOUS"),
+                                                C.c_float, C.c_int, C.c_double]
+        lib.fin_batch_set_indicator_every.argtypes = [vp, C.c_int]
+        lib.fin_batch_hybrid_stats.argtypes = [vp] + [C.POINTER(C.c_longlong)] * 4
         lib.fin_batch_last_error.restype = C.c_char_p
         for n in ("fin_batch_create", "fin_batch_destroy", "fin_batch_set_state", "fin_batch_get_state",
-                  "fin_batch_solve", "fin_batch_stats"):
+                  "fin_batch_solve", "fin_batch_stats", "fin_batch_set_indicator", "fin_batch_set_indicator_every",
+                  "fin_batch_hybrid_stats"):
             getattr(lib, n).restype = C.c_int
         lib._batch_bound = True
     return lib
@@ -94,6 +99,19 @@ class Batch:
         _check(self.lib, self.lib.fin_batch_solve(self.h, tend, dtv, steps))
         return dtv, steps
 
+    def set_indicator(self, params, z_threshold=0.0, judge_every=20, judge_tol=1e-3, every=1):
+        """Hybrid form: the troubled-face network, the judge step and the
+        indicator's period in accepted steps, for every problem (as
+        ``Solver.set_indicator``)."""
+        _check(self.lib, self.lib.fin_batch_set_indicator(self.h, np.ascontiguousarray(params, dtype=np.float32),
+                                                          z_threshold, judge_every, judge_tol))
+        _check(self.lib, self.lib.fin_batch_set_indicator_every(self.h, every))
+
+    def hybrid_stats(self):
+        v = [C.c_longlong() for _ in range(4)]
+        _check(self.lib, self.lib.fin_batch_hybrid_stats(self.h, *[C.byref(x) for x in v]))
+        return {"troubled_faces": v[0].value, "faces": v[1].value, "judges": v[2].value, "reverts": v[3].value}
+
     def stats(self):
         ms, reps, cfg = C.c_double(), C.c_longlong(), C.c_int()
         tune = np.zeros(2)
@@ -134,33 +152,61 @@ def first_dt(p, q):
     return p.desired_cfl * min((p.xhigh - p.xlow) / p.mx, (p.yhigh - p.ylow) / p.my) / a
 
 
-def run_sweep(n=1024, tend=0.25, seed=0, precision=FIN_PREC_FP32, separate=False):
+# Hybrid-form schedule of the sweep (as the single-problem benchmark's): the
+# indicator every 2nd accepted step, every 50th hybrid step judged against a
+# full-WENO step with tolerance 1e-3.
+HYB_EVERY, HYB_JUDGE_EVERY, HYB_JUDGE_TOL = 2, 50, 1e-3
+PRECISIONS = {"fp64": FIN_PREC_FP64, "fp32": FIN_PREC_FP32, "hybrid": FIN_PREC_HYBRID}
+
+
+def load_indicator(path=None):
+    """(network parameters, z threshold) of the trained troubled-face network."""
+    from .indicator import DEFAULT_WEIGHTS
+    W = np.load(path or DEFAULT_WEIGHTS)
+    return W["params"], float(W["z_threshold"])
+
+
+def run_sweep(n=1024, tend=0.25, seed=0, precision=FIN_PREC_FP32, separate=False, indicator=None):
     """The sweep batched (one persistent launch per stage over all problems)
     and, optionally, every problem run on its own; device times and
-    cell-updates/s of both."""
+    cell-updates/s of both.  The hybrid form takes indicator = (params,
+    z threshold), by default the trained network."""
+    hyb = precision == FIN_PREC_HYBRID
+    if hyb and indicator is None:
+        indicator = load_indicator()
     params = [_sweep_grid(seed, k, precision=precision) for k in range(n)]
     cells = np.array([p.mx * p.my for p in params], dtype=np.float64)
     dts = np.zeros(n)
-    out = {"problems": n, "seed": seed, "tend": tend, "precision": "fp32" if precision == FIN_PREC_FP32 else "fp64",
+    name = {v: k for k, v in PRECISIONS.items()}[precision]
+    out = {"problems": n, "seed": seed, "tend": tend, "precision": name,
            "grid_min": int(min(p.mx for p in params)), "grid_max": int(max(p.mx for p in params)),
            "cells_total": float(cells.sum())}
     with Batch(params) as b:
+        if hyb:
+            b.set_indicator(indicator[0], indicator[1], HYB_JUDGE_EVERY, HYB_JUDGE_TOL, HYB_EVERY)
         for k in range(n):
             p, q = sweep_problem(seed, k, precision=precision)
             dts[k] = first_dt(p, q)
             b.set_state(k, q)
         _, steps = b.solve(tend, dts)
         st = b.stats()
+        hst = b.hybrid_stats() if hyb else None
     cu = float(np.sum(cells * steps))
     out["batched"] = {"cell_updates": cu, "device_s": st["device_ms"] * 1e-3,
                       "cell_updates_per_s": cu / (st["device_ms"] * 1e-3), "steps_max": int(steps.max()),
                       "graph_replays": st["replays"], "tile_shape": st["tile_shape"],
                       "autotune_stage1_ms": st["tune_stage_ms"]}
+    if hyb:
+        out["batched"]["hybrid"] = dict(hst, troubled_fraction=hst["troubled_faces"] / max(hst["faces"], 1),
+                                        indicator_every=HYB_EVERY, judge_every=HYB_JUDGE_EVERY,
+                                        judge_tol=HYB_JUDGE_TOL)
     if separate:
         tot = 0.0
         for k in range(n):
             p, q = sweep_problem(seed, k, precision=precision)
             with Solver(p) as s:
+                if hyb:
+                    s.set_indicator(indicator[0], indicator[1], HYB_JUDGE_EVERY, HYB_JUDGE_TOL, HYB_EVERY)
                 s.set_state(q)
                 s.FinSolveRK(tend, np.array([0.0, dts[k], p.max_dt]))
                 tot += s.last_kernel_ms() * 1e-3
@@ -174,11 +220,10 @@ def main():
     ap.add_argument("--n", type=int, default=1024)
     ap.add_argument("--tend", type=float, default=0.25)
     ap.add_argument("--seed", type=int, default=0)
-    ap.add_argument("--precision", default="fp32", choices=["fp32", "fp64"])
+    ap.add_argument("--precision", default="fp32", choices=sorted(PRECISIONS))
     ap.add_argument("--separate", action="store_true", help="also run every problem on its own")
     a = ap.parse_args()
-    print(json.dumps(run_sweep(a.n, a.tend, a.seed, FIN_PREC_FP32 if a.precision == "fp32" else FIN_PREC_FP64,
-                               a.separate)))
+    print(json.dumps(run_sweep(a.n, a.tend, a.seed, PRECISIONS[a.precision], a.separate)))
 
 
 if __name__ == "__main__":

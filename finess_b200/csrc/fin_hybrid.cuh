@@ -16,7 +16,8 @@ struct IndicatorArgs {
     float gamma;
     const float* P;            // network parameters (FP32, mlp::NPARAM)
     float zthr;                // a face is troubled when its logit exceeds zthr
-    unsigned* flags;           // bit masks (flag_wx / flag_wy layout), zeroed before the launch
+    unsigned* flags;           // bit masks (flag_wx / flag_wy layout); zeroed once when allocated
+                               // (every owned face's bit is rewritten per run)
     unsigned int* status;
     unsigned long long* count; // troubled faces (accumulated)
     int tma;                   // tm maps q (box (TJ+8) x (TI+6) x 5, as the stage kernel's)
@@ -92,29 +93,148 @@ struct IndTile {
     unsigned int cnt;
 };
 
-// One flag per face of the state a.q.  Persistent CTAs walk the stage
-// kernel's TI x TJ cell tiles; per tile the CTA owns the x faces of rows
-// i0 .. i0+TI-1 and the y faces of columns j0 .. j0+TJ-1 (the last tile row /
+// Steps 2-5 of the indicator for the cell tile (i0, j0) whose FP32 state
+// (tile + halo) is in S.qs: the features of the tile's faces, the network on
+// tcgen05 and the flags.  Per tile the CTA owns the x faces of rows i0 ..
+// i0+TI-1 and the y faces of columns j0 .. j0+TJ-1 (the last tile row /
 // column also the domain's last face row / column): at most 511 faces, laid
 // out as four 128-row matrices (slots 0..255 x faces (fi, fj) = (s / 16,
 // s % 16), slots 256..510 y faces (fi, fj) = ((s-256) / 17, (s-256) % 17)).
-//   1. q's tile + halo: TMA (prefetched during the previous tile) or remap
-//      loads, FP64 -> FP32 in shared memory;
 //   2. each thread: the features of its two slots from shared memory;
 //   3. layer 1 on tcgen05 (4 x two K=16 steps into TMEM columns 0..127);
 //   4. 2 gelu, BF16, back into the X matrices; layer 2 into the same columns;
 //   5. 2 gelu + b2 -> output layer in FP32 -> flag.
 // TMEM lane quarter q = warp % 4 holds rows 32q .. 32q+31 of every matrix;
-// warps 0-3 take matrices 0 and 1, warps 4-7 matrices 2 and 3.
+// warps 0-3 take matrices 0 and 1, warps 4-7 matrices 2 and 3.  Every owned
+// face's bit is written (set or cleared, one AND and one OR per flag word
+// and warp), so the flags need no clearing between runs; bits that no face
+// owns are never touched.  Sets S.abort when a tensor-core wait ran out
+// (uniform across the CTA on return).
+template <class Cfg>
+__device__ __forceinline__ void indicator_tile(IndTile<Cfg>& S, const int mx, const int my, const float gamma,
+                                               const float zthr, unsigned* flags, const int i0, const int j0,
+                                               const uint32_t tmem, uint32_t& mma_phase)
+{
+    using namespace mlp;
+    constexpr int TI = Cfg::TI, TJ = Cfg::TJ, H = Cfg::H, RJ = Cfg::RJ, PQ = Cfg::RI * Cfg::RJ;
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const uint32_t lane_base = uint32_t((warp & 3) * 32) << 16;
+    // ---- 2. features of the thread's two slots ----
+    long long fword[2];   // flag word of the slot's face (-1: not owned)
+    unsigned fbit[2];
+    const int wx = flag_wx(my), wy = flag_wy(my);
+#pragma unroll 1
+    for (int h = 0; h < 2; h++) {
+        const int mt = 2 * (warp >> 2) + h, row = 32 * (warp & 3) + lane, sl = 128 * mt + row;
+        float xr[KIN];
+#pragma unroll
+        for (int k = 0; k < KIN; k++) xr[k] = 0.0f;
+        fword[h] = -1;
+        fbit[h] = 0;
+        bool isx = sl < 256;
+        int fi, fj;
+        if (isx) { fi = sl >> 4; fj = sl & 15; }
+        else { const int v = sl - 256; fi = v / (TJ + 1); fj = v - fi * (TJ + 1); }
+        const int gi = i0 + fi, gj = j0 + fj;
+        bool own;
+        if (isx) own = gj < my && gi <= mx && (fi < TI || gi == mx);
+        else own = sl < 511 && gi < mx && gj <= my && (fj < TJ || gj == my);
+        if (own) {
+            fword[h] = isx ? (long long)gi * wx + (gj >> 5) : (long long)(mx + 1) * wx + (long long)gi * wy + (gj >> 5);
+            fbit[h] = 1u << (gj & 31);
+            const int cn = isx ? 1 : 2, ct = isx ? 2 : 1;
+            const int base = isx ? (H + fi - 3) * RJ + (H + fj) : (H + fi) * RJ + (H + fj - 3);
+            const int str = isx ? RJ : 1;
+            float Q[6][MEQN];
+#pragma unroll
+            for (int st = 0; st < 6; st++) {
+                const int o = base + st * str;
+                Q[st][0] = S.qs[o];
+                Q[st][1] = S.qs[cn * PQ + o];
+                Q[st][2] = S.qs[ct * PQ + o];
+                Q[st][3] = S.qs[3 * PQ + o];
+                Q[st][4] = S.qs[4 * PQ + o];
+            }
+            ind::stencil_features<float>(Q, gamma, xr);
+            xr[NIN] = 1.0f;   // the layer-1 bias input
+        }
+        store_row32(S.X + mt * 128 * KIN, row, xr);
+    }
+    tc::fence_smem_to_async();
+    tc::fence_before_sync();
+    __syncthreads();
+    // ---- 3. layer 1 ----
+    if (tid == 0) {
+        tc::fence_after_sync();
+#pragma unroll
+        for (int mt = 0; mt < 4; mt++) ind::mma_128x32x32(tmem + 32 * mt, S.X + mt * 128 * KIN, S.w.W1);
+        tc::commit(&S.mbar_mma);
+    }
+    if (!tc::mbar_wait(&S.mbar_mma, mma_phase)) S.abort = 1;
+    mma_phase ^= 1;
+    tc::fence_after_sync();
+    // ---- 4. 2 gelu of layer 1 into the X matrices; layer 2 ----
+#pragma unroll 1
+    for (int h = 0; h < 2; h++) {
+        const int mt = 2 * (warp >> 2) + h, row = 32 * (warp & 3) + lane;
+        float v[32];
+        tc::tmem_ld32(tmem + lane_base + 32 * mt, v);
+#pragma unroll
+        for (int o = 0; o < NH; o++) v[o] = ind::gelu2(v[o]);
+        store_row32(S.X + mt * 128 * KIN, row, v);
+    }
+    tc::fence_smem_to_async();
+    tc::fence_before_sync();
+    __syncthreads();
+    if (S.abort) return;
+    if (tid == 0) {
+        tc::fence_after_sync();
+#pragma unroll
+        for (int mt = 0; mt < 4; mt++) ind::mma_128x32x32(tmem + 32 * mt, S.X + mt * 128 * KIN, S.w.W2);
+        tc::commit(&S.mbar_mma);
+    }
+    if (!tc::mbar_wait(&S.mbar_mma, mma_phase)) S.abort = 1;
+    mma_phase ^= 1;
+    tc::fence_after_sync();
+    // ---- 5. output layer and flags ----
+#pragma unroll 1
+    for (int h = 0; h < 2; h++) {
+        const int mt = 2 * (warp >> 2) + h;
+        float v[32];
+        tc::tmem_ld32(tmem + lane_base + 32 * mt, v);
+        float zz = S.w.b3;
+#pragma unroll
+        for (int o = 0; o < NH; o++) zz = fmaf(S.w.w3h[o], ind::gelu2(v[o] + S.w.b2[o]), zz);
+        const bool fl = fword[h] >= 0 && zz > zthr;
+        // lanes on one flag word combine their bits; the group's first lane
+        // clears the owned bits that are not flagged and sets the others
+        const unsigned grp = __match_any_sync(0xffffffffu, (unsigned long long)fword[h]);
+        const unsigned setb = __reduce_or_sync(grp, fl ? fbit[h] : 0u);
+        const unsigned ownb = __reduce_or_sync(grp, fbit[h]);
+        if (fword[h] >= 0 && lane == __ffs(grp) - 1) {
+            if (ownb & ~setb) atomicAnd(flags + fword[h], ~(ownb & ~setb));
+            if (setb) atomicOr(flags + fword[h], setb);
+        }
+        const unsigned bal = __ballot_sync(0xffffffffu, fl);
+        if (lane == 0 && bal) atomicAdd(&S.cnt, unsigned(__popc(bal)));
+    }
+    tc::fence_before_sync();
+    __syncthreads();
+}
+
+// One flag per face of the state a.q.  Persistent CTAs walk the stage
+// kernel's TI x TJ cell tiles; per tile
+//   1. q's tile + halo: TMA (prefetched during the previous tile) or remap
+//      loads, FP64 -> FP32 in shared memory;
+//   2-5. indicator_tile.
 template <class Cfg>
 __global__ void __launch_bounds__(Cfg::NT, 3) k_indicator(const __grid_constant__ IndicatorArgs a)
 {
-    using namespace mlp;
-    constexpr int TI = Cfg::TI, TJ = Cfg::TJ, H = Cfg::H, RI = Cfg::RI, RJ = Cfg::RJ, PQ = RI * RJ;
+    constexpr int TI = Cfg::TI, TJ = Cfg::TJ, H = Cfg::H;
     static_assert(Cfg::NT == 256 && (TI + 1) * TJ <= 256 && TI * (TJ + 1) <= 255 && TJ == 16, "face slots");
     extern __shared__ __align__(128) unsigned char smem_raw[];
     IndTile<Cfg>& S = *reinterpret_cast<IndTile<Cfg>*>(smem_raw);
-    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const int tid = threadIdx.x, warp = tid >> 5;
     ind::load_ind_weights(S.w, a.P, tid, Cfg::NT);
     if (warp == 0) tc::tmem_alloc(&S.tmem, 128);
     if (tid == 0) {
@@ -128,7 +248,6 @@ __global__ void __launch_bounds__(Cfg::NT, 3) k_indicator(const __grid_constant_
     __syncthreads();
     tc::fence_after_sync();
     const uint32_t tmem = S.tmem;
-    const uint32_t lane_base = uint32_t((warp & 3) * 32) << 16;
     const int mx = a.mx, my = a.my;
     const int ntj = (my + TJ - 1) / TJ;
     const long long ntiles = (long long)((mx + TI - 1) / TI) * ntj;
@@ -165,99 +284,7 @@ __global__ void __launch_bounds__(Cfg::NT, 3) k_indicator(const __grid_constant_
         __syncthreads();
         if (S.abort) { pending = false; break; }
         pending = t + gridDim.x < ntiles ? issue(t + gridDim.x) : false;
-        // ---- 2. features of the thread's two slots ----
-        long long fword[2];   // flag word of the slot's face (-1: not owned)
-        unsigned fbit[2];
-        const int wx = flag_wx(my), wy = flag_wy(my);
-#pragma unroll 1
-        for (int h = 0; h < 2; h++) {
-            const int mt = 2 * (warp >> 2) + h, row = 32 * (warp & 3) + lane, sl = 128 * mt + row;
-            float xr[KIN];
-#pragma unroll
-            for (int k = 0; k < KIN; k++) xr[k] = 0.0f;
-            fword[h] = -1;
-            fbit[h] = 0;
-            bool isx = sl < 256;
-            int fi, fj;
-            if (isx) { fi = sl >> 4; fj = sl & 15; }
-            else { const int v = sl - 256; fi = v / (TJ + 1); fj = v - fi * (TJ + 1); }
-            const int gi = i0 + fi, gj = j0 + fj;
-            bool own;
-            if (isx) own = gj < my && gi <= mx && (fi < TI || gi == mx);
-            else own = sl < 511 && gi < mx && gj <= my && (fj < TJ || gj == my);
-            if (own) {
-                fword[h] = isx ? (long long)gi * wx + (gj >> 5) : (long long)(mx + 1) * wx + (long long)gi * wy + (gj >> 5);
-                fbit[h] = 1u << (gj & 31);
-                const int cn = isx ? 1 : 2, ct = isx ? 2 : 1;
-                const int base = isx ? (H + fi - 3) * RJ + (H + fj) : (H + fi) * RJ + (H + fj - 3);
-                const int str = isx ? RJ : 1;
-                float Q[6][MEQN];
-#pragma unroll
-                for (int st = 0; st < 6; st++) {
-                    const int o = base + st * str;
-                    Q[st][0] = S.qs[o];
-                    Q[st][1] = S.qs[cn * PQ + o];
-                    Q[st][2] = S.qs[ct * PQ + o];
-                    Q[st][3] = S.qs[3 * PQ + o];
-                    Q[st][4] = S.qs[4 * PQ + o];
-                }
-                ind::stencil_features<float>(Q, a.gamma, xr);
-                xr[NIN] = 1.0f;   // the layer-1 bias input
-            }
-            store_row32(S.X + mt * 128 * KIN, row, xr);
-        }
-        tc::fence_smem_to_async();
-        tc::fence_before_sync();
-        __syncthreads();
-        // ---- 3. layer 1 ----
-        if (tid == 0) {
-            tc::fence_after_sync();
-#pragma unroll
-            for (int mt = 0; mt < 4; mt++) ind::mma_128x32x32(tmem + 32 * mt, S.X + mt * 128 * KIN, S.w.W1);
-            tc::commit(&S.mbar_mma);
-        }
-        if (!tc::mbar_wait(&S.mbar_mma, mma_phase)) S.abort = 1;
-        mma_phase ^= 1;
-        tc::fence_after_sync();
-        // ---- 4. 2 gelu of layer 1 into the X matrices; layer 2 ----
-#pragma unroll 1
-        for (int h = 0; h < 2; h++) {
-            const int mt = 2 * (warp >> 2) + h, row = 32 * (warp & 3) + lane;
-            float v[32];
-            tc::tmem_ld32(tmem + lane_base + 32 * mt, v);
-#pragma unroll
-            for (int o = 0; o < NH; o++) v[o] = ind::gelu2(v[o]);
-            store_row32(S.X + mt * 128 * KIN, row, v);
-        }
-        tc::fence_smem_to_async();
-        tc::fence_before_sync();
-        __syncthreads();
-        if (S.abort) break;
-        if (tid == 0) {
-            tc::fence_after_sync();
-#pragma unroll
-            for (int mt = 0; mt < 4; mt++) ind::mma_128x32x32(tmem + 32 * mt, S.X + mt * 128 * KIN, S.w.W2);
-            tc::commit(&S.mbar_mma);
-        }
-        if (!tc::mbar_wait(&S.mbar_mma, mma_phase)) S.abort = 1;
-        mma_phase ^= 1;
-        tc::fence_after_sync();
-        // ---- 5. output layer and flags ----
-#pragma unroll 1
-        for (int h = 0; h < 2; h++) {
-            const int mt = 2 * (warp >> 2) + h;
-            float v[32];
-            tc::tmem_ld32(tmem + lane_base + 32 * mt, v);
-            float zz = S.w.b3;
-#pragma unroll
-            for (int o = 0; o < NH; o++) zz = fmaf(S.w.w3h[o], ind::gelu2(v[o] + S.w.b2[o]), zz);
-            const bool fl = fword[h] >= 0 && zz > a.zthr;
-            if (fl) atomicOr(a.flags + fword[h], fbit[h]);
-            const unsigned bal = __ballot_sync(0xffffffffu, fl);
-            if (lane == 0 && bal) atomicAdd(&S.cnt, unsigned(__popc(bal)));
-        }
-        tc::fence_before_sync();
-        __syncthreads();
+        indicator_tile<Cfg>(S, mx, my, a.gamma, a.zthr, a.flags, i0, j0, tmem, mma_phase);
         if (S.abort) break;
     }
     // a copy still in flight lands before the shared memory is released

@@ -118,8 +118,12 @@ __device__ __forceinline__ void hyb_troubled_face(int w, const float2* fqx, cons
     }
 }
 
+// One stage on the cell tile (i0, j0) of the state a describes.  With a.tma
+// the tile's copies run on an mbarrier initialised here, so a CTA calls this
+// once (k_stage_hyb); a persistent caller that walks several tiles passes
+// a.tma = 0 and separates the calls by a barrier.
 template <int VER, bool P2, class Cfg>
-__global__ void __launch_bounds__(Cfg::NT, FIN_HYB_CTAS) k_stage_hyb(const __grid_constant__ StageArgs a)
+__device__ __forceinline__ void stage_hyb_tile(const StageArgs& a, const int i0, const int j0)
 {
     using R = float;
     using L = HybSmem<Cfg>;
@@ -143,9 +147,6 @@ __global__ void __launch_bounds__(Cfg::NT, FIN_HYB_CTAS) k_stage_hyb(const __gri
 
     const int tid = threadIdx.x, lane = tid & 31;
     const int mx = a.mx, my = a.my;
-    const int ntj = (my + TJ - 1) / TJ;
-    const int t = blockIdx.x;
-    const int i0 = (t / ntj) * TI, j0 = (t % ntj) * TJ;
     const float gam = a.gamma_f, eps = a.eps_f, pw = a.pw_f, ash = 0.5f * a.alpha_scaling_f;
     const float ag1 = a.alpha_in ? float(a.alpha_in[0]) : 0.0f;
     const float ag2 = a.alpha_in ? float(a.alpha_in[1]) : 0.0f;
@@ -382,6 +383,15 @@ __global__ void __launch_bounds__(Cfg::NT, FIN_HYB_CTAS) k_stage_hyb(const __gri
         double* dst = tid < 2 ? a.smax_out : a.alpha_out;
         if (dst) atomic_max_nonneg(dst + (tid & 1), v);
     }
+}
+
+// One CTA per tile of the state.
+template <int VER, bool P2, class Cfg>
+__global__ void __launch_bounds__(Cfg::NT, FIN_HYB_CTAS) k_stage_hyb(const __grid_constant__ StageArgs a)
+{
+    const int ntj = (a.my + Cfg::TJ - 1) / Cfg::TJ;
+    const int t = blockIdx.x;
+    stage_hyb_tile<VER, P2, Cfg>(a, (t / ntj) * Cfg::TI, (t % ntj) * Cfg::TJ);
 }
 
 }  // namespace fin

@@ -239,13 +239,15 @@ int fin_face_samples(fin_solver* s, long long offset, long long stride, long lon
 /* No single counterpart in the reference (an application would run
  * FinSolveRK, lib/2d/FinSolveRK.cpp:13, once per problem).  A batch holds
  * nprob independent 2D Euler problems of any grid sizes (params[k]: grid,
- * domain, boundaries, CFL numbers and nv per problem; precision (FP64 or
- * FP32), WENO version, power, epsilon, gamma, alpha_scaling and global_alpha
- * shared; SSP-RK3) and advances all of them to one end time, each with its
- * own adaptive dt: per problem the arithmetic and the step control are
- * fin_solve's, so the results agree with separate runs to rounding; the
- * stages of all problems run as one launch each, from a work queue of tiles.  States are passed in
- * the reference's ghosted layout of each problem, as fin_set_state. */
+ * domain, boundaries, CFL numbers and nv per problem; precision (FP64, FP32
+ * or hybrid), WENO version, power, epsilon, gamma, alpha_scaling and
+ * global_alpha shared; SSP-RK3) and advances all of them to one end time,
+ * each with its own adaptive dt: per problem the arithmetic and the step
+ * control are fin_solve's (in the hybrid form also the indicator's period,
+ * the judge step and the revert), so the results agree with separate runs to
+ * rounding; the stages of all problems run as one launch each, from a work
+ * queue of tiles.  States are passed in the reference's ghosted layout of
+ * each problem, as fin_set_state. */
 typedef struct fin_batch fin_batch;
 int fin_batch_create(const fin_params* params, int nprob, fin_batch** out);
 int fin_batch_destroy(fin_batch* b);
@@ -260,6 +262,16 @@ int fin_batch_solve(fin_batch* b, double tend, double* dtv1, int* steps);
  * active problem), the tile shape the autotuner chose (0: 15x16, 1: 7x32)
  * and its stage-1 times for both (tune_ms[2]). */
 int fin_batch_stats(fin_batch* b, double* device_ms, long long* replays, int* tile_cfg, double* tune_ms);
+/* Hybrid form (a batch created with precision FIN_PREC_HYBRID): as
+ * fin_set_indicator / fin_set_indicator_every, for every problem of the
+ * batch.  Until fin_batch_set_indicator the batch runs the plain FP32 form;
+ * after it the tile shape is the hybrid kernels' 15x16. */
+int fin_batch_set_indicator(fin_batch* b, const float* params, float z_threshold, int judge_every, double judge_tol);
+int fin_batch_set_indicator_every(fin_batch* b, int every);
+/* Troubled faces the indicator flagged and faces it ran on (summed over
+ * its runs), judge steps and reverts, summed over the problems. */
+int fin_batch_hybrid_stats(fin_batch* b, long long* troubled_faces, long long* faces, long long* judges,
+                           long long* reverts);
 const char* fin_batch_last_error(void);
 
 /* ---- for callers that cannot allocate device memory ------------------- */

@@ -60,6 +60,49 @@ def test_batch_equals_separate_runs(oracle, precision):
         assert rel_linf(interior(p, qb), interior(p, qs)) <= tol, k
 
 
+@pytest.mark.parametrize("judge_every,judge_tol,every", [(4, 1e-3, 2), (3, 0.0, 1)])
+def test_batch_hybrid_equals_separate_runs(oracle, judge_every, judge_tol, every):
+    """The hybrid form batched: per problem the same indicator period, judge
+    steps and reverts (judge_tol 0 reverts every judged step, so the plain
+    attempts that follow and the buffer swap run too) as a separate hybrid
+    run, the same steps, and the state to FP32 rounding."""
+    from finess_b200.batch import Batch, first_dt, load_indicator
+    from finess_b200.solver import Solver
+    from finess_b200._abi import FIN_PREC_HYBRID
+    ind = load_indicator()
+    params, states = _problems(FIN_PREC_HYBRID)
+    states = [oracle.set_bnd(p, q) for p, q in zip(params, states)]
+    tend = 0.05
+    dts = np.array([first_dt(p, q) for p, q in zip(params, states)])
+    with Batch(params) as b:
+        b.set_indicator(ind[0], ind[1], judge_every, judge_tol, every)
+        for k, q in enumerate(states):
+            b.set_state(k, q)
+        dt_out, steps = b.solve(tend, dts)
+        got = [b.get_state(k) for k in range(len(params))]
+        hst = b.hybrid_stats()
+    judges = reverts = 0
+    for k, (p, q) in enumerate(zip(params, states)):
+        with Solver(p) as s:
+            s.set_indicator(ind[0], ind[1], judge_every, judge_tol, every)
+            s.set_state(q)
+            dtv, n = s.FinSolveRK(tend, np.array([0.0, dts[k], p.max_dt]))
+            qs, ts = s.get_state()
+            st = s.hybrid_stats()
+        judges += st["judges"]
+        reverts += st["reverts"]
+        qb, tb = got[k]
+        assert steps[k] == n, (k, steps[k], n)
+        assert abs(dt_out[k] - dtv[1]) <= 1e-5 * dtv[1], (k, dt_out[k], dtv[1])
+        assert abs(tb - ts) <= 1e-14 * max(1.0, abs(ts))
+        assert rel_linf(interior(p, qb), interior(p, qs)) <= 1e-5, k
+    assert hst["judges"] == judges and hst["reverts"] == reverts
+    assert judges > 0
+    if judge_tol == 0.0:
+        assert reverts > 0
+    assert 0 < hst["troubled_faces"] < hst["faces"]
+
+
 def test_batch_rejects_mixed_forms():
     from finess_b200.batch import Batch
     from finess_b200.solver import FinError
