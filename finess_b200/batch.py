@@ -39,10 +39,12 @@ def _lib():
                                                 C.c_float, C.c_int, C.c_double]
         lib.fin_batch_set_indicator_every.argtypes = [vp, C.c_int]
         lib.fin_batch_hybrid_stats.argtypes = [vp] + [C.POINTER(C.c_longlong)] * 4
+        lib.fin_batch_set_kernel_timing.argtypes = [vp, C.c_int]
+        lib.fin_batch_kernel_times.argtypes = [vp, np.ctypeslib.ndpointer(np.float64, flags="C_CONTIGUOUS")]
         lib.fin_batch_last_error.restype = C.c_char_p
         for n in ("fin_batch_create", "fin_batch_destroy", "fin_batch_set_state", "fin_batch_get_state",
                   "fin_batch_solve", "fin_batch_stats", "fin_batch_set_indicator", "fin_batch_set_indicator_every",
-                  "fin_batch_hybrid_stats"):
+                  "fin_batch_hybrid_stats", "fin_batch_set_kernel_timing", "fin_batch_kernel_times"):
             getattr(lib, n).restype = C.c_int
         lib._batch_bound = True
     return lib
@@ -112,6 +114,17 @@ class Batch:
         _check(self.lib, self.lib.fin_batch_hybrid_stats(self.h, *[C.byref(x) for x in v]))
         return {"troubled_faces": v[0].value, "faces": v[1].value, "judges": v[2].value, "reverts": v[3].value}
 
+    def set_kernel_timing(self, on=True):
+        """Launch steps one by one with events between the launch groups
+        (diagnostic: no graph) and accumulate each group's device time."""
+        _check(self.lib, self.lib.fin_batch_set_kernel_timing(self.h, 1 if on else 0))
+
+    def kernel_times(self):
+        ms = np.zeros(5)
+        _check(self.lib, self.lib.fin_batch_kernel_times(self.h, ms))
+        return dict(zip(("control_ms", "indicator_ms", "hybrid_stages_ms", "plain_stages_ms", "judge_diff_ms"),
+                        map(float, ms)))
+
     def stats(self):
         ms, reps, cfg = C.c_double(), C.c_longlong(), C.c_int()
         tune = np.zeros(2)
@@ -166,11 +179,13 @@ def load_indicator(path=None):
     return W["params"], float(W["z_threshold"])
 
 
-def run_sweep(n=1024, tend=0.25, seed=0, precision=FIN_PREC_FP32, separate=False, indicator=None):
+def run_sweep(n=1024, tend=0.25, seed=0, precision=FIN_PREC_FP32, separate=False, indicator=None,
+              kernel_times=False):
     """The sweep batched (one persistent launch per stage over all problems)
     and, optionally, every problem run on its own; device times and
     cell-updates/s of both.  The hybrid form takes indicator = (params,
-    z threshold), by default the trained network."""
+    z threshold), by default the trained network.  kernel_times: the batch
+    runs without its graph, with the device time of each launch group."""
     hyb = precision == FIN_PREC_HYBRID
     if hyb and indicator is None:
         indicator = load_indicator()
@@ -188,14 +203,20 @@ def run_sweep(n=1024, tend=0.25, seed=0, precision=FIN_PREC_FP32, separate=False
             p, q = sweep_problem(seed, k, precision=precision)
             dts[k] = first_dt(p, q)
             b.set_state(k, q)
+        if kernel_times:
+            b.set_kernel_timing(True)
         _, steps = b.solve(tend, dts)
         st = b.stats()
         hst = b.hybrid_stats() if hyb else None
+        kt = b.kernel_times() if kernel_times else None
     cu = float(np.sum(cells * steps))
     out["batched"] = {"cell_updates": cu, "device_s": st["device_ms"] * 1e-3,
                       "cell_updates_per_s": cu / (st["device_ms"] * 1e-3), "steps_max": int(steps.max()),
                       "graph_replays": st["replays"], "tile_shape": st["tile_shape"],
                       "autotune_stage1_ms": st["tune_stage_ms"]}
+    if kt:
+        out["batched"]["graph"] = False
+        out["batched"]["kernel_times_ms"] = kt
     if hyb:
         out["batched"]["hybrid"] = dict(hst, troubled_fraction=hst["troubled_faces"] / max(hst["faces"], 1),
                                         indicator_every=HYB_EVERY, judge_every=HYB_JUDGE_EVERY,
@@ -222,8 +243,11 @@ def main():
     ap.add_argument("--seed", type=int, default=0)
     ap.add_argument("--precision", default="fp32", choices=sorted(PRECISIONS))
     ap.add_argument("--separate", action="store_true", help="also run every problem on its own")
+    ap.add_argument("--kernel-times", action="store_true",
+                    help="run the batch without its graph and report each launch group's device time")
     a = ap.parse_args()
-    print(json.dumps(run_sweep(a.n, a.tend, a.seed, PRECISIONS[a.precision], a.separate)))
+    print(json.dumps(run_sweep(a.n, a.tend, a.seed, PRECISIONS[a.precision], a.separate,
+                               kernel_times=a.kernel_times)))
 
 
 if __name__ == "__main__":

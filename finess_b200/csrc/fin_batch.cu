@@ -40,6 +40,7 @@
 #include "fin_stage_hyb.cuh"
 #include "fin_hybrid.cuh"
 #include "fin_mlp.cuh"
+#include "fin_tmap.h"
 
 using namespace fin;
 
@@ -88,6 +89,8 @@ struct BProb {
     double smax_full[2];    // the judge stages' face-speed maxima
     double aj[3][2];        // the judge stages' global alphas
     double diff[2];         // max |q_hybrid - q_full|, max |q_full|
+    int tslot[5];           // tensor maps of q[k]: entries 2 tslot[k] (tile + halo box), +1 (interior box)
+    int tmok;               // the maps exist (even my): the hybrid stages stage tiles by TMA
 };
 
 // Hybrid-form schedule shared by the problems of a batch (on = 0: no
@@ -107,7 +110,7 @@ struct BHyb {
 // the plain form, or the judge's stages from q^n through the same two stage
 // registers into q[4], with their own maxima, alphas and status).
 __global__ void k_batch_prep(BProb* pr, int n, StageArgs* args, StageArgs* args_p, const StageArgs tmpl,
-                             int global_alpha, const BHyb h, unsigned long long* cnt)
+                             int global_alpha, const BHyb h, unsigned long long* cnt, const CUtensorMap* tm)
 {
     const int p = blockIdx.x * blockDim.x + threadIdx.x;
     if (p >= n) return;
@@ -183,6 +186,12 @@ __global__ void k_batch_prep(BProb* pr, int n, StageArgs* args, StageArgs* args_
         }
         StageArgs ah = a;
         ah.flags = b.flags;
+        if (b.tmok) {   // q_in's tile + halo and the other operand (always q^n) by TMA
+            const CUtensorMap* tp = tm + size_t(p) * 10;
+            ah.tma = 1;
+            ah.gtm_in = tp + 2 * b.tslot[in];
+            ah.gtm_A = tp + 2 * b.tslot[b.cur] + 1;
+        }
         args[size_t(s) * n + p] = ah;
         if (b.use_hyb && b.judge) {
             a.status = &b.status_full;
@@ -227,6 +236,9 @@ __global__ void k_batch_ctl(BProb* pr, int n, int* nactive, const BHyb h)
             double* t = b.q[4];
             b.q[4] = b.q[b.nxt];
             b.q[b.nxt] = t;
+            const int ts = b.tslot[4];
+            b.tslot[4] = b.tslot[b.nxt];
+            b.tslot[b.nxt] = ts;
             b.alpha[b.nxt][0] = b.aj[2][0];
             b.alpha[b.nxt][1] = b.aj[2][1];
             sx = b.smax_full[0];
@@ -346,7 +358,9 @@ __global__ void __launch_bounds__(1024) k_batch_queue(const BProb* pr, int n, in
 // The walk of a work queue shared by the batch kernels: persistent CTAs take
 // tiles from an atomic counter, find the tile's problem by binary search in
 // the prefix sums and run body(p, i0, j0) on it, until the queue is empty or
-// body returns false (uniformly across the CTA).
+// body returns false (uniformly across the CTA).  The counter is bumped for
+// the next tile when a tile starts, so the atomic's round trip overlaps the
+// tile's work (the result is first needed after body).
 template <int TI, int TJ, class F>
 __device__ __forceinline__ void walk_queue(const BProb* pr, const int* act, const long long* tile0, const int* nact,
                                            unsigned long long* queue, F&& body)
@@ -354,12 +368,12 @@ __device__ __forceinline__ void walk_queue(const BProb* pr, const int* act, cons
     __shared__ long long s_tile;
     const int na = *nact;
     const long long total = tile0[na];
-    for (;;) {
-        __syncthreads();   // the previous tile's shared memory is free
-        if (threadIdx.x == 0) s_tile = (long long)atomicAdd(queue, 1ull);
-        __syncthreads();
-        const long long t = s_tile;
-        if (t >= total) return;
+    if (threadIdx.x == 0) s_tile = (long long)atomicAdd(queue, 1ull);
+    __syncthreads();
+    long long t = s_tile;
+    while (t < total) {
+        unsigned long long nx = 0;
+        if (threadIdx.x == 0) nx = atomicAdd(queue, 1ull);
         int lo = 0, hi = na - 1;   // the entry whose tiles contain t
         while (lo < hi) {
             const int mid = (lo + hi + 1) >> 1;
@@ -369,6 +383,10 @@ __device__ __forceinline__ void walk_queue(const BProb* pr, const int* act, cons
         const int p = act[lo];
         const int lt = int(t - tile0[lo]), tj = (pr[p].my + TJ - 1) / TJ;
         if (!body(p, (lt / tj) * TI, (lt % tj) * TJ)) return;
+        __syncthreads();   // the tile's shared memory and s_tile are free
+        if (threadIdx.x == 0) s_tile = (long long)nx;
+        __syncthreads();
+        t = s_tile;
     }
 }
 
@@ -397,17 +415,46 @@ k_stage_hyb_batch(const BProb* pr, const int* act, const long long* tile0, const
     });
 }
 
+// stage_remap with asynchronous copies (cp.async, 8 bytes each): the loads
+// land in stg while the CTA works on the previous tile; cp.async.wait_all and
+// a barrier before stg is read.
+template <class Cfg>
+__device__ __forceinline__ void stage_remap_async(double* stg, const double* q, size_t plane, int i0, int j0, int mx,
+                                                  int my, const int* bc, int tid)
+{
+    constexpr int H = Cfg::H, TI = Cfg::TI, TJ = Cfg::TJ, RI = Cfg::RI, RJ = Cfg::RJ;
+    for (int e = tid; e < RI * RJ; e += Cfg::NT) {
+        const int ii = e / RJ, jj = e - ii * RJ;
+        const bool xin = ii >= H && ii < H + TI, yin = jj >= H && jj < H + TJ;
+        if (!xin && !yin) continue;
+        const int gi = bc_remap(i0 + ii - H, mx, bc[0], bc[1]);
+        const int gj = bc_remap(j0 + jj - H, my, bc[2], bc[3]);
+        const size_t g = size_t(gi) * my + gj;
+#pragma unroll
+        for (int m = 0; m < MEQN; m++) {
+            const uint32_t dst = tc::smem_addr(stg + (m * RI + ii) * Cfg::SJ + jj + 1);
+            asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(dst), "l"(q + m * plane + g) : "memory");
+        }
+    }
+    asm volatile("cp.async.commit_group;" ::: "memory");
+}
+
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;" ::: "memory"); }
+
 // The indicator over the problems of a queue: per tile q[cur]'s tile + halo
-// by remap loads, then indicator_tile (the body of k_indicator) into the
-// problem's flags; troubled faces counted into *count.
+// (asynchronous copies issued while the previous tile's network runs),
+// then indicator_tile (the body of k_indicator) into the problem's flags;
+// troubled faces counted into *count.
 template <class Cfg>
 __global__ void __launch_bounds__(Cfg::NT, 3)
 k_indicator_batch(BProb* pr, const int* act, const long long* tile0, const int* nact, const float* P, float gamma,
                   float zthr, unsigned long long* count, unsigned long long* queue)
 {
-    const long long total = tile0[*nact];
+    const int na = *nact;
+    const long long total = tile0[na];
     if ((long long)blockIdx.x >= total) return;   // no tile for this CTA: skip the set-up
     extern __shared__ __align__(128) unsigned char smem_raw[];
+    __shared__ long long s_next;
     IndTile<Cfg>& S = *reinterpret_cast<IndTile<Cfg>*>(smem_raw);
     const int tid = threadIdx.x, warp = tid >> 5;
     ind::load_ind_weights(S.w, P, tid, Cfg::NT);
@@ -417,25 +464,60 @@ k_indicator_batch(BProb* pr, const int* act, const long long* tile0, const int* 
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
         S.abort = 0;
         S.cnt = 0;
+        s_next = (long long)atomicAdd(queue, 1ull);
     }
     tc::fence_before_sync();
     __syncthreads();
     tc::fence_after_sync();
     const uint32_t tmem = S.tmem;
     uint32_t mma_phase = 0;
-    walk_queue<Cfg::TI, Cfg::TJ>(pr, act, tile0, nact, queue, [&](int p, int i0, int j0) {
-        BProb& b = pr[p];
-        stage_remap<Cfg>(S.stg, b.q[b.cur], b.plane, i0, j0, b.mx, b.my, b.bc, tid);
+    // tile t -> problem and tile origin (binary search in the prefix sums)
+    auto locate = [&](long long t, int& p, int& i0, int& j0) {
+        int lo = 0, hi = na - 1;
+        while (lo < hi) {
+            const int mid = (lo + hi + 1) >> 1;
+            if (tile0[mid] <= t) lo = mid;
+            else hi = mid - 1;
+        }
+        p = act[lo];
+        const int lt = int(t - tile0[lo]), tj = (pr[p].my + Cfg::TJ - 1) / Cfg::TJ;
+        i0 = (lt / tj) * Cfg::TI;
+        j0 = (lt % tj) * Cfg::TJ;
+    };
+    auto prefetch = [&](int p, int i0, int j0) {
+        const BProb& b = pr[p];
+        stage_remap_async<Cfg>(S.stg, b.q[b.cur], b.plane, i0, j0, b.mx, b.my, b.bc, tid);
+    };
+    long long t = s_next;
+    int p = 0, i0 = 0, j0 = 0;
+    if (t < total) {
+        locate(t, p, i0, j0);
+        prefetch(p, i0, j0);
+    }
+    while (t < total) {
+        cp_async_wait_all();
         __syncthreads();
         stage_convert<Cfg, float>(S.stg, S.qs, tid);
-        __syncthreads();
+        if (tid == 0) s_next = (long long)atomicAdd(queue, 1ull);
+        __syncthreads();   // qs complete, stg free, the next tile published
+        const long long tn = s_next;
+        int pn = 0, in0 = 0, jn0 = 0;
+        if (tn < total) {
+            locate(tn, pn, in0, jn0);
+            prefetch(pn, in0, jn0);
+        }
+        BProb& b = pr[p];
         indicator_tile<Cfg>(S, b.mx, b.my, gamma, zthr, b.flags, i0, j0, tmem, mma_phase);
         if (S.abort) {
             if (tid == 0) atomicOr(&b.status, 4u);
-            return false;
+            break;
         }
-        return true;
-    });
+        t = tn;
+        p = pn;
+        i0 = in0;
+        j0 = jn0;
+    }
+    cp_async_wait_all();   // no copy stays in flight into released shared memory
     __syncthreads();
     if (tid == 0 && S.cnt) atomicAdd(count, (unsigned long long)S.cnt);
     tc::fence_after_sync();
@@ -524,6 +606,12 @@ struct fin_batch {
     BHyb hs;
     unsigned* dflags;           // every problem's flag masks
     unsigned long long* dcount; // troubled faces and faces the indicator ran on
+    CUtensorMap* dtm;           // per problem and buffer slot: tile + halo box, interior box
+    // kernel timing (steps launched one by one with events between the
+    // launch groups instead of graph replays)
+    bool timing;
+    std::vector<cudaEvent_t> tev;
+    double tms[5];              // control, indicator, hybrid stages, plain stages, judge difference
 };
 
 namespace {
@@ -531,6 +619,9 @@ namespace {
 // Work-queue counters of a step: the stages of the plain forms use 0-2; the
 // hybrid form the indicator 0, hybrid stages 1-3, plain stages 4-6, judge 7.
 constexpr int NCOUNTER = 8;
+// Steps between the host's looks at the active count, and the events a
+// timed step records.
+constexpr int CHUNK = 8, NSTEPEV = 7;
 
 bool hybrid_on(const fin_batch* b) { return b->hyb && b->mlpP != nullptr; }
 
@@ -646,13 +737,17 @@ int launch_indicator(fin_batch* b, QueueRef q, unsigned long long* counter)
     auto kern = k_indicator_batch<HybCfg>;
     const size_t smem = sizeof(IndTile<HybCfg>);
     static int grid = 0;
-    const int rg = resident_grid(kern, HybCfg::NT, smem, &grid);
-    if (rg) return rg;
-    // each CTA holds 128 TMEM columns: at most 4 of them fit an SM's 512
-    int nsm = 0, dev = 0;
-    BCK(cudaGetDevice(&dev));
-    BCK(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
-    grid = std::min(grid, 3 * nsm);
+    if (!grid) {
+        // three CTAs per SM, as the kernel is laid out for (registers and
+        // shared memory; 3 x 128 of the SM's 512 TMEM columns).  The
+        // occupancy calculator reported one CTA per SM for this kernel, so
+        // the grid is set from the layout.
+        BCK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
+        int nsm = 0, dev = 0;
+        BCK(cudaGetDevice(&dev));
+        BCK(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
+        grid = 3 * nsm;
+    }
     kern<<<grid, HybCfg::NT, smem, b->stream>>>(b->db, q.act, q.tile0, q.nact, b->mlpP, float(b->tmpl_p.gamma),
                                                 b->zthr, b->dcount, counter);
     BCK(cudaGetLastError());
@@ -689,44 +784,57 @@ int launch_prep(fin_batch* b, const BHyb& h)
 {
     const int nb = (b->n + 127) / 128;
     k_batch_prep<<<nb, 128, 0, b->stream>>>(b->db, b->n, b->dargs, b->dargs_p, template_args(b->tmpl_p),
-                                            b->tmpl_p.global_alpha, h, b->dcount);
+                                            b->tmpl_p.global_alpha, h, b->dcount, b->dtm);
     BCK(cudaGetLastError());
     return FIN_OK;
 }
 
 // One step of every active problem: prep, three stages, control; in the
 // hybrid form prep, the indicator, three hybrid and three plain stages, the
-// judge's difference, control.
-int enqueue_step(fin_batch* b)
+// judge's difference, control.  ev (kernel timing, else null): NSTEPEV
+// events recorded between the launch groups (see fin_batch_kernel_times).
+int enqueue_step(fin_batch* b, cudaEvent_t* ev = nullptr)
 {
     const int nb = (b->n + 127) / 128;
     const BHyb h = schedule(b);
+    auto mark = [&](int k) -> cudaError_t { return ev ? cudaEventRecord(ev[k], b->stream) : cudaSuccess; };
     int rc;
+    BCK(mark(0));
     if ((rc = launch_prep(b, h))) return rc;
     if (!h.on) {
         if ((rc = launch_queue_cfg(b, b->cfg))) return rc;
         BCK(cudaMemsetAsync(b->dqueue, 0, 3 * sizeof(unsigned long long), b->stream));
+        BCK(mark(1));
+        BCK(mark(2));
+        BCK(mark(3));
         for (int s = 0; s < 3; s++)
             if ((rc = launch_stage_cfg(b, b->cfg, queue_ref(b, QSEL_ALL), b->dargs + size_t(s) * b->n, b->dqueue + s)))
                 return rc;
+        BCK(mark(4));
     } else {
         static_assert(HybCfg::TI == BatchCfgA::TI && HybCfg::TJ == BatchCfgA::TJ, "one tile shape for all queues");
         if ((rc = launch_queue(b, HybCfg::TI, HybCfg::TJ, (1u << QSEL_IND) | (1u << QSEL_HYB) | (1u << QSEL_PLAIN))))
             return rc;
         BCK(cudaMemsetAsync(b->dqueue, 0, NCOUNTER * sizeof(unsigned long long), b->stream));
+        BCK(mark(1));
         if ((rc = launch_indicator(b, queue_ref(b, QSEL_IND), b->dqueue))) return rc;
+        BCK(mark(2));
         for (int s = 0; s < 3; s++)
             if ((rc = launch_hyb_stage(b, queue_ref(b, QSEL_HYB), b->dargs + size_t(s) * b->n, b->dqueue + 1 + s)))
                 return rc;
+        BCK(mark(3));
         for (int s = 0; s < 3; s++)
             if ((rc = launch_batch_stage<BatchCfgA>(b, queue_ref(b, QSEL_PLAIN), b->dargs_p + size_t(s) * b->n,
                                                     b->dqueue + 4 + s)))
                 return rc;
+        BCK(mark(4));
         if ((rc = launch_diff(b, queue_ref(b, QSEL_PLAIN), b->dqueue + 7))) return rc;
     }
+    BCK(mark(5));
     BCK(cudaMemsetAsync(b->dactive, 0, sizeof(int), b->stream));
     k_batch_ctl<<<nb, 128, 0, b->stream>>>(b->db, b->n, b->dactive, h);
     BCK(cudaGetLastError());
+    BCK(mark(6));
     return FIN_OK;
 }
 
@@ -856,6 +964,7 @@ int fin_batch_create(const fin_params* params, int nprob, fin_batch** out)
         for (int q = 0; q < (b->hyb ? 5 : 4); q++)
             if ((e = cudaMalloc(&h.q[q], MEQN * h.plane * sizeof(double))) != cudaSuccess) return fail(e, "cudaMalloc state");
         h.ind_since = -1;
+        for (int q = 0; q < 5; q++) h.tslot[q] = q;
         b->aos_max = std::max(b->aos_max, size_t(p.mx + 2 * p.mbc) * (p.my + 2 * p.mbc) * MEQN);
     }
     if (b->hyb) {
@@ -872,6 +981,23 @@ int fin_batch_create(const fin_params* params, int nprob, fin_batch** out)
         }
         if ((e = cudaMalloc(&b->dargs_p, 3 * size_t(nprob) * sizeof(StageArgs))) != cudaSuccess)
             return fail(e, "cudaMalloc");
+        // tensor maps of every state buffer (grids with even my), written
+        // once: the judge's buffer swaps permute the slots, not the maps
+        std::vector<CUtensorMap> tms(size_t(nprob) * 10);
+        memset(tms.data(), 0, tms.size() * sizeof(CUtensorMap));
+        for (int k = 0; k < nprob; k++) {
+            BProb& h = b->hb[k];
+            bool ok = true;
+            for (int q = 0; q < 5 && ok; q++)
+                ok = make_state_map(&tms[size_t(k) * 10 + 2 * q], h.q[q], h.mx, h.my, h.plane, HybCfg::SJ, HybCfg::RI) &&
+                     make_state_map(&tms[size_t(k) * 10 + 2 * q + 1], h.q[q], h.mx, h.my, h.plane, HybCfg::TJ,
+                                    HybCfg::TI);
+            h.tmok = ok ? 1 : 0;
+        }
+        if ((e = cudaMalloc(&b->dtm, tms.size() * sizeof(CUtensorMap))) != cudaSuccess) return fail(e, "cudaMalloc");
+        if ((e = cudaMemcpy(b->dtm, tms.data(), tms.size() * sizeof(CUtensorMap), cudaMemcpyHostToDevice)) !=
+            cudaSuccess)
+            return fail(e, "cudaMemcpy");
     }
     if ((e = cudaMalloc(&b->dcount, 2 * sizeof(unsigned long long))) != cudaSuccess) return fail(e, "cudaMalloc");
     if ((e = cudaMemset(b->dcount, 0, 2 * sizeof(unsigned long long))) != cudaSuccess) return fail(e, "memset");
@@ -900,6 +1026,7 @@ int fin_batch_destroy(fin_batch* b)
         for (int q = 0; q < 5; q++) cudaFree(h.q[q]);
     cudaFree(b->dflags);
     cudaFree(b->dcount);
+    cudaFree(b->dtm);
     cudaFree(b->mlpP);
     cudaFree(b->dargs_p);
     cudaFree(b->dact);
@@ -912,6 +1039,8 @@ int fin_batch_destroy(fin_batch* b)
     cudaFree(b->d_aos);
     if (b->ev0) cudaEventDestroy(b->ev0);
     if (b->ev1) cudaEventDestroy(b->ev1);
+    for (cudaEvent_t e : b->tev)
+        if (e) cudaEventDestroy(e);
     if (b->stream) cudaStreamDestroy(b->stream);
     delete b;
     return FIN_OK;
@@ -994,14 +1123,23 @@ int fin_batch_solve(fin_batch* b, double tend, double* dtv1, int* steps)
         // the hybrid form's kernels are built for one tile shape (15 x 16)
         if (b->cfg < 0 && hybrid_on(b)) b->cfg = 0;
         if (b->cfg < 0 && (rc = autotune(b))) return rc;
-        if ((rc = build_graph(b))) return rc;
+        if (!b->timing && (rc = build_graph(b))) return rc;
         BCK(cudaEventRecord(b->ev0, b->stream));
-        const int chunk = 8;   // replays between the host's looks at the active count
         while (nact > 0) {
-            for (int r = 0; r < chunk; r++) BCK(cudaGraphLaunch(b->graph, b->stream));
-            reps += chunk;
+            for (int r = 0; r < CHUNK; r++) {
+                if (!b->timing) BCK(cudaGraphLaunch(b->graph, b->stream));
+                else if ((rc = enqueue_step(b, b->tev.data() + r * NSTEPEV))) return rc;
+            }
+            reps += CHUNK;
             BCK(cudaMemcpyAsync(&nact, b->dactive, sizeof(int), cudaMemcpyDeviceToHost, b->stream));
             BCK(cudaStreamSynchronize(b->stream));
+            for (int r = 0; b->timing && r < CHUNK; r++) {
+                const cudaEvent_t* e = b->tev.data() + r * NSTEPEV;
+                float m[6];
+                for (int k = 0; k < 6; k++) BCK(cudaEventElapsedTime(&m[k], e[k], e[k + 1]));
+                b->tms[0] += m[0] + m[5];
+                for (int k = 1; k < 5; k++) b->tms[k] += m[k];
+            }
         }
     }
     BCK(cudaEventRecord(b->ev1, b->stream));
@@ -1074,6 +1212,25 @@ int fin_batch_set_indicator_every(fin_batch* b, int every)
         cudaGraphExecDestroy(b->graph);
         b->graph = nullptr;
     }
+    return FIN_OK;
+}
+
+int fin_batch_set_kernel_timing(fin_batch* b, int on)
+{
+    if (!b) return berr(FIN_ERR_ARG, "null batch");
+    if (on && b->tev.empty()) {
+        b->tev.assign(CHUNK * NSTEPEV, nullptr);
+        for (cudaEvent_t& e : b->tev) BCK(cudaEventCreate(&e));
+    }
+    b->timing = on != 0;
+    for (double& t : b->tms) t = 0.0;
+    return FIN_OK;
+}
+
+int fin_batch_kernel_times(fin_batch* b, double* ms)
+{
+    if (!b || !ms) return berr(FIN_ERR_ARG, "null argument");
+    for (int k = 0; k < 5; k++) ms[k] = b->tms[k];
     return FIN_OK;
 }
 

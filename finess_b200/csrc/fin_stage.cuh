@@ -72,6 +72,11 @@ struct StageArgs {
     CUtensorMap tm_in;
     CUtensorMap tm_A;
     CUtensorMap tm_qi;   // q_in with the interior-tile box (TJ x TI x 5)
+    // The same two maps held in global memory (batches, whose stage
+    // arguments live in global memory): used instead of tm_in / tm_A when
+    // set, after a tensormap-proxy acquire fence.
+    const CUtensorMap* gtm_in;
+    const CUtensorMap* gtm_A;
 };
 
 // Troubled-face flags, one bit per face: x faces (rows 0 .. mx) take

@@ -159,12 +159,16 @@ __device__ __forceinline__ void stage_hyb_tile(const StageArgs& a, const int i0,
     // ---- phase 0: q_in's tile + halo and the other operand's interior by
     // TMA (or q_in through the boundary remap); the flag masks ----
     if (tt && tid == 0) {
+        const CUtensorMap* tmi = a.gtm_in ? a.gtm_in : &a.tm_in;
+        const CUtensorMap* tme = a.gtm_A ? a.gtm_A : &a.tm_A;
+        if (a.gtm_in) tc::tensormap_acquire(a.gtm_in);
+        if (ext && a.gtm_A) tc::tensormap_acquire(a.gtm_A);
         tc::mbar_init(mbq, 1);
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
         tc::mbar_expect_tx(mbq, uint32_t(Cfg::STG_BYTES + (ext && !L::SHARE ? Cfg::ABUF_BYTES : 0)));
-        tc::tma_load_3d(stg, &a.tm_in, j0 - 4, i0 - H, 0, mbq);
-        if (ext && !L::SHARE) tc::tma_load_3d(ebuf, &a.tm_A, j0, i0, 0, mbq);
-        if (ext && L::SHARE) tc::tma_prefetch_3d(&a.tm_A, j0, i0, 0);
+        tc::tma_load_3d(stg, tmi, j0 - 4, i0 - H, 0, mbq);
+        if (ext && !L::SHARE) tc::tma_load_3d(ebuf, tme, j0, i0, 0, mbq);
+        if (ext && L::SHARE) tc::tma_prefetch_3d(tme, j0, i0, 0);
     }
     {
         const int wx = flag_wx(my), wy = flag_wy(my);

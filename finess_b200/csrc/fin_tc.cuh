@@ -117,6 +117,15 @@ __device__ __forceinline__ void tma_load_3d(void* dst, const CUtensorMap* map, i
         : "memory");
 }
 
+// Before a tensor map that lives in global memory (written there by a host
+// copy) is used by TMA: order the tensormap proxy's view of its 128 bytes
+// after the generic-proxy writes that stored it.
+__device__ __forceinline__ void tensormap_acquire(const CUtensorMap* map)
+{
+    asm volatile("fence.proxy.tensormap::generic.acquire.gpu [%0], 128;" ::"l"(reinterpret_cast<uint64_t>(map))
+                 : "memory");
+}
+
 // The same box of a 3D tensor prefetched into L2 only (no shared memory, no
 // completion to wait for).
 __device__ __forceinline__ void tma_prefetch_3d(const CUtensorMap* map, int x, int y, int z)

@@ -272,6 +272,13 @@ int fin_batch_set_indicator_every(fin_batch* b, int every);
  * its runs), judge steps and reverts, summed over the problems. */
 int fin_batch_hybrid_stats(fin_batch* b, long long* troubled_faces, long long* faces, long long* judges,
                            long long* reverts);
+/* Kernel timing: with on != 0 the solves launch each step on its own with
+ * CUDA events between the launch groups (no graph), and accumulate the
+ * device time of each group since the call: ms[5] = control (prep, work
+ * queues, control), indicator, hybrid stages, plain stages, judge
+ * difference. */
+int fin_batch_set_kernel_timing(fin_batch* b, int on);
+int fin_batch_kernel_times(fin_batch* b, double* ms);
 const char* fin_batch_last_error(void);
 
 /* ---- for callers that cannot allocate device memory ------------------- */
