@@ -415,6 +415,35 @@ k_stage_hyb_batch(const BProb* pr, const int* act, const long long* tile0, const
     });
 }
 
+// Clears, per tile of the indicator's queue, the flag words that hold the
+// tile's faces: the x faces of rows i0 .. i0+TI-1 (and row mx for the last
+// tile row), the y faces of rows i0 .. i0+TI-1 at columns j0 .. j0+TJ.  A
+// word shared with a neighbouring tile is cleared by both, all before the
+// indicator sets any bit (a launch of its own); bits that no face owns are
+// zero from the allocation.
+template <class Cfg>
+__global__ void __launch_bounds__(Cfg::NT) k_batch_clear_flags(BProb* pr, const int* act, const long long* tile0,
+                                                               const int* nact, unsigned long long* queue)
+{
+    static_assert(Cfg::TJ == 16 && Cfg::TI < 32, "one word per x-face row, two per y-face row");
+    walk_queue<Cfg::TI, Cfg::TJ>(pr, act, tile0, nact, queue, [&](int p, int i0, int j0) {
+        const BProb& b = pr[p];
+        const int mx = b.mx, my = b.my, wx = flag_wx(my), wy = flag_wy(my), t = threadIdx.x, k = j0 >> 5;
+        if (t <= Cfg::TI) {
+            const int gi = i0 + t;
+            if (t < Cfg::TI ? gi <= mx : gi == mx) b.flags[size_t(gi) * wx + k] = 0u;
+        } else if (t >= 32 && t < 32 + Cfg::TI) {
+            const int gi = i0 + t - 32;
+            if (gi < mx) {
+                unsigned* row = b.flags + size_t(mx + 1) * wx + size_t(gi) * wy;
+                row[k] = 0u;
+                if (((j0 + Cfg::TJ) >> 5) != k && ((j0 + Cfg::TJ) >> 5) < wy) row[(j0 + Cfg::TJ) >> 5] = 0u;
+            }
+        }
+        return true;
+    });
+}
+
 // stage_remap with asynchronous copies (cp.async, 8 bytes each): the loads
 // land in stg while the CTA works on the previous tile; cp.async.wait_all and
 // a barrier before stg is read.
@@ -617,8 +646,9 @@ struct fin_batch {
 namespace {
 
 // Work-queue counters of a step: the stages of the plain forms use 0-2; the
-// hybrid form the indicator 0, hybrid stages 1-3, plain stages 4-6, judge 7.
-constexpr int NCOUNTER = 8;
+// hybrid form the indicator 0, hybrid stages 1-3, plain stages 4-6, judge 7,
+// the flag clearing 8.
+constexpr int NCOUNTER = 9;
 // Steps between the host's looks at the active count, and the events a
 // timed step records.
 constexpr int CHUNK = 8, NSTEPEV = 7;
@@ -754,6 +784,13 @@ int launch_indicator(fin_batch* b, QueueRef q, unsigned long long* counter)
     return FIN_OK;
 }
 
+int launch_clear_flags(fin_batch* b, QueueRef q, unsigned long long* counter)
+{
+    k_batch_clear_flags<HybCfg><<<148 * 4, HybCfg::NT, 0, b->stream>>>(b->db, q.act, q.tile0, q.nact, counter);
+    BCK(cudaGetLastError());
+    return FIN_OK;
+}
+
 int launch_diff(fin_batch* b, QueueRef q, unsigned long long* counter)
 {
     k_batch_diff<HybCfg><<<148 * 4, HybCfg::NT, 0, b->stream>>>(b->db, q.act, q.tile0, q.nact, counter);
@@ -817,6 +854,7 @@ int enqueue_step(fin_batch* b, cudaEvent_t* ev = nullptr)
             return rc;
         BCK(cudaMemsetAsync(b->dqueue, 0, NCOUNTER * sizeof(unsigned long long), b->stream));
         BCK(mark(1));
+        if ((rc = launch_clear_flags(b, queue_ref(b, QSEL_IND), b->dqueue + 8))) return rc;
         if ((rc = launch_indicator(b, queue_ref(b, QSEL_IND), b->dqueue))) return rc;
         BCK(mark(2));
         for (int s = 0; s < 3; s++)
@@ -968,8 +1006,8 @@ int fin_batch_create(const fin_params* params, int nprob, fin_batch** out)
         b->aos_max = std::max(b->aos_max, size_t(p.mx + 2 * p.mbc) * (p.my + 2 * p.mbc) * MEQN);
     }
     if (b->hyb) {
-        // one allocation for every problem's flag masks, zeroed once: bits
-        // that no face owns stay zero, the indicator rewrites the others
+        // one allocation for every problem's flag masks (cleared per run by
+        // k_batch_clear_flags; bits that no face owns stay zero from here)
         size_t words = 0;
         for (const fin_params& p : b->p) words += flag_words(p.mx, p.my);
         if ((e = cudaMalloc(&b->dflags, words * sizeof(unsigned))) != cudaSuccess) return fail(e, "cudaMalloc flags");

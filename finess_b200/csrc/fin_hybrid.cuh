@@ -16,8 +16,7 @@ struct IndicatorArgs {
     float gamma;
     const float* P;            // network parameters (FP32, mlp::NPARAM)
     float zthr;                // a face is troubled when its logit exceeds zthr
-    unsigned* flags;           // bit masks (flag_wx / flag_wy layout); zeroed once when allocated
-                               // (every owned face's bit is rewritten per run)
+    unsigned* flags;           // bit masks (flag_wx / flag_wy layout), zeroed before the launch
     unsigned int* status;
     unsigned long long* count; // troubled faces (accumulated)
     int tma;                   // tm maps q (box (TJ+8) x (TI+6) x 5, as the stage kernel's)
@@ -105,11 +104,9 @@ struct IndTile {
 //   4. 2 gelu, BF16, back into the X matrices; layer 2 into the same columns;
 //   5. 2 gelu + b2 -> output layer in FP32 -> flag.
 // TMEM lane quarter q = warp % 4 holds rows 32q .. 32q+31 of every matrix;
-// warps 0-3 take matrices 0 and 1, warps 4-7 matrices 2 and 3.  Every owned
-// face's bit is written (set or cleared, one AND and one OR per flag word
-// and warp), so the flags need no clearing between runs; bits that no face
-// owns are never touched.  Sets S.abort when a tensor-core wait ran out
-// (uniform across the CTA on return).
+// warps 0-3 take matrices 0 and 1, warps 4-7 matrices 2 and 3.  Flagged
+// faces set their bits (the words are cleared before the run).  Sets S.abort
+// when a tensor-core wait ran out (uniform across the CTA on return).
 template <class Cfg>
 __device__ __forceinline__ void indicator_tile(IndTile<Cfg>& S, const int mx, const int my, const float gamma,
                                                const float zthr, unsigned* flags, const int i0, const int j0,
@@ -206,15 +203,7 @@ __device__ __forceinline__ void indicator_tile(IndTile<Cfg>& S, const int mx, co
 #pragma unroll
         for (int o = 0; o < NH; o++) zz = fmaf(S.w.w3h[o], ind::gelu2(v[o] + S.w.b2[o]), zz);
         const bool fl = fword[h] >= 0 && zz > zthr;
-        // lanes on one flag word combine their bits; the group's first lane
-        // clears the owned bits that are not flagged and sets the others
-        const unsigned grp = __match_any_sync(0xffffffffu, (unsigned long long)fword[h]);
-        const unsigned setb = __reduce_or_sync(grp, fl ? fbit[h] : 0u);
-        const unsigned ownb = __reduce_or_sync(grp, fbit[h]);
-        if (fword[h] >= 0 && lane == __ffs(grp) - 1) {
-            if (ownb & ~setb) atomicAnd(flags + fword[h], ~(ownb & ~setb));
-            if (setb) atomicOr(flags + fword[h], setb);
-        }
+        if (fl) atomicOr(flags + fword[h], fbit[h]);
         const unsigned bal = __ballot_sync(0xffffffffu, fl);
         if (lane == 0 && bal) atomicAdd(&S.cnt, unsigned(__popc(bal)));
     }

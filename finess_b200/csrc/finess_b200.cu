@@ -517,6 +517,7 @@ int launch_indicator(fin_solver* s, int buf)
         configured = true;
     }
     CK(cudaMemsetAsync(s->ind_count, 0, sizeof(unsigned long long), s->stream));
+    CK(cudaMemsetAsync(s->flags, 0, flag_words(s->p.mx, s->p.my) * sizeof(unsigned), s->stream));
     const long long nf = (long long)(s->p.mx + 1) * s->p.my + (long long)s->p.mx * (s->p.my + 1);
     const long long tiles = (long long)((s->p.mx + Cfg::TI - 1) / Cfg::TI) * ((s->p.my + Cfg::TJ - 1) / Cfg::TJ);
     const int grid = int(std::min<long long>(tiles, 148 * 3));
@@ -837,9 +838,6 @@ int fin_create(const fin_params* p, fin_solver** out)
     if (p->precision == FIN_PREC_HYBRID) {
         if ((e = cudaMalloc(&s->flags, flag_words(p->mx, p->my) * sizeof(unsigned))) != cudaSuccess)
             return fail(e, "cudaMalloc flags");
-        // bits no face owns stay zero; the indicator rewrites every owned bit
-        if ((e = cudaMemset(s->flags, 0, flag_words(p->mx, p->my) * sizeof(unsigned))) != cudaSuccess)
-            return fail(e, "memset flags");
         if ((e = cudaMalloc(&s->ind_count, 16)) != cudaSuccess) return fail(e, "cudaMalloc counter");
         if ((e = cudaMemset(s->ind_count, 0, 16)) != cudaSuccess) return fail(e, "memset");
         s->zthr = 0.0f;

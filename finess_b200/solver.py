@@ -141,8 +141,15 @@ class Solver:
         assert q.shape == ghosted_shape(self.p), (q.shape, ghosted_shape(self.p))
         _check(self.lib.fin_set_state(self.h, q, t))
 
-    def get_state(self):
-        q = np.zeros(ghosted_shape(self.p))
+    def get_state(self, out=None):
+        """(q, t): the state in the reference's ghosted layout, into `out`
+        (a C-contiguous float64 array of that shape, e.g. in pinned host
+        memory) when given."""
+        if out is not None:
+            assert out.shape == ghosted_shape(self.p) and out.dtype == np.float64 and out.flags["C_CONTIGUOUS"]
+            q = out
+        else:
+            q = np.zeros(ghosted_shape(self.p))
         t = C.c_double()
         _check(self.lib.fin_get_state(self.h, q, C.byref(t)))
         return q, t.value
