@@ -14,7 +14,7 @@ NVCC_FLAGS = [
     "-Xcompiler", "-fPIC", "-shared",
     "-Xptxas", "-v",
 ]
-SOURCES = ["finess_b200.cu", "fin_ini.cpp", "fin_noalloc.cu", "fin_mlp.cu", "fin_batch.cu", "fin_mhd.cu"]
+SOURCES = ["finess_b200.cu", "fin_ini.cpp", "fin_noalloc.cu", "fin_mlp.cu", "fin_batch.cu", "fin_mhd.cu", "fin_output.cu"]
 
 
 def _newest_source():

@@ -7,6 +7,7 @@
 // on the host and copies the reference exactly; per step the host reads back
 // 16 bytes (the face-speed maxima) to evaluate GetCFL.
 #include <cuda_runtime.h>
+#include <sys/stat.h>
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
@@ -20,6 +21,7 @@
 #include "fin_intflux.cuh"
 #include "fin_hybrid.cuh"
 #include "fin_tmap.h"
+#include "fin_output.h"
 
 using namespace fin;
 
@@ -110,6 +112,13 @@ struct fin_solver {
     CUtensorMap tm_q[NBUF];
     CUtensorMap tm_a[NBUF];
     bool tma_ok;
+    // output files (fin_output.cu); pointers, since the struct is memset
+    fin::io::FrameWriter* writer;   // asynchronous q%04d.dat / a%04d.dat writer (made on first use)
+    std::string* cons_path;         // conservation.dat appended after every accepted step (null: off)
+    double* d_cons;                 // device totals (MEQN doubles) then the partial sums
+    double* h_cons;                 // pinned copy of the totals
+    bool cons_pending;              // h_cons holds the totals at cons_t, not yet written
+    double cons_t;
 };
 
 // ---------------------------------------------------------------------------
@@ -879,6 +888,10 @@ int fin_destroy(fin_solver* s)
 {
     if (!s) return FIN_OK;
     if (s->stream) cudaStreamSynchronize(s->stream);
+    delete s->writer;   // waits for a frame still being written
+    delete s->cons_path;
+    cudaFree(s->d_cons);
+    if (s->h_cons) cudaFreeHost(s->h_cons);
     for (int b = 0; b < NBUF; b++) cudaFree(s->q[b]);
     cudaFree(s->mlpP);
     cudaFree(s->flags);
@@ -1155,6 +1168,33 @@ int fin_solve(fin_solver* s, double tend, double* dtv, int* nsteps_out)
 }
 
 // lib/2d/FinSolveRK.cpp:13-371, stopping early after max_steps accepted steps.
+// Conservation totals of q[cur] (lib/2d/ConSoln.cpp:34-93, written by
+// FinSolveRK.cpp:362 after every accepted step): computed and copied to
+// pinned memory on the stream; the line goes to the file at the next
+// synchronisation (flush_conservation), so no step waits for it.
+static int queue_conservation(fin_solver* s)
+{
+    if (!s->cons_path) return FIN_OK;
+    fin::io::launch_totals(s->stream, s->q[s->cur], MEQN, s->plane, size_t(s->p.mx) * s->p.my, s->dx * s->dy,
+                           s->d_cons + MEQN, s->d_cons);
+    s->launches += 2;
+    CK(cudaGetLastError());
+    CK(cudaMemcpyAsync(s->h_cons, s->d_cons, MEQN * sizeof(double), cudaMemcpyDeviceToHost, s->stream));
+    s->cons_pending = true;
+    s->cons_t = s->t;
+    return FIN_OK;
+}
+
+// After a synchronisation of the stream: the pending line, if any.
+static int flush_conservation(fin_solver* s)
+{
+    if (!s->cons_pending) return FIN_OK;
+    s->cons_pending = false;
+    if (fin::io::append_conservation(*s->cons_path, s->cons_t, s->h_cons, MEQN))
+        return set_err(FIN_ERR_ARG, "cannot write " + *s->cons_path);
+    return FIN_OK;
+}
+
 int fin_advance(fin_solver* s, double tend, double* dtv, int max_steps, int* nsteps_out)
 {
     if (!s || !dtv) return set_err(FIN_ERR_ARG, "null argument");
@@ -1182,6 +1222,7 @@ int fin_advance(fin_solver* s, double tend, double* dtv, int max_steps, int* nst
             if ((rc = take_stages(s, dt, nxt))) goto done;
             bool nonfinite = false;
             if ((rc = get_cfl(s, dt, dtv[2], &cfl, &nonfinite))) goto done;
+            if ((rc = flush_conservation(s))) goto done;
             if ((rc = collect_kernel_times(s))) goto done;
             settle_judge(s, nxt, dt, &cfl);
             // Qnew's time after the step: RK3 keeps UpdateSoln.cpp:27's
@@ -1218,6 +1259,7 @@ int fin_advance(fin_solver* s, double tend, double* dtv, int max_steps, int* nst
             }
         }
         accepted++;
+        if ((rc = queue_conservation(s))) goto done;   // ConSoln(Qnew), FinSolveRK.cpp:362
     }
     dtv[1] = dt;
 done:
@@ -1227,6 +1269,10 @@ done:
         float ms = 0.f;
         if (e1 == cudaSuccess) e1 = cudaEventElapsedTime(&ms, s->ev0, s->ev1);
         if (e1 == cudaSuccess) ms_total = ms;
+        if (e1 == cudaSuccess) {
+            const int rf = flush_conservation(s);
+            if (!rc) rc = rf;
+        }
     }
     s->last_ms = ms_total;
     if (nsteps_out) *nsteps_out = accepted;
@@ -1311,6 +1357,107 @@ int fin_conservation_totals(fin_solver* s, double* totals)
         totals[m] = sum;
     }
     return FIN_OK;
+}
+
+int fin_set_conservation_file(fin_solver* s, const char* outdir)
+{
+    if (!s) return set_err(FIN_ERR_ARG, "null solver");
+    if (s->cons_pending) {
+        CK(cudaStreamSynchronize(s->stream));
+        int rc = flush_conservation(s);
+        if (rc) return rc;
+    }
+    delete s->cons_path;
+    s->cons_path = nullptr;
+    if (!outdir) return FIN_OK;
+    struct stat st;
+    if (stat(outdir, &st) != 0 || !S_ISDIR(st.st_mode)) return set_err(FIN_ERR_ARG, std::string("no directory ") + outdir);
+    if (!s->d_cons) CK(cudaMalloc(&s->d_cons, (MEQN + 2 * MEQN * fin::io::NCHUNK) * sizeof(double)));
+    if (!s->h_cons) CK(cudaMallocHost(&s->h_cons, MEQN * sizeof(double)));
+    s->cons_path = new std::string(std::string(outdir) + "/conservation.dat");
+    return FIN_OK;
+}
+
+int fin_write_conservation(fin_solver* s)
+{
+    if (!s) return set_err(FIN_ERR_ARG, "null solver");
+    if (!s->cons_path) return set_err(FIN_ERR_ARG, "no conservation file set (fin_set_conservation_file)");
+    int rc = queue_conservation(s);
+    if (rc) return rc;
+    CK(cudaStreamSynchronize(s->stream));
+    return flush_conservation(s);
+}
+
+int fin_output_frame(fin_solver* s, int nframe, const char* outdir)
+{
+    if (!s || !outdir || nframe < 0) return set_err(FIN_ERR_ARG, "bad argument");
+    if (!s->writer) s->writer = new fin::io::FrameWriter();
+    char name[32];
+    std::snprintf(name, sizeof(name), "/q%04d.dat", nframe);
+    const std::string qpath = std::string(outdir) + name;
+    std::snprintf(name, sizeof(name), "/a%04d.dat", nframe);
+    const std::string apath = std::string(outdir) + name;
+    // the Euler path holds no aux planes (its AuxFunc sets none,
+    // apps/2d/euler/lib/AuxFunc.cpp:10-13): maux planes of zeros
+    const int rc = s->writer->start(s->stream, s->q[s->cur], MEQN, nullptr, s->p.maux, s->plane, s->p.mx, s->p.my,
+                                    s->t, qpath, apath);
+    if (rc) return set_err(rc, s->writer->err());
+    s->launches++;
+    return FIN_OK;
+}
+
+int fin_output_wait(fin_solver* s)
+{
+    if (!s) return set_err(FIN_ERR_ARG, "null solver");
+    if (!s->writer) return FIN_OK;
+    const int rc = s->writer->wait();
+    if (rc) return set_err(rc, s->writer->err());
+    return FIN_OK;
+}
+
+int fin_read_frame(fin_solver* s, const char* path)
+{
+    if (!s || !path) return set_err(FIN_ERR_ARG, "null argument");
+    if (s->writer) {   // a frame still being written may be the one read
+        const int rw = s->writer->wait();
+        if (rw) return set_err(rw, s->writer->err());
+    }
+    const size_t n = size_t(s->p.mx) * s->p.my * MEQN;
+    double* stage = nullptr;
+    CK(cudaMalloc(&stage, n * sizeof(double)));
+    double t = 0.0;
+    std::string msg;
+    const int rc = fin::io::read_frame(path, s->stream, s->q[s->cur], MEQN, s->plane, s->p.mx, s->p.my, stage, &t, &msg);
+    cudaFree(stage);
+    if (rc) return set_err(rc, msg);
+    s->launches++;
+    s->t = t;
+    s->ind_since = -1;
+    CK(cudaMemsetAsync(s->slots + SLOT_STATUS, 0, sizeof(double), s->stream));
+    int r2 = compute_alpha(s, s->cur);
+    if (r2) return r2;
+    s->alpha_valid = true;
+    return check_status(s);
+}
+
+int fin_write_qhelp(const fin_params* p, const char* outdir)
+{
+    if (!p || !outdir) return set_err(FIN_ERR_ARG, "null argument");
+    const std::string path = std::string(outdir) + "/qhelp.dat";
+    FILE* f = std::fopen(path.c_str(), "w");
+    if (!f) return set_err(FIN_ERR_ARG, "cannot open " + path);
+    // lib/2d/WriteQhelp.cpp:33-42, field by field
+    std::fprintf(f, "%16d   : ndims   \n", 2);
+    std::fprintf(f, "%16d   : meqn    \n", p->meqn);
+    std::fprintf(f, "%16d   : maux    \n", p->maux);
+    std::fprintf(f, "%16d   : nout    \n", p->nout);
+    std::fprintf(f, "%16d   : mx      \n", p->mx);
+    std::fprintf(f, "%16d   : my      \n", p->my);
+    std::fprintf(f, "%16.8e : xlow    \n", p->xlow);
+    std::fprintf(f, "%16.8e : xhigh   \n", p->xhigh);
+    std::fprintf(f, "%16.8e : ylow    \n", p->ylow);
+    std::fprintf(f, "%16.8e : yhigh   \n", p->yhigh);
+    return std::fclose(f) == 0 ? FIN_OK : set_err(FIN_ERR_ARG, "write failed: " + path);
 }
 
 int fin_last_kernel_ms(fin_solver* s, double* ms)

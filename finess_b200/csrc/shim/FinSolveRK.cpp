@@ -2,9 +2,12 @@
 // (lib/2d/RunFinpack.h:18, lib/2d/FinSolveRK.cpp:13) over fin_solve: the state
 // goes to the device once per call (one output frame of RunFinpack.cpp:95-130),
 // every step runs there, and the frame's result comes back with its ghost
-// frame filled as SetBndValues would fill it.  The per-stage hooks
-// (BeforeStep/AfterStep, hooks.h) and the per-step ConSoln file are not
-// called on the device path.
+// frame filled as SetBndValues would fill it.  conservation.dat gets its line
+// after every accepted step (FinSolveRK.cpp:362 calls ConSoln there) from
+// totals summed on the device; where the output directory does not exist the
+// lines are dropped, as the reference's ofstream drops them.  The per-stage
+// hooks (BeforeStep/AfterStep, hooks.h) are not called on the device path.
+#include "IniParams.h"
 #include "fin_shim.h"
 
 void FinSolveRK(StateVars& Qnew, double tend, double dtv[])
@@ -13,6 +16,7 @@ void FinSolveRK(StateVars& Qnew, double tend, double dtv[])
     std::vector<double> q;
     fin_shim_pack(Qnew.const_ref_q(), q);
     fin_shim_check(fin_set_state(s, q.data(), Qnew.get_t()), "FinSolveRK");
+    fin_set_conservation_file(s, global_ini_params.get_output_dir().c_str());
     int nsteps = 0;
     fin_shim_check(fin_solve(s, tend, dtv, &nsteps), "FinSolveRK");
     double t = 0.0;

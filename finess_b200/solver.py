@@ -77,6 +77,15 @@ def load_library(path=LIB_PATH):
     lib.fin_params_from_ini.argtypes = [C.c_char_p, P]
     lib.fin_params_from_ini.restype = C.c_int
     lib.fin_ini_last_error.restype = C.c_char_p
+    lib.fin_output_frame.argtypes = [vp, C.c_int, C.c_char_p]
+    lib.fin_output_wait.argtypes = [vp]
+    lib.fin_read_frame.argtypes = [vp, C.c_char_p]
+    lib.fin_set_conservation_file.argtypes = [vp, C.c_char_p]
+    lib.fin_write_conservation.argtypes = [vp]
+    lib.fin_write_qhelp.argtypes = [P, C.c_char_p]
+    for name in ("fin_output_frame", "fin_output_wait", "fin_read_frame", "fin_set_conservation_file",
+                 "fin_write_conservation", "fin_write_qhelp"):
+        getattr(lib, name).restype = C.c_int
     for name in ("fin_create", "fin_destroy", "fin_set_state", "fin_get_state", "fin_construct_l",
                  "fin_global_wave_spd", "fin_solve", "fin_step_fixed", "fin_conservation_totals",
                  "fin_last_kernel_ms", "fin_launch_count", "fin_device_layout", "fin_state_device_ptr",
@@ -84,6 +93,12 @@ def load_library(path=LIB_PATH):
         getattr(lib, name).restype = C.c_int
     _lib = lib
     return lib
+
+
+def write_qhelp(p, outdir):
+    """qhelp.dat of the parameters under outdir."""
+    lib = load_library()
+    _check(lib.fin_write_qhelp(C.byref(p), os.fsencode(outdir)))
 
 
 def params_from_ini(path):
@@ -236,6 +251,26 @@ class Solver:
         cfl = C.c_double()
         _check(self.lib.fin_step_fixed(self.h, dt, C.byref(cfl)))
         return cfl.value
+
+    # -- output files (lib/2d/Output.cpp, ConSoln.cpp, WriteQhelp.cpp) -----
+    def output_frame(self, nframe, outdir):
+        """Starts writing q%04d.dat / a%04d.dat of the current state under
+        outdir (asynchronous; output_wait() returns when they are on disk)."""
+        _check(self.lib.fin_output_frame(self.h, nframe, os.fsencode(outdir)))
+
+    def output_wait(self):
+        _check(self.lib.fin_output_wait(self.h))
+
+    def read_frame(self, path):
+        """Restart from a q%04d.dat file: its values become the state, its header t."""
+        _check(self.lib.fin_read_frame(self.h, os.fsencode(path)))
+
+    def set_conservation_file(self, outdir):
+        """conservation.dat under outdir, a line per accepted step (None: off)."""
+        _check(self.lib.fin_set_conservation_file(self.h, None if outdir is None else os.fsencode(outdir)))
+
+    def write_conservation(self):
+        _check(self.lib.fin_write_conservation(self.h))
 
     def conservation_totals(self):
         out = np.zeros(self.p.meqn)

@@ -160,6 +160,39 @@ int fin_step_fixed(fin_solver* s, double dt, double* cfl_out);
  * with compensated summation (lib/2d/ConSoln.cpp:52-64). totals[meqn]. */
 int fin_conservation_totals(fin_solver* s, double* totals);
 
+/* ---- output files ----------------------------------------------------- */
+/* The reference's frame files from the device state, in its formats:
+ * q%04d.dat and a%04d.dat (void Output(const StateVars&, int nframe),
+ * lib/2d/Output.cpp:12-62: a header line with t, then every value of
+ * component m = 1..meqn (maux for the aux file), j = 1..my, i = 1..mx (i
+ * fastest) as "%24.16e\n", i.e. setprecision(16), setw(24), scientific),
+ * written under outdir.  Asynchronous: the state is reordered on the device
+ * and copied to pinned host memory on a side stream, then host threads
+ * format and write the files while the solver goes on; fin_output_wait
+ * returns when they are on disk (the next fin_output_frame, fin_read_frame
+ * and fin_destroy wait too).  The Euler path holds no aux planes (its
+ * AuxFunc sets none, apps/2d/euler/lib/AuxFunc.cpp:10-13): a%04d.dat gets
+ * maux planes of zeros. */
+int fin_output_frame(fin_solver* s, int nframe, const char* outdir);
+int fin_output_wait(fin_solver* s);
+/* Restart: a q%04d.dat file (this library's or the reference's) becomes the
+ * state, its header the time; alpha and the hybrid flags as fin_set_state. */
+int fin_read_frame(fin_solver* s, const char* path);
+/* conservation.dat (void ConSoln(const StateVars&), lib/2d/ConSoln.cpp:
+ * 34-93): with a directory set, fin_advance / fin_solve append a line after
+ * every accepted step, as FinSolveRK.cpp:362 (FinSolveMD.cpp:284,
+ * FinSolveLxW.cpp:229) calls ConSoln: "%24.16e " for t and for each total
+ * dx*dy*sum q (magnitudes below 1e-99 printed as 0), then a newline; the
+ * file is truncated when t == 0.  The totals are summed on the device with
+ * compensation (the reference sums in order), so they agree with the
+ * reference's to its rounding error.  NULL switches it off.
+ * fin_write_conservation appends the line of the current state now
+ * (RunFinpack.cpp:89 at t = 0). */
+int fin_set_conservation_file(fin_solver* s, const char* outdir);
+int fin_write_conservation(fin_solver* s);
+/* qhelp.dat (void WriteQhelp(), lib/2d/WriteQhelp.cpp:20-43) under outdir. */
+int fin_write_qhelp(const fin_params* p, const char* outdir);
+
 /* Device time of the last fin_solve/fin_advance/fin_step_fixed call in
  * milliseconds (CUDA events on the solver's stream around the whole call). */
 int fin_last_kernel_ms(fin_solver* s, double* ms);

@@ -8,8 +8,10 @@
 * ``MhdRefLib``: oracle/_ref/libfinref_mhd.so, the same for the ideal-MHD
   path (lib/2d/ConstructL.cpp with apps/2d/mhd/lib and the Orszag-Tang case).
   The MHD arrays are q (mx+2mbc, my+2mbc, 8) and aux (mx+2mbc, my+2mbc, 1).
+* ``IoRefLib``: oracle/_ref/libfinref_io.so, the reference's output routines
+  (lib/2d/Output.cpp, WriteQhelp.cpp, ConSoln.cpp) writing their files.
 
-Both take and return numpy arrays in the reference's ghosted dTensorBC3 layout
+All take and return numpy arrays in the reference's ghosted dTensorBC3 layout
 (lib/tensors.h:267-273), shape (mx+2mbc, my+2mbc, meqn).  Only tests/,
 __graft_entry__.smoke() and bench.py's CPU-baseline leg use this module.
 """
@@ -350,3 +352,39 @@ class MhdRefLib:
         dtv = np.array([0.0, dt, p.max_dt])
         rc = self.lib.ref_mhd_finsolve(q, aux, C.byref(tt), tend, dtv)
         return rc, q, aux, tt.value, dtv[1]
+
+
+REF_IO_SO = os.path.join(HERE, "_ref", "libfinref_io.so")
+
+
+class IoRefLib:
+    """The reference's own output routines (lib/2d/Output.cpp, WriteQhelp.cpp,
+    ConSoln.cpp); available where oracle/_ref was built."""
+
+    @staticmethod
+    def available(path=REF_IO_SO):
+        return os.path.exists(path)
+
+    def __init__(self, path=REF_IO_SO):
+        lib = C.CDLL(path)
+        lib.ref_io_setup.argtypes = [C.POINTER(FinParams), C.c_char_p]
+        lib.ref_io_output.argtypes = [_dp, _dp, C.c_double, C.c_int]
+        lib.ref_io_consoln.argtypes = [_dp, _dp, C.c_double]
+        self.lib = lib
+
+    def _aux(self, p, aux):
+        if aux is None:
+            return np.zeros((p.mx + 2 * p.mbc, p.my + 2 * p.mbc, max(p.maux, 1)))
+        return np.ascontiguousarray(aux, dtype=np.float64)
+
+    def output(self, p, outdir, q, t, nframe, aux=None):
+        self.lib.ref_io_setup(C.byref(p), os.fsencode(outdir))
+        self.lib.ref_io_output(np.ascontiguousarray(q, dtype=np.float64), self._aux(p, aux), t, nframe)
+
+    def qhelp(self, p, outdir):
+        self.lib.ref_io_setup(C.byref(p), os.fsencode(outdir))
+        self.lib.ref_io_qhelp()
+
+    def consoln(self, p, outdir, q, t, aux=None):
+        self.lib.ref_io_setup(C.byref(p), os.fsencode(outdir))
+        self.lib.ref_io_consoln(np.ascontiguousarray(q, dtype=np.float64), self._aux(p, aux), t)
