@@ -43,6 +43,7 @@ class FinParams(C.Structure):
         ("tfinal", C.c_double),
         ("nout", C.c_int),
         ("constrained_transport", C.c_int),
+        ("mpp_limiter", C.c_int),
     ]
 
     def copy(self):
@@ -73,6 +74,7 @@ def default_params(**overrides):
     p.physics = FIN_PHYS_EULER
     p.precision = FIN_PREC_FP64
     p.tfinal, p.nout = 0.0, 1
+    p.mpp_limiter = 0
     p.constrained_transport = 1
     for k, v in overrides.items():
         if not hasattr(p, k):

@@ -214,6 +214,6 @@ extern "C" int fin_params_from_ini(const char* path, fin_params* p)
     if (!(p->yhigh > p->ylow)) return fail("grid.yhigh should > grid.ylow.");
     if (!(p->alpha_scaling >= 1.0)) return fail("weno.alpha_scaling should >= 1.");
     if (!(p->epsilon > 0.0)) return fail("weno.epsilon should > 0.");
-    if (mpp) return fail("finess.mpp_limiter = true selects the MPP limiter path, which is not built here");
+    p->mpp_limiter = mpp;
     return FIN_OK;
 }

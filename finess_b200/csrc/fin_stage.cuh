@@ -59,6 +59,14 @@ struct StageArgs {
     const double* Fg;
     const double* Gg;
     size_t gplane;
+    // Lax-Wendroff with the MPP limiter (FinSolveLxW.cpp:126-151): the stage
+    // writes its face fluxes (flux_x [m][mx+1][my], flux_y [m][mx][my+1],
+    // ConstructLxWL's Fhat / Ghat) and no update (flux_only), and leaves the
+    // first face of each direction out of the face-speed maximum, whose smax
+    // entry ConstructLFL.cpp:62-65 overwrites with the global wave speed.
+    double* flux_x;
+    double* flux_y;
+    int flux_only;
     // Hybrid form: troubled-face flags of the step as bit masks (layout of
     // flag_wx / flag_wy below, written by the indicator).  A face takes full
     // WENO when any flag in the 3 x 3 window of same-direction faces around
@@ -510,16 +518,26 @@ __device__ __forceinline__ void stage_tile(const StageArgs& a, const int i0, con
 #pragma unroll
             for (int m = 0; m < MEQN; m++) Fh[m * (TI + 1) * TJ + fi * TJ + fj] = o[m];
             const int gfi = i0 + fi, gj = j0 + fj;
+            if (FG && a.flux_x && gfi <= mx && gj < my) {
+#pragma unroll
+                for (int m = 0; m < MEQN; m++) a.flux_x[(size_t(m) * (mx + 1) + gfi) * my + gj] = double(o[m]);
+            }
             // GetCFL's Max skips NaN entries (Max(NaN, c) = c), so only
             // finite face speeds enter the CFL maximum.
-            if (gfi < mx && gj < my && alpha <= R(1e30)) smax_x = Max(smax_x, alpha);
+            if (gfi < mx && gj < my && alpha <= R(1e30) && !(FG && a.flux_only && gfi == 0 && gj == 0))
+                smax_x = Max(smax_x, alpha);
             if (a.face_alpha_x && gfi <= mx && gj < my) a.face_alpha_x[size_t(gfi) * my + gj] = double(alpha);
         } else {
             const R o[MEQN] = {fh[0], fh[2], fh[1], fh[3], fh[4]};
 #pragma unroll
             for (int m = 0; m < MEQN; m++) Gh[m * TI * (TJ + 1) + fi * (TJ + 1) + fj] = o[m];
             const int gi = i0 + fi, gfj = j0 + fj;
-            if (gi < mx && gfj < my && alpha <= R(1e30)) smax_y = Max(smax_y, alpha);
+            if (FG && a.flux_y && gi < mx && gfj <= my) {
+#pragma unroll
+                for (int m = 0; m < MEQN; m++) a.flux_y[(size_t(m) * mx + gi) * (my + 1) + gfj] = double(o[m]);
+            }
+            if (gi < mx && gfj < my && alpha <= R(1e30) && !(FG && a.flux_only && gi == 0 && gfj == 0))
+                smax_y = Max(smax_y, alpha);
             if (a.face_alpha_y && gi < mx && gfj <= my) a.face_alpha_y[size_t(gi) * (my + 1) + gfj] = double(alpha);
         }
     }
@@ -531,7 +549,7 @@ __device__ __forceinline__ void stage_tile(const StageArgs& a, const int i0, con
     // ---- phase 3: flux difference, stage update, next-stage wave speed ----
     double cs_x = 0.0, cs_y = 0.0;
     const double gam = a.gamma;
-    for (int c = tid; c < TI * TJ; c += NT) {
+    for (int c = tid; c < ((FG && a.flux_only) ? 0 : TI * TJ); c += NT) {
         const int ci = c / TJ, cj = c - ci * TJ;
         const int gi = i0 + ci, gj = j0 + cj;
         if (gi >= mx || gj >= my) continue;

@@ -22,6 +22,7 @@
 #include "fin_hybrid.cuh"
 #include "fin_tmap.h"
 #include "fin_output.h"
+#include "fin_mpp.cuh"
 
 using namespace fin;
 
@@ -119,6 +120,11 @@ struct fin_solver {
     double* h_cons;                 // pinned copy of the totals
     bool cons_pending;              // h_cons holds the totals at cons_t, not yet written
     double cons_t;
+    // Lax-Wendroff with the MPP limiter (fin_mpp.cuh): high-order face
+    // fluxes and the cells' limiting factors
+    double* mpp_fx;                 // [m][mx+1][my]
+    double* mpp_fy;                 // [m][mx][my+1]
+    double* mpp_amin;               // [4][mx][my]
 };
 
 // ---------------------------------------------------------------------------
@@ -537,6 +543,62 @@ int launch_indicator(fin_solver* s, int buf)
     return FIN_OK;
 }
 
+// The Lax-Wendroff step with the MPP limiter (FinSolveLxW.cpp:120-151):
+// ConstructIntegratedR, the stage kernel in its flux-only mode (ConstructLxWL's
+// Fhat / Ghat and the face-speed maxima without the first face of each
+// direction, whose smax entry ConstructLFL.cpp:62-65 replaces by the global
+// wave speed; get_cfl puts it back), then k_mpp_limit and k_mpp_update
+// (ConstructLFL's fluxes, ApplyMPPLimiter2D and the update, fin_mpp.cuh).
+int take_stage_lxw_mpp(fin_solver* s, double dt, int nxt)
+{
+    const fin_params& p = s->p;
+    const int qn = s->cur;
+    const size_t nx = size_t(p.mx + 1) * p.my, ny = size_t(p.mx) * (p.my + 1), nc = size_t(p.mx) * p.my;
+    if (!s->mpp_fx) CK(cudaMalloc(&s->mpp_fx, MEQN * nx * sizeof(double)));
+    if (!s->mpp_fy) CK(cudaMalloc(&s->mpp_fy, MEQN * ny * sizeof(double)));
+    if (!s->mpp_amin) CK(cudaMalloc(&s->mpp_amin, 4 * nc * sizeof(double)));
+    CK(cudaMemsetAsync(s->slots + SLOT_SMAX, 0, 2 * sizeof(double), s->stream));
+    CK(cudaMemsetAsync(s->slots + SLOT_STATUS, 0, sizeof(double), s->stream));
+    CK(cudaMemsetAsync(alpha_slot(s, nxt), 0, 2 * sizeof(double), s->stream));
+    int rc;
+    if ((rc = launch_intflux(s, p.time_order > 2 ? 1 : 0, s->q[qn], nullptr, dt, 0, 0, 0, 0))) return rc;
+    StageArgs a = base_args(s);
+    a.smax_out = s->slots + SLOT_SMAX;
+    a.Fg = s->Fg; a.Gg = s->Gg; a.gplane = s->gplane;
+    a.qin = s->q[qn]; a.A = s->q[qn]; a.B = nullptr; a.qout = s->q[nxt];
+    a.a1 = 1.0; a.a2 = 0.0; a.bdt = dt;
+    a.alpha_in = p.global_alpha ? alpha_slot(s, qn) : nullptr;
+    a.alpha_out = nullptr;
+    a.flux_x = s->mpp_fx;
+    a.flux_y = s->mpp_fy;
+    a.flux_only = 1;
+    if ((rc = launch_stage_timed(s, a, 0))) return rc;
+    mpp::MppArgs m;
+    memset(&m, 0, sizeof(m));
+    m.q = s->q[qn];
+    m.qout = s->q[nxt];
+    m.plane = s->plane;
+    m.mx = p.mx;
+    m.my = p.my;
+    m.bc[0] = p.bc_xlow; m.bc[1] = p.bc_xhigh; m.bc[2] = p.bc_ylow; m.bc[3] = p.bc_yhigh;
+    m.fhat = s->mpp_fx;
+    m.ghat = s->mpp_fy;
+    m.amin = s->mpp_amin;
+    m.alpha = alpha_slot(s, qn);
+    m.dt = dt;
+    m.dx = s->dx;
+    m.dy = s->dy;
+    m.gamma = p.gamma;
+    m.alpha_out = alpha_slot(s, nxt);
+    m.status = s->status;
+    const unsigned blocks = unsigned((nc + 127) / 128);
+    mpp::k_mpp_limit<<<blocks, 128, 0, s->stream>>>(m);
+    mpp::k_mpp_update<<<blocks, 128, 0, s->stream>>>(m);
+    s->launches += 2;
+    CK(cudaGetLastError());
+    return FIN_OK;
+}
+
 // Lax-Wendroff (FinSolveLxW.cpp:120-176) and two-stage multiderivative
 // (FinSolveMD.cpp:116-170, time_order 4) steps from q[cur] into q[nxt].
 int take_stages_lw(fin_solver* s, double dt, int nxt)
@@ -554,6 +616,7 @@ int take_stages_lw(fin_solver* s, double dt, int nxt)
     StageArgs a = base_args(s);
     a.smax_out = s->slots + SLOT_SMAX;
     a.Fg = s->Fg; a.Gg = s->Gg; a.gplane = s->gplane;
+    if (p.time_stepping_method == FIN_TS_LXW && p.mpp_limiter) return take_stage_lxw_mpp(s, dt, nxt);
     if (p.time_stepping_method == FIN_TS_LXW) {
         // F = ConstructIntegratedR(dt, q); q^{n+1} = q + dt L
         if ((rc = launch_intflux(s, p.time_order > 2 ? 1 : 0, s->q[qn], nullptr, dt, 0, 0, 0, 0))) return rc;
@@ -729,9 +792,15 @@ int get_cfl(fin_solver* s, double dt, double dtmax, double* cfl, bool* nonfinite
     if (st & 12u) return set_err(FIN_ERR_CUDA, "a bounded device wait (tensor-core or TMA copy) ran out");
     if (st & 16u) return set_err(FIN_ERR_CUDA, "a TMA destination in shared memory was not 128-byte aligned");
     if (dt > dtmax) return set_err(FIN_ERR_DT_BOUNDS, "dt is out of bounds");
+    double sx = s->h_slots[SLOT_SMAX], sy = s->h_slots[SLOT_SMAX + 1];
+    if (s->p.time_stepping_method == FIN_TS_LXW && s->p.mpp_limiter) {
+        // ConstructLFL.cpp:64-65 set smax(1,1,.) to q^n's global wave speeds
+        sx = Max(sx, s->h_slots[SLOT_ALPHA + 2 * s->cur]);
+        sy = Max(sy, s->h_slots[SLOT_ALPHA + 2 * s->cur + 1]);
+    }
     double c = -100.0;
-    c = Max(dt * s->h_slots[SLOT_SMAX] / s->dx, c);
-    c = Max(dt * s->h_slots[SLOT_SMAX + 1] / s->dy, c);
+    c = Max(dt * sx / s->dx, c);
+    c = Max(dt * sy / s->dy, c);
     if (c > 1.0e8) return set_err(FIN_ERR_CFL_BOUNDS, "CFL number is out of bounds");
     *cfl = c;
     return FIN_OK;
@@ -808,6 +877,7 @@ void fin_params_default(fin_params* p)
     p->tfinal = 0.0;
     p->nout = 1;
     p->constrained_transport = 1;
+    p->mpp_limiter = 0;
 }
 
 const char* fin_last_error(void) { return g_err.c_str(); }
@@ -892,6 +962,9 @@ int fin_destroy(fin_solver* s)
     delete s->cons_path;
     cudaFree(s->d_cons);
     if (s->h_cons) cudaFreeHost(s->h_cons);
+    cudaFree(s->mpp_fx);
+    cudaFree(s->mpp_fy);
+    cudaFree(s->mpp_amin);
     for (int b = 0; b < NBUF; b++) cudaFree(s->q[b]);
     cudaFree(s->mlpP);
     cudaFree(s->flags);

@@ -103,6 +103,16 @@ def riemann_init(p, xc0=0.8, yc0=0.8, states=None):
     return primitive_to_conserved(p.gamma, rho, u, v, pr)
 
 
+def double_rarefaction_init(p, speed=2.0, rho=1.0, pr=0.4):
+    """Near-vacuum test for the positivity limiter: two rarefactions moving
+    apart from x = 0.5 (u = -speed left, +speed right), a weak transverse
+    wave in v, constant rho and p."""
+    x, y = cell_centres(p)
+    u = np.where(x < 0.5 * (p.xlow + p.xhigh), -speed, speed)
+    v = 0.1 * np.sin(2.0 * math.pi * (y - p.ylow) / (p.yhigh - p.ylow))
+    return primitive_to_conserved(p.gamma, np.full_like(x, rho), u, v, np.full_like(x, pr))
+
+
 # --------------------------------------------------------------------------
 # 3. Shock / entropy-wave interaction on [-5,5]x[0,1], periodic in y.
 # --------------------------------------------------------------------------

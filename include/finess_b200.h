@@ -26,7 +26,7 @@
 extern "C" {
 #endif
 
-#define FIN_ABI_VERSION 1
+#define FIN_ABI_VERSION 2
 
 /* ---- status codes ---------------------------------------------------- */
 enum {
@@ -82,6 +82,11 @@ typedef struct fin_params {
     /* [mhd] (python/finess/params/mhd.py:20-26): rebuild B1, B2 from the
      * potential A3 after every stage (apps/2d/mhd/lib/AfterStep.cpp:31-56) */
     int constrained_transport;
+    /* [finess] mpp_limiter (python/finess/params/finess.py:21-26): the
+     * Lax-Wendroff step limits its fluxes toward Lax-Friedrichs ones to keep
+     * density and pressure positive (FinSolveLxW.cpp:126-151); the
+     * reference reads it only in FinSolveLxW */
+    int mpp_limiter;
 } fin_params;
 
 /* Defaults of python/finess/params/finess.py, weno.py, euler.py and mhd.py. */

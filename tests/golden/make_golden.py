@@ -6,7 +6,8 @@ inputs.
 The reference repository stores no golden vectors for this path, so these
 files pin its behaviour: each .npz holds the inputs (ghosted q after the BC
 remap, parameters) and the reference's outputs.  Re-run with
-``python tests/golden/make_golden.py`` after ``make -C oracle ref ref_mhd``.
+``python tests/golden/make_golden.py`` after ``make -C oracle ref ref_mhd`` (``... mhd`` or
+``... mpp`` rewrites only the MHD or the MPP-limiter fixtures).
 """
 import json
 import os
@@ -140,8 +141,39 @@ def mhd_main():
         print("wrote", name, t1, dt1)
 
 
+def mpp_main():
+    """Lax-Wendroff frames with the MPP limiter (FinSolveLxW.cpp:126-151:
+    ConstructLxWL's fluxes, ConstructLFL, ApplyMPPLimiter2D): the
+    four-quadrant Riemann problem and a near-vacuum double rarefaction."""
+    ref = RefLib()
+    runs = []
+    p = P.riemann_params(n=22, weno=FIN_WENO_JS, method=FIN_TS_MD, time_stepping_method=FIN_TS_LXW,
+                         time_order=3, mpp_limiter=1)
+    runs.append(("finsolvelxwmpp_js_riemann22", p, P.riemann_init(p), 0.0, 0.02, 1e-3))
+    p = P.riemann_params(n=26, weno=FIN_WENO_Z, method=FIN_TS_MD, time_stepping_method=FIN_TS_LXW,
+                         time_order=3, mpp_limiter=1)
+    p.my = 12
+    # strong enough that the unlimited method breaks down (NaN) by t = 0.05
+    runs.append(("finsolvelxwmpp_z_rarefaction26", p, P.double_rarefaction_init(p, speed=3.0, pr=0.2), 0.0, 0.05,
+                 1e-3))
+    for name, p, q0, t0, tend, dt in runs:
+        q0 = ref.set_bnd(p, q0)
+        rc, q1, t1, dt1 = ref.finsolve(p, q0, t0, tend, dt)
+        assert rc == 0
+        p_off = p.copy()
+        p_off.mpp_limiter = 0
+        _, q_off, _, _ = ref.finsolve(p_off, q0, t0, tend, dt)
+        np.savez_compressed(os.path.join(HERE, name + ".npz"), params=params_json(p), q0=q0, q1=q1,
+                            t0=t0, t1=t1, tend=tend, dt0=dt, dt1=dt1, q1_unlimited=q_off)
+        mb = p.mbc
+        gap = np.abs(q1 - q_off)[mb:mb + p.mx, mb:mb + p.my].max()
+        print("wrote", name, t1, dt1, "limiter changed the interior by", float(gap))
+
+
 if __name__ == "__main__":
     if sys.argv[1:] == ["mhd"]:
         mhd_main()
+    elif sys.argv[1:] == ["mpp"]:
+        mpp_main()
     else:
         main()

@@ -45,7 +45,7 @@ def test_params_default_matches_python(lib):
     lib.fin_params_default(C.byref(p))
     q = default_params()
     assert p.as_dict() == q.as_dict()
-    assert lib.fin_abi_version() == 1
+    assert lib.fin_abi_version() == 2
 
 
 def test_create_fails_cleanly_without_gpu_or_with_bad_args(lib):

@@ -262,3 +262,52 @@ def test_md_lxw_steps_vs_oracle(Solver, oracle, method, kind):
             qg, _ = s.get_state()
             assert rel_linf(interior(p, qg), interior(p, qo)) <= TOL_STEP
             assert abs(cg - co) <= 1e-14 * co
+
+
+@pytest.mark.parametrize("path", golden_cases("finsolvelxwmpp_"))
+def test_finsolve_lxw_mpp_golden(Solver, path):
+    """Lax-Wendroff frames with the MPP limiter (ConstructLFL,
+    ApplyMPPLimiter2D, FinSolveLxW.cpp:126-151) against the reference's own
+    run; in the near-vacuum case the limiter changes the frame, and the
+    device matches the limited frame, not the unlimited one."""
+    g = load_golden(path)
+    p = g["p"]
+    assert p.mpp_limiter == 1
+    with Solver(p) as s:
+        s.set_state(g["q0"], float(g["t0"]))
+        dtv, n = s.FinSolveMD(float(g["tend"]), [0.0, float(g["dt0"]), p.max_dt])
+        q1, t1 = s.get_state()
+    assert rel_linf(interior(p, q1), interior(p, g["q1"])) <= TOL_FRAME
+    assert abs(t1 - float(g["t1"])) <= 1e-14 * abs(float(g["t1"]))
+    assert abs(dtv[1] - float(g["dt1"])) <= 1e-10 * float(g["dt1"])
+    if "rarefaction" in path:
+        # without the limiter the reference's frame breaks down (NaN); with
+        # it, density and pressure stay positive, here as there
+        assert not np.all(np.isfinite(interior(p, g["q1_unlimited"])))
+        qi = interior(p, q1)
+        rho = qi[..., 0]
+        pr = (p.gamma - 1) * (qi[..., 4] - 0.5 * (qi[..., 1] ** 2 + qi[..., 2] ** 2) / rho)
+        assert rho.min() > 0 and pr.min() > 0
+
+
+def test_lxw_mpp_live_reference(Solver):
+    """One MPP Lax-Wendroff frame on a random four-quadrant state against the
+    reference's FinSolveLxW run live (where oracle/_ref was built)."""
+    from oracle import RefLib
+    if not RefLib.available():
+        pytest.skip("oracle/_ref/libfinref.so not built")
+    from finess_b200._abi import FIN_TS_LXW, FIN_TS_MD
+    ref = RefLib()
+    p = P.riemann_params(n=33, weno=FIN_WENO_Z, method=FIN_TS_MD, time_stepping_method=FIN_TS_LXW, time_order=3,
+                         mpp_limiter=1)
+    p.my = 29
+    q0 = ref.set_bnd(p, P.random_riemann_state(p, np.random.default_rng(77)))
+    rc, q1, t1, dt1 = ref.finsolve(p, q0, 0.0, 0.03, 1e-3)
+    assert rc == 0
+    with Solver(p) as s:
+        s.set_state(q0, 0.0)
+        dtv, n = s.FinSolveMD(0.03, [0.0, 1e-3, p.max_dt])
+        q2, t2 = s.get_state()
+    assert rel_linf(interior(p, q2), interior(p, q1)) <= TOL_FRAME
+    assert abs(t2 - t1) <= 1e-14 * abs(t1)
+    assert abs(dtv[1] - dt1) <= 1e-10 * dt1

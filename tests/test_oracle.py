@@ -114,3 +114,16 @@ def test_reference_hessian_convention(reflib):
     orc.oracle_flux_derivs(1.4, Q, A2, H2)
     assert np.max(np.abs(A1 - A2)) < 1e-14 and np.max(np.abs(H1 - H2)) < 1e-13
     assert abs(H1.reshape(2, 5, 5, 5)[0, 4, 1, 4] - 1.0 / Q[0]) < 1e-15
+
+
+@pytest.mark.parametrize("path", golden_cases("finsolvelxwmpp_"))
+def test_reference_reproduces_mpp_golden(reflib, path):
+    """The MPP-limiter Lax-Wendroff fixtures are the reference's own frames:
+    rerunning its FinSolveLxW (with apps/2d/euler/lib/ApplyMPPLimiter2D)
+    reproduces them bit for bit."""
+    g = load_golden(path)
+    p = g["p"]
+    rc, q1, t1, dt1 = reflib.finsolve(p, g["q0"], float(g["t0"]), float(g["tend"]), float(g["dt0"]))
+    assert rc == 0
+    assert np.array_equal(interior(p, q1), interior(p, g["q1"]))
+    assert t1 == float(g["t1"]) and dt1 == float(g["dt1"])
