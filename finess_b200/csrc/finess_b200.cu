@@ -23,6 +23,7 @@
 #include "fin_tmap.h"
 #include "fin_output.h"
 #include "fin_mpp.cuh"
+#include "fin_rk.cuh"
 
 using namespace fin;
 
@@ -125,6 +126,7 @@ struct fin_solver {
     double* mpp_fx;                 // [m][mx+1][my]
     double* mpp_fy;                 // [m][mx][my+1]
     double* mpp_amin;               // [4][mx][my]
+    int timed_stages;               // stage launches timed in the current step (at most 3)
 };
 
 // ---------------------------------------------------------------------------
@@ -392,10 +394,14 @@ int launch_stage(fin_solver* s, const StageArgs& a)
 // A stage launch bracketed by events when kernel timing is on (stage k of 3).
 int launch_stage_timed(fin_solver* s, const StageArgs& a, int k)
 {
-    if (s->time_kernels) CK(cudaEventRecord(s->kev[2 * k], s->stream));
+    const bool timed = s->time_kernels && k < 3;   // three event pairs; later stages of a step run untimed
+    if (timed) CK(cudaEventRecord(s->kev[2 * k], s->stream));
     int rc = launch_stage(s, a);
     if (rc) return rc;
-    if (s->time_kernels) CK(cudaEventRecord(s->kev[2 * k + 1], s->stream));
+    if (timed) {
+        CK(cudaEventRecord(s->kev[2 * k + 1], s->stream));
+        s->timed_stages = std::max(s->timed_stages, k + 1);
+    }
     return FIN_OK;
 }
 
@@ -403,7 +409,8 @@ int launch_stage_timed(fin_solver* s, const StageArgs& a, int k)
 int collect_kernel_times(fin_solver* s)
 {
     if (!s->time_kernels) return FIN_OK;
-    const int nst = s->p.time_stepping_method == FIN_TS_RK ? 3 : (s->p.time_stepping_method == FIN_TS_MD ? 2 : 1);
+    const int nst = s->timed_stages;
+    s->timed_stages = 0;
     for (int k = 0; k < nst; k++) {
         float ms = 0.f;
         CK(cudaEventElapsedTime(&ms, s->kev[2 * k], s->kev[2 * k + 1]));
@@ -737,11 +744,97 @@ void settle_judge(fin_solver* s, int nxt, double dt, double* cfl)
 // The stages of one step of size dt from q[cur] into q[nxt] (RK3:
 // FinSolveRK.cpp:158-211 with SetRKinfo.cpp:50-64).  Leaves the face-speed
 // maxima of the step in slots SMAX and alpha(q[nxt]) in its slot.
+// FinSolveRK's other orders (FinSolveRK.cpp:117-156, 213-299; coefficients
+// of SetRKinfo.cpp:27-126): forward Euler, SSP-RK2, the ten-stage SSP-RK4 of
+// Ketcheson (2008) and the eight-stage fifth-order method, each stage
+// q_out = a1 A + a2 B + (beta dt) L(q_in) through the stage kernel (the
+// in-place stages of the reference alternate between two registers here),
+// with the element-wise parts of orders 4 and 5 in fin_rk.cuh.  A stage whose
+// reference coefficient multiplies a register by 0 drops that term (0 x
+// finite = 0).
+int take_stages_rk_other(fin_solver* s, double dt, int nxt)
+{
+    const fin_params& p = s->p;
+    const int qn = s->cur;
+    int r1, r2;
+    stage_registers(s, nxt, &r1, &r2);
+    CK(cudaMemsetAsync(s->slots + SLOT_SMAX, 0, 2 * sizeof(double), s->stream));
+    CK(cudaMemsetAsync(s->slots + SLOT_STATUS, 0, sizeof(double), s->stream));
+    const bool ga = p.global_alpha != 0;
+    StageArgs a = base_args(s);
+    a.smax_out = s->slots + SLOT_SMAX;
+    int k = 0;
+    // q[out] = a1 q[A] + a2 q[B] + bdt L(q[in]); A, B < 0: term absent
+    auto stage = [&](int in, int A, double a1, int B, double a2, double bdt, int out) -> int {
+        if (out >= 0) CK(cudaMemsetAsync(alpha_slot(s, out), 0, 2 * sizeof(double), s->stream));
+        a.qin = s->q[in];
+        a.A = A >= 0 ? s->q[A] : nullptr;
+        a.a1 = a1;
+        a.B = B >= 0 ? s->q[B] : nullptr;
+        a.a2 = a2;
+        a.bdt = bdt;
+        a.qout = s->q[out >= 0 ? out : r2];
+        a.alpha_in = ga ? alpha_slot(s, in) : nullptr;
+        a.alpha_out = out >= 0 ? alpha_slot(s, out) : nullptr;
+        return launch_stage_timed(s, a, k++);
+    };
+    const size_t n = size_t(p.mx) * p.my;
+    const int eb = grid_blocks(n);
+    int rc;
+    switch (p.time_order) {
+    case 1:   // :123-130
+        return stage(qn, qn, 1.0, -1, 0.0, 1.0 * dt, nxt);
+    case 2:   // :136-157
+        if ((rc = stage(qn, qn, 1.0, -1, 0.0, 1.0 * dt, r1))) return rc;
+        return stage(r1, r1, 0.5, qn, 0.5, 0.5 * dt, nxt);
+    case 4: {  // :213-265, stages 1-9 with (1, 0, 1/6), stage 10 with (1, 3/5, 1/10)
+        const double b = (1.0 / 6.0) * dt;
+        int in = qn, out = r1;
+        for (int st = 1; st <= 5; st++) {
+            if ((rc = stage(in, in, 1.0, -1, 0.0, b, out))) return rc;
+            in = out;
+            out = out == r1 ? r2 : r1;
+        }
+        // q1 in `in`; q2 = q^n until the swap: q2 <- (q2 + 9 q1)/25 into nxt,
+        // q1 <- 15 q2 - 5 q1 in place
+        CK(cudaMemsetAsync(alpha_slot(s, in), 0, 2 * sizeof(double), s->stream));
+        rk::k_rk4_swap<<<eb, 256, 0, s->stream>>>(s->q[qn], s->q[nxt], s->q[in], s->plane, n, p.gamma,
+                                                  alpha_slot(s, in), s->status);
+        s->launches++;
+        CK(cudaGetLastError());
+        out = in == r1 ? r2 : r1;
+        for (int st = 6; st <= 9; st++) {
+            if ((rc = stage(in, in, 1.0, -1, 0.0, b, out))) return rc;
+            in = out;
+            out = out == r1 ? r2 : r1;
+        }
+        // q^{n+1} = 1 q2 + (3/5) q1 + ((1/10) dt) L(q1), written over q2
+        return stage(in, nxt, 1.0, in, 3.0 / 5.0, (1.0 / 10.0) * dt, nxt);
+    }
+    case 5: {  // :267-288: per stage L(q1) into r2, then the update of q1 (nxt) and q2 (r1)
+        const rk::Rk5Coef c = rk::rk5_coefficients();
+        for (int st = 0; st < 8; st++) {
+            const int in = st == 0 ? qn : nxt;
+            if ((rc = stage(in, -1, 0.0, -1, 0.0, 1.0, -1))) return rc;
+            CK(cudaMemsetAsync(alpha_slot(s, nxt), 0, 2 * sizeof(double), s->stream));
+            rk::k_rk5_update<<<eb, 256, 0, s->stream>>>(s->q[in], s->q[nxt], st == 0 ? nullptr : s->q[r1], s->q[r1],
+                                                        s->q[qn], s->q[r2], s->plane, n, c.g1[st], c.g2[st],
+                                                        c.g3[st], c.delta[st], c.beta[st] * dt, p.gamma,
+                                                        alpha_slot(s, nxt), s->status);
+            s->launches++;
+            CK(cudaGetLastError());
+        }
+        return FIN_OK;
+    }
+    default:
+        return set_err(FIN_ERR_UNSUPPORTED, "Runge-Kutta time_order must be 1 to 5");
+    }
+}
+
 int take_stages_rk(fin_solver* s, double dt, int nxt, const unsigned* flags, int q1, int q2)
 {
     const fin_params& p = s->p;
-    if (p.time_order != 3)
-        return set_err(FIN_ERR_UNSUPPORTED, "only SSP-RK3 (time_order 3) is built");
+    if (p.time_order != 3) return take_stages_rk_other(s, dt, nxt);
     const int qn = s->cur;
     // reset smax, the status word and the alpha slots of the three buffers
     // written this step
@@ -815,8 +908,10 @@ int validate(const fin_params* p)
         return set_err(FIN_ERR_ARG, "Requested WENO Reconstruction not implemented.");
     if (p->mx < 1 || p->my < 1) return set_err(FIN_ERR_ARG, "mx, my must be positive");
     if (p->mbc < 3) return set_err(FIN_ERR_ARG, "mbc must be >= 3 for WENO5");
-    if (p->time_stepping_method == FIN_TS_RK && p->time_order != 3)
-        return set_err(FIN_ERR_UNSUPPORTED, "Runge-Kutta: only SSP-RK3 (time_order 3) is built");
+    if (p->time_stepping_method == FIN_TS_RK && (p->time_order < 1 || p->time_order > 5))
+        return set_err(FIN_ERR_UNSUPPORTED, "Runge-Kutta: time_order 1 to 5 (FinSolveRK.cpp:117-299)");
+    if (p->time_stepping_method == FIN_TS_RK && p->time_order != 3 && p->precision == FIN_PREC_HYBRID)
+        return set_err(FIN_ERR_UNSUPPORTED, "the hybrid form is built for SSP-RK3 (time_order 3)");
     if (p->time_stepping_method == FIN_TS_MD && p->time_order != 4)
         return set_err(FIN_ERR_UNSUPPORTED, "Multiderivative: only time_order 4 (two-stage) is built");
     if (p->time_stepping_method != FIN_TS_RK && p->time_stepping_method != FIN_TS_MD &&
@@ -1241,6 +1336,37 @@ int fin_solve(fin_solver* s, double tend, double* dtv, int* nsteps_out)
 }
 
 // lib/2d/FinSolveRK.cpp:13-371, stopping early after max_steps accepted steps.
+// Qnew's time after one RK step from t (UpdateSoln.cpp:27 applied per stage
+// with SetRKinfo's coefficients, each product and sum rounded on its own;
+// Qstar's time, *t_star, carries over between steps as in FinSolveRK).  The
+// fifth-order method's ten-argument UpdateSoln leaves the times alone
+// (UpdateSoln.cpp:44-80), so its Qnew keeps the step's start time.
+static double rk_time(int order, double t, double dt, double* t_star)
+{
+    switch (order) {
+    case 1:
+        return 1.0 * t + 0.0 * t + 1.0 * dt;
+    case 2:
+        *t_star = 1.0 * t + 0.0 * *t_star + 1.0 * dt;
+        return 0.5 * *t_star + 0.5 * t + 0.5 * dt;
+    case 4: {
+        double t1 = t, t2 = t;
+        for (int s = 1; s <= 5; s++) t1 = 1.0 * t1 + 0.0 * t1 + (1.0 / 6.0) * dt;
+        const double tmp = (t2 + 9.0 * t1) / 25.0;
+        t2 = tmp;
+        t1 = 15.0 * tmp - 5.0 * t1;
+        for (int s = 6; s <= 9; s++) t1 = 1.0 * t1 + 0.0 * t1 + (1.0 / 6.0) * dt;
+        return 1.0 * t2 + (3.0 / 5.0) * t1 + (1.0 / 10.0) * dt;
+    }
+    case 5:
+        return t;
+    default:
+        *t_star = 1.0 * t + 0.0 * *t_star + 1.0 * dt;
+        *t_star = 0.75 * t + 0.25 * *t_star + 0.25 * dt;
+        return (2.0e0 / 3.0e0) * *t_star + (1.0e0 / 3.0e0) * t + (2.0e0 / 3.0e0) * dt;
+    }
+}
+
 // Conservation totals of q[cur] (lib/2d/ConSoln.cpp:34-93, written by
 // FinSolveRK.cpp:362 after every accepted step): computed and copied to
 // pinned memory on the stream; the line goes to the file at the next
@@ -1302,13 +1428,8 @@ int fin_advance(fin_solver* s, double tend, double* dtv, int max_steps, int* nst
             // bookkeeping over its stages; FinSolveMD.cpp:162 and
             // FinSolveLxW.cpp:175 set Qold.t + dt (= told + dt here).
             double t_new;
-            if (p.time_stepping_method == FIN_TS_RK) {
-                t_star = 1.0 * s->t + 0.0 * t_star + 1.0 * dt;
-                t_star = 0.75 * s->t + 0.25 * t_star + 0.25 * dt;
-                t_new = (2.0e0 / 3.0e0) * t_star + (1.0e0 / 3.0e0) * s->t + (2.0e0 / 3.0e0) * dt;
-            } else {
-                t_new = s->t + dt;
-            }
+            if (p.time_stepping_method == FIN_TS_RK) t_new = rk_time(p.time_order, s->t, dt, &t_star);
+            else t_new = s->t + dt;
             if (cfl > 0.0) dt = Min(dtv[2], dt * CFL_target / cfl);
             else dt = dtv[2];
             if (p.verbosity)

@@ -7,7 +7,8 @@ The reference repository stores no golden vectors for this path, so these
 files pin its behaviour: each .npz holds the inputs (ghosted q after the BC
 remap, parameters) and the reference's outputs.  Re-run with
 ``python tests/golden/make_golden.py`` after ``make -C oracle ref ref_mhd`` (``... mhd`` or
-``... mpp`` rewrites only the MHD or the MPP-limiter fixtures).
+``... mpp`` or ``... rk`` rewrites only the MHD, the MPP-limiter or the other Runge-Kutta
+orders' fixtures).
 """
 import json
 import os
@@ -170,10 +171,34 @@ def mpp_main():
         print("wrote", name, t1, dt1, "limiter changed the interior by", float(gap))
 
 
+def rk_orders_main():
+    """FinSolveRK frames of the other Runge-Kutta orders (FinSolveRK.cpp:
+    117-299): forward Euler, SSP-RK2, the ten-stage SSP-RK4 and the
+    eight-stage fifth-order method."""
+    ref = RefLib()
+    runs = []
+    for order, weno, wname in ((1, FIN_WENO_JS, "js"), (2, FIN_WENO_Z, "z"), (4, FIN_WENO_JS, "js"),
+                               (5, FIN_WENO_Z, "z")):
+        p = P.riemann_params(n=24, weno=weno, time_order=order)
+        p.my = 20
+        runs.append((f"finsolverk{order}_{wname}_riemann24", p, P.riemann_init(p), 0.0, 0.03, 1e-3))
+        p = P.vortex_params(n=20, weno=weno, time_order=order, global_alpha=1)
+        runs.append((f"finsolverk{order}_{wname}_vortex20", p, P.vortex_exact(p), 0.0, 0.3, 0.05))
+    for name, p, q0, t0, tend, dt in runs:
+        q0 = ref.set_bnd(p, q0)
+        rc, q1, t1, dt1 = ref.finsolve(p, q0, t0, tend, dt)
+        assert rc == 0
+        np.savez_compressed(os.path.join(HERE, name + ".npz"), params=params_json(p), q0=q0, q1=q1,
+                            t0=t0, t1=t1, tend=tend, dt0=dt, dt1=dt1)
+        print("wrote", name, t1, dt1)
+
+
 if __name__ == "__main__":
     if sys.argv[1:] == ["mhd"]:
         mhd_main()
     elif sys.argv[1:] == ["mpp"]:
         mpp_main()
+    elif sys.argv[1:] == ["rk"]:
+        rk_orders_main()
     else:
         main()

@@ -311,3 +311,21 @@ def test_lxw_mpp_live_reference(Solver):
     assert rel_linf(interior(p, q2), interior(p, q1)) <= TOL_FRAME
     assert abs(t2 - t1) <= 1e-14 * abs(t1)
     assert abs(dtv[1] - dt1) <= 1e-10 * dt1
+
+
+@pytest.mark.parametrize("path", golden_cases("finsolverk1_") + golden_cases("finsolverk2_") +
+                         golden_cases("finsolverk4_") + golden_cases("finsolverk5_"))
+def test_finsolve_rk_orders_golden(Solver, path):
+    """FinSolveRK frames with time_order 1, 2, 4 (ten-stage SSP) and 5
+    (eight stages, whose UpdateSoln leaves Qnew's time at the last step's
+    start) against the reference's own run."""
+    g = load_golden(path)
+    p = g["p"]
+    with Solver(p) as s:
+        s.set_state(g["q0"], float(g["t0"]))
+        dtv, n = s.FinSolveRK(float(g["tend"]), [0.0, float(g["dt0"]), p.max_dt])
+        q1, t1 = s.get_state()
+    assert n > 0
+    assert rel_linf(interior(p, q1), interior(p, g["q1"])) <= TOL_FRAME
+    assert abs(t1 - float(g["t1"])) <= 1e-14 * abs(float(g["t1"]))
+    assert abs(dtv[1] - float(g["dt1"])) <= 1e-10 * float(g["dt1"])

@@ -127,3 +127,15 @@ def test_reference_reproduces_mpp_golden(reflib, path):
     assert rc == 0
     assert np.array_equal(interior(p, q1), interior(p, g["q1"]))
     assert t1 == float(g["t1"]) and dt1 == float(g["dt1"])
+
+
+@pytest.mark.parametrize("path", golden_cases("finsolverk1_") + golden_cases("finsolverk2_") +
+                         golden_cases("finsolverk4_") + golden_cases("finsolverk5_"))
+def test_reference_reproduces_rk_orders_golden(reflib, path):
+    """The other Runge-Kutta orders' fixtures are the reference's own frames."""
+    g = load_golden(path)
+    p = g["p"]
+    rc, q1, t1, dt1 = reflib.finsolve(p, g["q0"], float(g["t0"]), float(g["tend"]), float(g["dt0"]))
+    assert rc == 0
+    assert np.array_equal(interior(p, q1), interior(p, g["q1"]))
+    assert t1 == float(g["t1"]) and dt1 == float(g["dt1"])
