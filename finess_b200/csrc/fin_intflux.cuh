@@ -3,6 +3,12 @@
 // of the domain and its 3-cell ghost frame,
 //   1-state:  F = f + dt/2 (f_t + dt/3 f_tt)                     (:59-296)
 //   2-state:  F = a1 f(q1) + dt b1 f_t(q1) + a2 f(q2) + dt b2 f_t(q2)   (:525-606)
+//   2-state with f_tt (the overload of :608-700, time_order 5 of FinSolveMD):
+//             F = a1 f(q1) + dt (b1 f_t(q1) + c1 dt f_tt(q1))
+//               + a2 f(q2) + dt (b2 f_t(q2) + c2 dt f_tt(q2)),
+//             its f_tt by LocalIntegrate (:298-524), whose mixed derivatives
+//             take a 4th-order stencil (:427-442) where the 1-state form
+//             takes a 2nd-order one
 // with f_t = -A (f_x + g_y) and, when time_order > 2 in the 1-state form,
 //   f_tt = A (f_x+g_y)_t + f''[w, w],
 //   (f_x+g_y)_t = f''[q_x, w] + g''[q_y, w] + A (f_xx + g_xy) + B (f_xy + g_yy),
@@ -36,6 +42,7 @@ struct IntFluxArgs {
     double dx, dy, gamma;
     double dt;              // 1-state: the dt argument of ConstructIntegratedR
     double a1, b1, a2, b2;  // 2-state coefficients
+    double c1, c2;          // f_tt coefficients of the three-coefficient form
     int bc[4];
 };
 
@@ -111,7 +118,9 @@ __device__ __forceinline__ double diff2(double rdx2, double f0, double f1, doubl
     return tmp * rdx2;
 }
 
-// MODE 0: 1-state, f_t only (time_order <= 2); 1: 1-state with f_tt; 2: 2-state.
+// MODE 0: 1-state, f_t only (time_order <= 2); 1: 1-state with f_tt; 2: 2-state;
+// 3: 2-state with f_tt (q2 null: the second state's terms, all with zero
+// coefficients, add nothing).
 template <int MODE, int TI, int TJ>
 __global__ void __launch_bounds__(TI * TJ) k_intflux(const IntFluxArgs a)
 {
@@ -128,7 +137,7 @@ __global__ void __launch_bounds__(TI * TJ) k_intflux(const IntFluxArgs a)
     const double rdx = 1.0 / a.dx, rdy = 1.0 / a.dy;
     double Fo[MEQN] = {0, 0, 0, 0, 0}, Go[MEQN] = {0, 0, 0, 0, 0};
 
-    const int nstate = MODE == 2 ? 2 : 1;
+    const int nstate = (MODE == 2 || (MODE == 3 && a.q2)) ? 2 : 1;
     for (int st = 0; st < nstate; st++) {
         const double* q = st == 0 ? a.q1 : a.q2;
         if (st) __syncthreads();
@@ -158,7 +167,7 @@ __global__ void __launch_bounds__(TI * TJ) k_intflux(const IntFluxArgs a)
             const double fx = diff1(rdx, AT(fb, m, -2, 0), AT(fb, m, -1, 0), AT(fb, m, 1, 0), AT(fb, m, 2, 0));
             const double gy = diff1(rdy, AT(gb, m, 0, -2), AT(gb, m, 0, -1), AT(gb, m, 0, 1), AT(gb, m, 0, 2));
             w[m] = fx + gy;
-            if (MODE == 1) {
+            if (MODE == 1 || MODE == 3) {
                 qx[m] = diff1(rdx, AT(qb, m, -2, 0), AT(qb, m, -1, 0), AT(qb, m, 1, 0), AT(qb, m, 2, 0));
                 qy[m] = diff1(rdy, AT(qb, m, 0, -2), AT(qb, m, 0, -1), AT(qb, m, 0, 1), AT(qb, m, 0, 2));
             }
@@ -178,7 +187,7 @@ __global__ void __launch_bounds__(TI * TJ) k_intflux(const IntFluxArgs a)
             }
         } else {
             double ftt[MEQN] = {0, 0, 0, 0, 0}, gtt[MEQN] = {0, 0, 0, 0, 0};
-            if (MODE == 1) {
+            if (MODE == 1 || MODE == 3) {
                 double h1[MEQN], h2[MEQN], fpg[MEQN], v1[MEQN], v2[MEQN], t1[MEQN], t2[MEQN];
                 const DVar vx = dvar(a.gamma, c, qx), vy = dvar(a.gamma, c, qy);
                 dflux2(a.gamma, 1, c, qx, vx, w, vw, h1);
@@ -189,13 +198,26 @@ __global__ void __launch_bounds__(TI * TJ) k_intflux(const IntFluxArgs a)
                                              AT(fb, m, 1, 0), AT(fb, m, 2, 0));
                     const double gyy = diff2(rdy * rdy, AT(gb, m, 0, -2), AT(gb, m, 0, -1), AT(gb, m, 0, 0),
                                              AT(gb, m, 0, 1), AT(gb, m, 0, 2));
-                    // 2nd-order mixed derivative, ConstructIntegratedR.cpp:204-211
-                    double fxy = 0.5 * (AT(fb, m, 1, 1) - AT(fb, m, -1, 1)) * rdx;
-                    fxy -= 0.5 * (AT(fb, m, 1, -1) - AT(fb, m, -1, -1)) * rdx;
-                    fxy *= 0.5 * rdy;
-                    double gxy = 0.5 * (AT(gb, m, 1, 1) - AT(gb, m, -1, 1)) * rdx;
-                    gxy -= 0.5 * (AT(gb, m, 1, -1) - AT(gb, m, -1, -1)) * rdx;
-                    gxy *= 0.5 * rdy;
+                    double fxy, gxy;
+                    if (MODE == 3) {
+                        // 4th-order mixed derivative of LocalIntegrate, ConstructIntegratedR.cpp:427-442
+                        auto mixed = [&](const double* r) {
+                            double t = 0.25 * (AT(r, m, 1, 1) - AT(r, m, -1, 1) - AT(r, m, 1, -1) + AT(r, m, -1, -1));
+                            t -= (1. / 24.) * (AT(r, m, 2, 1) + AT(r, m, -2, -1) - AT(r, m, 2, -1) - AT(r, m, -2, 1) -
+                                               AT(r, m, 1, 2) - AT(r, m, -1, -2) + AT(r, m, 1, -2) + AT(r, m, -1, 2));
+                            return t * (1. / (a.dx * a.dy));
+                        };
+                        fxy = mixed(fb);
+                        gxy = mixed(gb);
+                    } else {
+                        // 2nd-order mixed derivative, ConstructIntegratedR.cpp:204-211
+                        fxy = 0.5 * (AT(fb, m, 1, 1) - AT(fb, m, -1, 1)) * rdx;
+                        fxy -= 0.5 * (AT(fb, m, 1, -1) - AT(fb, m, -1, -1)) * rdx;
+                        fxy *= 0.5 * rdy;
+                        gxy = 0.5 * (AT(gb, m, 1, 1) - AT(gb, m, -1, 1)) * rdx;
+                        gxy -= 0.5 * (AT(gb, m, 1, -1) - AT(gb, m, -1, -1)) * rdx;
+                        gxy *= 0.5 * rdy;
+                    }
                     v1[m] = fxx + gxy;
                     v2[m] = fxy + gyy;
                 }
@@ -215,10 +237,20 @@ __global__ void __launch_bounds__(TI * TJ) k_intflux(const IntFluxArgs a)
                     gtt[m] += h2[m];
                 }
             }
+            if (MODE == 3) {
+                const double al = st == 0 ? a.a1 : a.a2, be = st == 0 ? a.b1 : a.b2, ch = st == 0 ? a.c1 : a.c2;
 #pragma unroll
-            for (int m = 0; m < MEQN; m++) {
-                Fo[m] = AT(fb, m, 0, 0) + 0.5 * a.dt * (-ft[m] + a.dt / 3.0 * ftt[m]);
-                Go[m] = AT(gb, m, 0, 0) + 0.5 * a.dt * (-gt[m] + a.dt / 3.0 * gtt[m]);
+                for (int m = 0; m < MEQN; m++) {
+                    // ConstructIntegratedR.cpp:685-692, left to right
+                    Fo[m] = Fo[m] + al * AT(fb, m, 0, 0) + a.dt * (be * -ft[m] + ch * a.dt * ftt[m]);
+                    Go[m] = Go[m] + al * AT(gb, m, 0, 0) + a.dt * (be * -gt[m] + ch * a.dt * gtt[m]);
+                }
+            } else {
+#pragma unroll
+                for (int m = 0; m < MEQN; m++) {
+                    Fo[m] = AT(fb, m, 0, 0) + 0.5 * a.dt * (-ft[m] + a.dt / 3.0 * ftt[m]);
+                    Go[m] = AT(gb, m, 0, 0) + 0.5 * a.dt * (-gt[m] + a.dt / 3.0 * gtt[m]);
+                }
             }
         }
 #undef AT

@@ -489,7 +489,7 @@ int check_status(fin_solver* s)
 // the f_tt terms, 2 = 2-state.
 constexpr int IF_TI = 16, IF_TJ = 16;
 int launch_intflux(fin_solver* s, int mode, const double* q1, const double* q2, double dt, double a1,
-                   double b1, double a2, double b2)
+                   double b1, double a2, double b2, double c1 = 0.0, double c2 = 0.0)
 {
     IntFluxArgs f;
     memset(&f, 0, sizeof(f));
@@ -498,12 +498,14 @@ int launch_intflux(fin_solver* s, int mode, const double* q1, const double* q2, 
     f.mx = s->p.mx; f.my = s->p.my;
     f.dx = s->dx; f.dy = s->dy; f.gamma = s->p.gamma; f.dt = dt;
     f.a1 = a1; f.b1 = b1; f.a2 = a2; f.b2 = b2;
+    f.c1 = c1; f.c2 = c2;
     f.bc[0] = s->p.bc_xlow; f.bc[1] = s->p.bc_xhigh; f.bc[2] = s->p.bc_ylow; f.bc[3] = s->p.bc_yhigh;
     constexpr size_t smem = 3 * MEQN * (IF_TI + 4) * (IF_TJ + 4) * sizeof(double);
     dim3 grid((s->p.my + 6 + IF_TJ - 1) / IF_TJ, (s->p.mx + 6 + IF_TI - 1) / IF_TI);
     if (mode == 0) k_intflux<0, IF_TI, IF_TJ><<<grid, IF_TI * IF_TJ, smem, s->stream>>>(f);
     else if (mode == 1) k_intflux<1, IF_TI, IF_TJ><<<grid, IF_TI * IF_TJ, smem, s->stream>>>(f);
-    else k_intflux<2, IF_TI, IF_TJ><<<grid, IF_TI * IF_TJ, smem, s->stream>>>(f);
+    else if (mode == 2) k_intflux<2, IF_TI, IF_TJ><<<grid, IF_TI * IF_TJ, smem, s->stream>>>(f);
+    else k_intflux<3, IF_TI, IF_TJ><<<grid, IF_TI * IF_TJ, smem, s->stream>>>(f);
     s->launches++;
     CK(cudaGetLastError());
     return FIN_OK;
@@ -632,6 +634,30 @@ int take_stages_lw(fin_solver* s, double dt, int nxt)
         a.alpha_in = ga ? alpha_slot(s, qn) : nullptr;
         a.alpha_out = alpha_slot(s, nxt);
         return launch_stage_timed(s, a, 0);
+    }
+    if (p.time_order == 5) {
+        // FinSolveMD.cpp:172-226 (coefficients tuned for stability along the
+        // imaginary axis, rho = 8.209945182837015e-02), the three-coefficient
+        // ConstructIntegratedR of ConstructIntegratedR.cpp:608-700:
+        // stage 1: F = CIR((2/5) dt; 1, 1/2, (125/8) rho; q^n | 0, 0, 0; q*),
+        //          q* = q^n + ((2/5) dt) L(q^n)
+        const double d1 = 2.0 / 5.0 * dt;
+        if ((rc = launch_intflux(s, 3, s->q[qn], nullptr, d1, 1.0, 0.5, 0.0, 0.0, 125. / 8. * 8.209945182837015e-02,
+                                 0.0)))
+            return rc;
+        a.qin = s->q[qn]; a.A = s->q[qn]; a.B = nullptr; a.qout = s->q[q1];
+        a.a1 = 1.0; a.a2 = 0.0; a.bdt = d1;
+        a.alpha_in = ga ? alpha_slot(s, qn) : nullptr;
+        a.alpha_out = alpha_slot(s, q1);
+        if ((rc = launch_stage_timed(s, a, 0))) return rc;
+        // stage 2: F = CIR(dt; 1, 1/2, 1/16; q^n | 0, 0, 5/48; q*); q^{n+1} = q^n + dt L(q*)
+        if ((rc = launch_intflux(s, 3, s->q[qn], s->q[q1], dt, 1.0, 0.5, 0.0, 0.0, (1.0 / 16.0), (5.0 / 48.0))))
+            return rc;
+        a.qin = s->q[q1]; a.A = s->q[qn]; a.B = nullptr; a.qout = s->q[nxt];
+        a.a1 = 1.0; a.a2 = 0.0; a.bdt = dt;
+        a.alpha_in = ga ? alpha_slot(s, q1) : nullptr;
+        a.alpha_out = alpha_slot(s, nxt);
+        return launch_stage_timed(s, a, 1);
     }
     // stage 1: F = ConstructIntegratedR(dt/2, q^n) (f_tt included: time_order 4 > 2);
     //          q* = q^n + (dt/2) L
@@ -912,8 +938,8 @@ int validate(const fin_params* p)
         return set_err(FIN_ERR_UNSUPPORTED, "Runge-Kutta: time_order 1 to 5 (FinSolveRK.cpp:117-299)");
     if (p->time_stepping_method == FIN_TS_RK && p->time_order != 3 && p->precision == FIN_PREC_HYBRID)
         return set_err(FIN_ERR_UNSUPPORTED, "the hybrid form is built for SSP-RK3 (time_order 3)");
-    if (p->time_stepping_method == FIN_TS_MD && p->time_order != 4)
-        return set_err(FIN_ERR_UNSUPPORTED, "Multiderivative: only time_order 4 (two-stage) is built");
+    if (p->time_stepping_method == FIN_TS_MD && p->time_order != 4 && p->time_order != 5)
+        return set_err(FIN_ERR_UNSUPPORTED, "Multiderivative: time_order 4 or 5 (two-stage, FinSolveMD.cpp:116-226)");
     if (p->time_stepping_method != FIN_TS_RK && p->time_stepping_method != FIN_TS_MD &&
         p->time_stepping_method != FIN_TS_LXW)
         return set_err(FIN_ERR_ARG, "time_stepping_method");

@@ -184,6 +184,12 @@ def rk_orders_main():
         runs.append((f"finsolverk{order}_{wname}_riemann24", p, P.riemann_init(p), 0.0, 0.03, 1e-3))
         p = P.vortex_params(n=20, weno=weno, time_order=order, global_alpha=1)
         runs.append((f"finsolverk{order}_{wname}_vortex20", p, P.vortex_exact(p), 0.0, 0.3, 0.05))
+    # the fifth-order two-stage multiderivative method (FinSolveMD.cpp:172-226)
+    p = P.riemann_params(n=24, weno=FIN_WENO_Z, method=FIN_TS_MD, time_order=5)
+    p.my = 20
+    runs.append(("finsolvemd5_z_riemann24", p, P.riemann_init(p), 0.0, 0.02, 1e-3))
+    p = P.vortex_params(n=20, weno=FIN_WENO_JS, mbc=5, time_stepping_method=FIN_TS_MD, time_order=5)
+    runs.append(("finsolvemd5_js_vortex20", p, P.vortex_exact(p), 0.0, 0.3, 0.05))
     for name, p, q0, t0, tend, dt in runs:
         q0 = ref.set_bnd(p, q0)
         rc, q1, t1, dt1 = ref.finsolve(p, q0, t0, tend, dt)

@@ -314,11 +314,12 @@ def test_lxw_mpp_live_reference(Solver):
 
 
 @pytest.mark.parametrize("path", golden_cases("finsolverk1_") + golden_cases("finsolverk2_") +
-                         golden_cases("finsolverk4_") + golden_cases("finsolverk5_"))
+                         golden_cases("finsolverk4_") + golden_cases("finsolverk5_") + golden_cases("finsolvemd5_"))
 def test_finsolve_rk_orders_golden(Solver, path):
     """FinSolveRK frames with time_order 1, 2, 4 (ten-stage SSP) and 5
     (eight stages, whose UpdateSoln leaves Qnew's time at the last step's
-    start) against the reference's own run."""
+    start), and FinSolveMD frames with time_order 5 (the three-coefficient
+    ConstructIntegratedR), against the reference's own run."""
     g = load_golden(path)
     p = g["p"]
     with Solver(p) as s:

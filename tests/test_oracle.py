@@ -130,7 +130,7 @@ def test_reference_reproduces_mpp_golden(reflib, path):
 
 
 @pytest.mark.parametrize("path", golden_cases("finsolverk1_") + golden_cases("finsolverk2_") +
-                         golden_cases("finsolverk4_") + golden_cases("finsolverk5_"))
+                         golden_cases("finsolverk4_") + golden_cases("finsolverk5_") + golden_cases("finsolvemd5_"))
 def test_reference_reproduces_rk_orders_golden(reflib, path):
     """The other Runge-Kutta orders' fixtures are the reference's own frames."""
     g = load_golden(path)
