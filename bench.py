@@ -8,6 +8,7 @@ initial data; the state (673 MB per FP64 array) is far larger than the 126 MB
 L2, so no L2 flush is needed between steps.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--forms fp64,fp32,hybrid]
+    python bench.py --space-orders [--n N] [--steps K]    # LLF, WENO7/9/11 beside WENO5 (FP64)
 
 The headline form is the hybrid (FP32 bulk + troubled-face network run every
 HYB_EVERY accepted steps, judge step every HYB_JUDGE_EVERY steps) when trained
@@ -279,6 +280,58 @@ def run_reference_arm(args):
     print(json.dumps(line), flush=True)
 
 
+SPACE_ORDERS = ((5, "JS"), (1, "JS"), (7, "JS"), (7, "Z"), (7, "FD"), (9, "JS"), (9, "Z"), (9, "FD"), (11, "JS"))
+
+
+def run_space_orders(args):
+    """The other spatial orders of ConstructL (LLF, JS7/9/11, Z7/9, FD7/9,
+    FP64, SSP-RK3) beside WENO5-JS: the isentropic vortex on [0,10]^2 at
+    n x n, periodic, CFL 0.4, one JSON line per scheme with the device time
+    per step (fin_advance, CUDA events) and, where oracle/_ref exists, the
+    reference's own FinSolveRK on a bounded 256^2 sample (3 steps, all host
+    threads)."""
+    ws, rank, _ = dist_env()
+    if rank != 0:
+        return
+    from finess_b200 import problems as P
+    from finess_b200._abi import FIN_WENO_FD, FIN_WENO_JS, FIN_WENO_Z
+    from finess_b200.batch import first_dt as batch_first_dt
+    from finess_b200.solver import Solver
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    from oracle import RefLib
+    ref = RefLib() if (RefLib.available() and not args.no_cpu_baseline) else None
+    ver = {"JS": FIN_WENO_JS, "Z": FIN_WENO_Z, "FD": FIN_WENO_FD}
+    n = args.n if args.n != N_CELLS else 2048
+    for so, vn in SPACE_ORDERS:
+        mbc = max(3, (so + 1) // 2)
+        p = P.vortex_params(n=n, weno=ver[vn], space_order=so, mbc=mbc)
+        q0 = P.vortex_exact(p)
+        dt0 = batch_first_dt(p, q0)
+        with Solver(p) as s:
+            s.set_state(q0)
+            s.advance(1.0, np.array([0.0, dt0, p.max_dt]), args.warmup)
+            _, k = s.advance(1.0, np.array([0.0, dt0, p.max_dt]), args.steps)
+            ms = s.last_kernel_ms()
+        line = {"metric": f"2D Euler space_order {so} ({vn}) cell-updates/s, FP64 SSP-RK3", "value": n * n * k / (ms * 1e-3),
+                "unit": UNIT, "n_gpus": 1, "steps": k, "warmup": args.warmup, "ms_per_step": ms / k,
+                "higher_is_better": True, "dtype": "f64", "data": "synthetic",
+                "config": {"workload": "euler2d_vortex_periodic_rk3", "grid": f"{n}x{n}", "space_order": so,
+                           "weno": vn, "mbc": mbc, "cfl": 0.4}}
+        if ref is not None:
+            m = 256
+            pr = P.vortex_params(n=m, weno=ver[vn], space_order=so, mbc=mbc)
+            qr = P.vortex_exact(pr)
+            dtr = batch_first_dt(pr, qr)
+            qr = ref.set_bnd(pr, qr)
+            t0 = time.perf_counter()
+            rc, _, _, _ = ref.finsolve(pr, qr, 0.0, 2.5 * dtr, dtr)   # three steps
+            el = time.perf_counter() - t0
+            line["cpu_baseline"] = {"value": m * m * 3 / el, "unit": UNIT, "kind": "reference",
+                                    "cores": int(os.environ.get("OMP_NUM_THREADS", os.cpu_count() or 1)),
+                                    "sample": f"3 SSP-RK3 steps at {m}x{m}, {el:.2f} s", "rc": rc}
+        print(json.dumps(line), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -290,8 +343,15 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-md", action="store_true")
     ap.add_argument("--no-accuracy", action="store_true")
+    ap.add_argument("--space-orders", action="store_true",
+                    help="time the other spatial orders (LLF, WENO7/9/11) instead of the headline workload")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
+    if args.space_orders:
+        if args.steps == 50:
+            args.steps = 10
+        run_space_orders(args)
+        return
     if args.impl == "reference":
         run_reference_arm(args)
         return

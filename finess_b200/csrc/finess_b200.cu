@@ -24,6 +24,7 @@
 #include "fin_output.h"
 #include "fin_mpp.cuh"
 #include "fin_rk.cuh"
+#include "fin_weno_hi.cuh"
 
 using namespace fin;
 
@@ -381,8 +382,62 @@ int launch_stage_hyb(fin_solver* s, const StageArgs& a)
     return set_err(FIN_ERR_ARG, "weno_version");
 }
 
+int grid_blocks(size_t n);
+
+// Spatial orders other than 5 (fin_weno_hi.cuh, FP64): one thread per face
+// into the face-flux arrays, then the flux difference and stage update.
+template <int ORDER, int VER>
+int launch_stage_hi_t(fin_solver* s, const StageArgs& a)
+{
+    const size_t nx = size_t(a.mx + 1) * a.my, ny = size_t(a.mx) * (a.my + 1);
+    if (!s->mpp_fx) CK(cudaMalloc(&s->mpp_fx, MEQN * nx * sizeof(double)));
+    if (!s->mpp_fy) CK(cudaMalloc(&s->mpp_fy, MEQN * ny * sizeof(double)));
+    hi::HiArgs h;
+    memset(&h, 0, sizeof(h));
+    h.q = a.qin;
+    h.plane = a.plane;
+    h.mx = a.mx;
+    h.my = a.my;
+    for (int k = 0; k < 4; k++) h.bc[k] = a.bc[k];
+    h.gamma = a.gamma;
+    h.eps = a.eps;
+    h.pw = a.pw;
+    h.alpha_scaling = a.alpha_scaling;
+    h.alpha_in = a.alpha_in;
+    h.fx = s->mpp_fx;
+    h.fy = s->mpp_fy;
+    h.smax_out = a.smax_out;
+    h.face_alpha_x = a.face_alpha_x;
+    h.face_alpha_y = a.face_alpha_y;
+    h.status = a.status;
+    const size_t nf = nx + ny;
+    hi::k_hi_faces<ORDER, VER><<<unsigned((nf + 127) / 128), 128, 0, s->stream>>>(h);
+    CK(cudaGetLastError());
+    hi::k_hi_update<<<grid_blocks(size_t(a.mx) * a.my), 256, 0, s->stream>>>(s->mpp_fx, s->mpp_fy, a);
+    CK(cudaGetLastError());
+    s->launches += 2;
+    return FIN_OK;
+}
+
+int launch_stage_hi(fin_solver* s, const StageArgs& a)
+{
+    const int v = s->p.weno_version;
+    switch (s->p.space_order) {
+    case 1: return launch_stage_hi_t<1, FIN_WENO_JS>(s, a);
+    case 7:
+        return v == FIN_WENO_Z ? launch_stage_hi_t<7, FIN_WENO_Z>(s, a)
+             : v == FIN_WENO_FD ? launch_stage_hi_t<7, FIN_WENO_FD>(s, a) : launch_stage_hi_t<7, FIN_WENO_JS>(s, a);
+    case 9:
+        return v == FIN_WENO_Z ? launch_stage_hi_t<9, FIN_WENO_Z>(s, a)
+             : v == FIN_WENO_FD ? launch_stage_hi_t<9, FIN_WENO_FD>(s, a) : launch_stage_hi_t<9, FIN_WENO_JS>(s, a);
+    case 11: return launch_stage_hi_t<11, FIN_WENO_JS>(s, a);
+    }
+    return set_err(FIN_ERR_ARG, "Requested WENO Reconstruction not implemented.");
+}
+
 int launch_stage(fin_solver* s, const StageArgs& a)
 {
+    if (s->p.space_order != 5) return launch_stage_hi(s, a);
     if (a.Fg) return launch_stage_fg(s, a);
     if (a.flags) return launch_stage_hyb(s, a);
     if (s->p.precision == FIN_PREC_HYBRID) return launch_stage_r<float>(s, a);
@@ -929,11 +984,23 @@ int validate(const fin_params* p)
 {
     if (!p) return set_err(FIN_ERR_ARG, "null params");
     if (p->physics != FIN_PHYS_EULER || p->meqn != 5) return set_err(FIN_ERR_UNSUPPORTED, "only 2D Euler (meqn 5)");
-    if (p->space_order != 5) return set_err(FIN_ERR_UNSUPPORTED, "space_order must be 5");
     if (p->weno_version != FIN_WENO_JS && p->weno_version != FIN_WENO_Z && p->weno_version != FIN_WENO_FD)
         return set_err(FIN_ERR_ARG, "Requested WENO Reconstruction not implemented.");
+    // GetWenoReconstruct (lib/WenoReconstruct.cpp:40-71): JS 5/7/9/11, FD 5/7/9,
+    // Z 5/7/9, and order 1 (LLF) for every version; anything else throws there
+    {
+        const int so = p->space_order, v = p->weno_version;
+        const bool built = so == 1 || so == 5 || so == 7 || so == 9 || (so == 11 && v == FIN_WENO_JS);
+        if (!built) return set_err(FIN_ERR_ARG, "Requested WENO Reconstruction not implemented.");
+    }
     if (p->mx < 1 || p->my < 1) return set_err(FIN_ERR_ARG, "mx, my must be positive");
     if (p->mbc < 3) return set_err(FIN_ERR_ARG, "mbc must be >= 3 for WENO5");
+    if (p->space_order != 5) {
+        // ConstructL.cpp:31-33: the stencil reaches r = (space_order + 1) / 2 cells out
+        if (p->mbc < (p->space_order + 1) / 2) return set_err(FIN_ERR_ARG, "mbc must be >= (space_order + 1) / 2");
+        if (p->time_stepping_method != FIN_TS_RK || p->precision != FIN_PREC_FP64)
+            return set_err(FIN_ERR_UNSUPPORTED, "space orders other than 5 are built for FP64 Runge-Kutta stepping");
+    }
     if (p->time_stepping_method == FIN_TS_RK && (p->time_order < 1 || p->time_order > 5))
         return set_err(FIN_ERR_UNSUPPORTED, "Runge-Kutta: time_order 1 to 5 (FinSolveRK.cpp:117-299)");
     if (p->time_stepping_method == FIN_TS_RK && p->time_order != 3 && p->precision == FIN_PREC_HYBRID)
@@ -956,7 +1023,7 @@ int validate(const fin_params* p)
     if ((p->bc_xlow == FIN_BC_PERIODIC) != (p->bc_xhigh == FIN_BC_PERIODIC) ||
         (p->bc_ylow == FIN_BC_PERIODIC) != (p->bc_yhigh == FIN_BC_PERIODIC))
         return set_err(FIN_ERR_ARG, "periodic boundaries come in pairs");
-    const int H = 3;
+    const int H = std::max(3, (p->space_order + 1) / 2);
     if ((p->bc_xlow == FIN_BC_PERIODIC && p->mx < H) || (p->bc_ylow == FIN_BC_PERIODIC && p->my < H))
         return set_err(FIN_ERR_ARG, "periodic direction shorter than the stencil halo");
     if (p->precision != FIN_PREC_FP64 && p->precision != FIN_PREC_FP32 && p->precision != FIN_PREC_HYBRID)

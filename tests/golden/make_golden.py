@@ -7,8 +7,8 @@ The reference repository stores no golden vectors for this path, so these
 files pin its behaviour: each .npz holds the inputs (ghosted q after the BC
 remap, parameters) and the reference's outputs.  Re-run with
 ``python tests/golden/make_golden.py`` after ``make -C oracle ref ref_mhd`` (``... mhd`` or
-``... mpp`` or ``... rk`` rewrites only the MHD, the MPP-limiter or the other Runge-Kutta
-orders' fixtures).
+``... mpp``, ``... rk`` or ``... space`` rewrites only the MHD, the MPP-limiter, the other
+Runge-Kutta orders' or the other spatial orders' fixtures).
 """
 import json
 import os
@@ -199,8 +199,76 @@ def rk_orders_main():
         print("wrote", name, t1, dt1)
 
 
+SPACE_ORDERS = ((1, FIN_WENO_JS, "js"), (7, FIN_WENO_JS, "js"), (7, FIN_WENO_Z, "z"), (7, FIN_WENO_FD, "fd"),
+                (9, FIN_WENO_JS, "js"), (9, FIN_WENO_Z, "z"), (9, FIN_WENO_FD, "fd"), (11, FIN_WENO_JS, "js"))
+
+
+def space_orders_main():
+    """ConstructL and FinSolveRK (SSP-RK3) of the other spatial orders that
+    GetWenoReconstruct accepts (lib/WenoReconstruct.cpp:40-71): LLF (order 1),
+    JS7/9/11, Z7/9 and FD7/9, each with mbc = r = (order + 1) / 2 (order 1
+    keeps mbc 3)."""
+    ref = RefLib()
+    rng = np.random.default_rng(7911)
+    for so, weno, wname in SPACE_ORDERS:
+        mbc = max(3, (so + 1) // 2)
+        cases = []
+        p = P.vortex_params(n=22, weno=weno, space_order=so, mbc=mbc)
+        p.my = 16
+        cases.append((f"hiorder_constructl{so}_{wname}_smooth_periodic", p, P.random_smooth_state(p, rng)))
+        p = P.riemann_params(n=18, weno=weno, space_order=so, mbc=mbc, global_alpha=0)
+        p.my = 24
+        cases.append((f"hiorder_constructl{so}_{wname}_riemann_local_alpha", p, P.random_riemann_state(p, rng)))
+        for name, p, q in cases:
+            q = ref.set_bnd(p, q)
+            L, smax = ref.construct_l(p, q)
+            a1, a2 = ref.global_wave_spd(p, q)
+            np.savez_compressed(os.path.join(HERE, name + ".npz"), params=params_json(p), q=q, L=L, smax=smax,
+                                alpha=np.array([a1, a2]))
+            print("wrote", name)
+        runs = []
+        p = P.riemann_params(n=24, weno=weno, space_order=so, mbc=mbc)
+        p.my = 20
+        # linear weights oscillate at the shocks and the reference's own run
+        # loses positivity by t = 0.01 (FD7) / 0.015 (FD9): stop before that
+        tend = 0.005 if weno == FIN_WENO_FD else 0.03
+        runs.append((f"hiorder_finsolverk{so}_{wname}_riemann24", p, P.riemann_init(p), 0.0, tend, 1e-3))
+        p = P.vortex_params(n=20, weno=weno, space_order=so, mbc=mbc)
+        runs.append((f"hiorder_finsolverk{so}_{wname}_vortex20", p, P.vortex_exact(p), 0.0, 0.3, 0.05))
+        for name, p, q0, t0, tend, dt in runs:
+            q0 = ref.set_bnd(p, q0)
+            rc, q1, t1, dt1 = ref.finsolve(p, q0, t0, tend, dt)
+            assert rc == 0
+            # FinSolveRK fills no ghost cells after the last update, so with
+            # mbc > 3 the outer layers of its frame are left-over heap data:
+            # store the frame with its ghosts refilled (tests compare interiors)
+            q1 = ref.set_bnd(p, q1)
+            assert np.isfinite(q1).all(), name
+            # The reference's own sensitivity: how far its frame moves when
+            # every value of q0 moves by one ulp (largest of three seeded
+            # perturbations).  The high-order smoothness indicators cancel
+            # terms with coefficients up to ~4e8, so near-flat states put
+            # roundoff into the weights and the orders 9 and 11 frames move
+            # by up to ~1e-7.
+            sens = 0.0
+            prng = np.random.default_rng(1234)
+            for _ in range(3):
+                up = prng.random(q0.shape) < 0.5
+                qp = ref.set_bnd(p, np.where(up, np.nextafter(q0, np.inf), np.nextafter(q0, -np.inf)))
+                rcp_, qp1, _, _ = ref.finsolve(p, qp, t0, tend, dt)
+                assert rcp_ == 0
+                m = mbc
+                a, b = qp1[m:m + p.mx, m:m + p.my], q1[m:m + p.mx, m:m + p.my]
+                sens = max(sens, float(np.abs(a - b).max() / np.abs(b).max()))
+            np.savez_compressed(os.path.join(HERE, name + ".npz"), params=params_json(p), q0=q0, q1=q1,
+                                t0=t0, t1=t1, tend=tend, dt0=dt, dt1=dt1, sens=sens)
+            print("wrote", name, t1, dt1, "sensitivity", sens)
+
+
 if __name__ == "__main__":
-    if sys.argv[1:] == ["mhd"]:
+    if sys.argv[1:] == ["space"]:
+        space_orders_main()
+    elif sys.argv[1:] == ["mhd"]:
         mhd_main()
     elif sys.argv[1:] == ["mpp"]:
         mpp_main()

@@ -330,3 +330,53 @@ def test_finsolve_rk_orders_golden(Solver, path):
     assert rel_linf(interior(p, q1), interior(p, g["q1"])) <= TOL_FRAME
     assert abs(t1 - float(g["t1"])) <= 1e-14 * abs(float(g["t1"]))
     assert abs(dtv[1] - float(g["dt1"])) <= 1e-10 * float(g["dt1"])
+
+
+@pytest.mark.parametrize("path", golden_cases("hiorder_constructl"))
+def test_construct_l_space_orders_golden(Solver, path):
+    """ConstructL of the other spatial orders (LLF, JS7/9/11, Z7/9, FD7/9,
+    the generic FP64 face kernel) against the reference's own output."""
+    g = load_golden(path)
+    p = g["p"]
+    with Solver(p) as s:
+        L, smax = s.ConstructL(g["q"])
+    assert rel_linf(interior(p, L), interior(p, g["L"])) <= TOL_STEP
+    assert rel_linf(smax, g["smax"]) <= 1e-14
+
+
+@pytest.mark.parametrize("path", golden_cases("hiorder_finsolverk"))
+def test_finsolve_rk_space_orders_golden(Solver, path):
+    """SSP-RK3 frames of the other spatial orders.  Bar: 1e-11, or ten times
+    the reference's own sensitivity where that is larger.  The sensitivity
+    (stored with each fixture) is how far the reference's frame moves when
+    every value of its initial state moves by one ulp.  The smoothness
+    indicators of orders 9 and 11 cancel terms with coefficients up to
+    ~4e8, so on near-flat states the weights carry roundoff and those
+    frames move by up to ~1e-7 from one ulp of input.  An implementation
+    that is not bit-identical differs by a few times that.  The LLF and FD
+    frames (sensitivity ~1e-15) keep 1e-11."""
+    g = load_golden(path)
+    p = g["p"]
+    with Solver(p) as s:
+        s.set_state(g["q0"], float(g["t0"]))
+        dtv, n = s.FinSolveRK(float(g["tend"]), [0.0, float(g["dt0"]), p.max_dt])
+        q1, t1 = s.get_state()
+    tol = max(TOL_FRAME, 10.0 * float(g["sens"]))
+    assert n > 0
+    assert rel_linf(interior(p, q1), interior(p, g["q1"])) <= tol
+    assert abs(t1 - float(g["t1"])) <= 1e-14 * abs(float(g["t1"]))
+    assert abs(dtv[1] - float(g["dt1"])) <= max(1e-10, tol) * float(g["dt1"])
+
+
+@pytest.mark.parametrize("so,weno", [(3, FIN_WENO_JS), (11, FIN_WENO_Z), (11, FIN_WENO_FD), (13, FIN_WENO_JS)])
+def test_unbuilt_space_orders_are_refused(Solver, so, weno):
+    """GetWenoReconstruct (lib/WenoReconstruct.cpp:40-71) throws for these."""
+    p = P.riemann_params(n=16, weno=weno, space_order=so, mbc=7)
+    with pytest.raises(Exception, match="not implemented"):
+        Solver(p)
+
+
+def test_space_order_needs_mbc(Solver):
+    p = P.riemann_params(n=16, weno=FIN_WENO_JS, space_order=9, mbc=4)
+    with pytest.raises(Exception, match="mbc"):
+        Solver(p)

@@ -139,3 +139,24 @@ def test_reference_reproduces_rk_orders_golden(reflib, path):
     assert rc == 0
     assert np.array_equal(interior(p, q1), interior(p, g["q1"]))
     assert t1 == float(g["t1"]) and dt1 == float(g["dt1"])
+
+
+@pytest.mark.parametrize("path", golden_cases("hiorder_constructl"))
+def test_reference_reproduces_space_order_constructl(reflib, path):
+    """ConstructL of the other spatial orders (LLF, JS7/9/11, Z7/9, FD7/9):
+    the fixtures are the reference's own output."""
+    g = load_golden(path)
+    p, q = g["p"], g["q"]
+    L, smax = reflib.construct_l(p, q)
+    assert np.array_equal(interior(p, L), interior(p, g["L"]))
+    assert np.array_equal(smax, g["smax"])
+
+
+@pytest.mark.parametrize("path", golden_cases("hiorder_finsolverk"))
+def test_reference_reproduces_space_order_frames(reflib, path):
+    g = load_golden(path)
+    p = g["p"]
+    rc, q1, t1, dt1 = reflib.finsolve(p, g["q0"], float(g["t0"]), float(g["tend"]), float(g["dt0"]))
+    assert rc == 0
+    assert np.array_equal(interior(p, q1), interior(p, g["q1"]))
+    assert t1 == float(g["t1"]) and dt1 == float(g["dt1"])
