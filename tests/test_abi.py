@@ -66,3 +66,30 @@ def test_mhd_create_validates_without_gpu(lib):
     bad = P.orszag_tang_params(n=16, mbc=3)
     assert lib.fin_mhd_create(C.byref(bad), C.byref(h)) == 1
     assert b"mbc" in lib.fin_mhd_last_error()
+
+
+def test_space_order_validation_without_gpu(lib):
+    """The (space_order, weno_version) pairs GetWenoReconstruct
+    (lib/WenoReconstruct.cpp:40-71) throws for are refused with its message;
+    the others need mbc >= (order + 1) / 2 and FP64 Runge-Kutta stepping."""
+    from finess_b200 import problems as P
+    from finess_b200._abi import FIN_PREC_FP32, FIN_TS_LXW, FIN_TS_MD, FIN_WENO_FD, FIN_WENO_JS, FIN_WENO_Z
+    h = C.c_void_p()
+    for so, w in ((3, FIN_WENO_JS), (11, FIN_WENO_Z), (11, FIN_WENO_FD), (13, FIN_WENO_JS), (0, FIN_WENO_Z)):
+        bad = P.riemann_params(n=16, weno=w, space_order=so, mbc=7)
+        assert lib.fin_create(C.byref(bad), C.byref(h)) != 0 and not h.value
+        assert b"Requested WENO Reconstruction not implemented." in lib.fin_last_error()
+    bad = P.riemann_params(n=16, weno=FIN_WENO_JS, space_order=11, mbc=5)
+    assert lib.fin_create(C.byref(bad), C.byref(h)) != 0
+    assert b"mbc must be >= (space_order + 1) / 2" in lib.fin_last_error()
+    for kw in ({"precision": FIN_PREC_FP32}, {"time_stepping_method": FIN_TS_LXW, "time_order": 3},
+               {"time_stepping_method": FIN_TS_MD, "time_order": 4}):
+        bad = P.riemann_params(n=16, weno=FIN_WENO_Z, space_order=7, mbc=5, **kw)
+        assert lib.fin_create(C.byref(bad), C.byref(h)) != 0
+        assert b"space orders other than 5" in lib.fin_last_error()
+    # an accepted pair gets past validation (without a GPU it stops at the device)
+    ok = P.riemann_params(n=16, weno=FIN_WENO_FD, space_order=9, mbc=5)
+    if lib.fin_create(C.byref(ok), C.byref(h)) == 0:
+        lib.fin_destroy(h)
+    else:
+        assert b"Requested WENO" not in lib.fin_last_error() and b"space order" not in lib.fin_last_error()
