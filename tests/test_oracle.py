@@ -160,3 +160,18 @@ def test_reference_reproduces_space_order_frames(reflib, path):
     assert rc == 0
     assert np.array_equal(interior(p, q1), interior(p, g["q1"]))
     assert t1 == float(g["t1"]) and dt1 == float(g["dt1"])
+
+
+@pytest.mark.parametrize("path", golden_cases("hiorder_finsolverk"))
+def test_space_order_frame_bar_is_tight(path):
+    """The GPU bar of these frames is max(1e-11, 10 x the reference's one-ulp
+    sensitivity).  The linear (LLF, FD) frames must keep 1e-11; the WENO
+    frames of orders 7-11 may loosen only as far as the reference itself
+    moves (at most ~1e-7, JS11 on the Riemann problem)."""
+    g = load_golden(path)
+    sens = float(g["sens"])
+    assert 0.0 <= sens < 2e-7
+    name = path.split("/")[-1]
+    if "_fd_" in name or "finsolverk1_" in name:
+        assert 10.0 * sens < 1e-11
+    assert np.isfinite(interior(g["p"], g["q1"])).all()
