@@ -1,5 +1,5 @@
-// The other spatial orders of ConstructL (space_order 1, 7, 9, 11; 5 as a
-// cross-check of the fused kernel): one thread per face gathers the 2r-point
+// The other spatial orders of ConstructL (space_order 1, 7, 9, 11; order 5
+// is the fused stage kernel's): one thread per face gathers the 2r-point
 // stencil (r = (space_order+1)/2, ConstructL.cpp:31-33, 94-113), forms the
 // characteristic split values and reconstructs them with the reference's
 // WENO of that order (lib/WenoReconstruct.cpp:151-375, 440-575, 618-690), the
@@ -177,11 +177,9 @@ __device__ __forceinline__ double recon11(const double* u, double eps, double pw
 template <int ORDER, int VER>
 __device__ __forceinline__ double recon(const double* u, double eps, double pw)
 {
+    static_assert(ORDER == 1 || ORDER == 7 || ORDER == 9 || ORDER == 11, "orders 1, 7, 9, 11");
     if constexpr (ORDER == 1) return u[0];   // WenoReconstructLLF, :686-695
-    else if constexpr (ORDER == 5) {
-        return VER == FIN_WENO_FD ? weno5<double, FIN_WENO_FD, true>(u, eps, pw)
-                                  : (pw == 2.0 ? weno5<double, VER, true>(u, eps, pw) : weno5<double, VER, false>(u, eps, pw));
-    } else if constexpr (ORDER == 7) return recon7<VER>(u, eps, pw);
+    else if constexpr (ORDER == 7) return recon7<VER>(u, eps, pw);
     else if constexpr (ORDER == 9) return recon9<VER>(u, eps, pw);
     else return recon11(u, eps, pw);
 }
