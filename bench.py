@@ -359,24 +359,9 @@ def main():
     ws, rank, local = dist_env()
     import torch
     torch.cuda.set_device(local)
-    if ws > 1:
-        import datetime
-        import torch.distributed as dist
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
-
-    def barrier():
-        if ws > 1:
-            import torch.distributed as dist
-            dist.barrier()
-        torch.cuda.synchronize()
-
-    def max_over_ranks(v):
-        if ws == 1:
-            return v
-        import torch.distributed as dist
-        t = torch.tensor([v], device="cuda", dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
+    from finess_b200 import replicas
+    from finess_b200.replicas import barrier, max_over_ranks
+    replicas.init(ws, backend="nccl", timeout_s=120)
 
     from finess_b200 import problems as P
     from finess_b200.solver import fma_peak_tflops
@@ -518,9 +503,7 @@ def main():
             "clocks": clocks, "gpu_launches": launches,
         }
         print(json.dumps(line), flush=True)
-    if ws > 1:
-        import torch.distributed as dist
-        dist.destroy_process_group()
+    replicas.finish()
 
 
 if __name__ == "__main__":
