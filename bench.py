@@ -9,6 +9,7 @@ L2, so no L2 flush is needed between steps.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--forms fp64,fp32,hybrid]
     python bench.py --space-orders [--n N] [--steps K]    # LLF, WENO7/9/11 beside WENO5 (FP64)
+    python bench.py --mpp [--n N] [--steps K]             # Lax-Wendroff with / without the MPP limiter
 
 The headline form is the hybrid (FP32 bulk + troubled-face network run every
 HYB_EVERY accepted steps, judge step every HYB_JUDGE_EVERY steps) when trained
@@ -332,6 +333,37 @@ def run_space_orders(args):
         print(json.dumps(line), flush=True)
 
 
+def run_mpp(args):
+    """Lax-Wendroff (time_order 3, mbc 5, WENO5-Z, FP64) with and without the
+    MPP positivity limiter on the four-quadrant Riemann problem at 2048^2 and
+    4096^2: device time per step through fin_advance (CUDA events), one JSON
+    line per case."""
+    ws, rank, _ = dist_env()
+    if rank != 0:
+        return
+    from finess_b200 import problems as P
+    from finess_b200._abi import FIN_TS_LXW, FIN_TS_MD, FIN_WENO_Z
+    from finess_b200.batch import first_dt as batch_first_dt
+    from finess_b200.solver import Solver
+    for n in ((args.n,) if args.n != N_CELLS else (2048, 4096)):
+        for mpp in (0, 1):
+            p = P.riemann_params(n=n, weno=FIN_WENO_Z, method=FIN_TS_MD, time_stepping_method=FIN_TS_LXW,
+                                 time_order=3, mpp_limiter=mpp)
+            q0 = P.riemann_init(p)
+            dt0 = batch_first_dt(p, q0)
+            with Solver(p) as s:
+                s.set_state(q0)
+                s.advance(1.0, np.array([0.0, dt0, p.max_dt]), args.warmup)
+                _, k = s.advance(1.0, np.array([0.0, dt0, p.max_dt]), args.steps)
+                ms = s.last_kernel_ms()
+            print(json.dumps({"metric": "2D Euler Lax-Wendroff cell-updates/s" + (" with the MPP limiter" if mpp else ""),
+                              "value": n * n * k / (ms * 1e-3), "unit": UNIT, "n_gpus": 1, "steps": k,
+                              "warmup": args.warmup, "ms_per_step": ms / k, "higher_is_better": True,
+                              "dtype": "f64", "data": "synthetic",
+                              "config": {"workload": "euler2d_riemann4q_wenoz_lxw", "grid": f"{n}x{n}",
+                                         "mpp_limiter": mpp, "mbc": 5}}), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -345,8 +377,15 @@ def main():
     ap.add_argument("--no-accuracy", action="store_true")
     ap.add_argument("--space-orders", action="store_true",
                     help="time the other spatial orders (LLF, WENO7/9/11) instead of the headline workload")
+    ap.add_argument("--mpp", action="store_true",
+                    help="time Lax-Wendroff with and without the MPP limiter instead of the headline workload")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
+    if args.mpp:
+        if args.steps == 50:
+            args.steps = 20
+        run_mpp(args)
+        return
     if args.space_orders:
         if args.steps == 50:
             args.steps = 10
