@@ -69,11 +69,15 @@ __global__ void k_na_planes_to_aos(const double* planes, double* aos, int mx, in
     }
 }
 
-// GlobalWaveSpd (lib/2d/GlobalWaveSpd.cpp:52-78): block max, one atomic per block.
-__global__ void k_na_wave_spd_max(const double* q, int mx, int my, size_t plane, double gamma, double* alpha_out)
+// GlobalWaveSpd (lib/2d/GlobalWaveSpd.cpp:52-78): block max, one atomic per
+// block; a non-finite speed sets bit 0 of the status word, as in the main
+// library's k_wave_spd_max.
+__global__ void k_na_wave_spd_max(const double* q, int mx, int my, size_t plane, double gamma, double* alpha_out,
+                                  unsigned int* status)
 {
     __shared__ double red[2][32];
     double ax = 0.0, ay = 0.0;
+    bool nonfinite = false;
     const size_t n = size_t(mx) * my;
     for (size_t g = blockIdx.x * size_t(blockDim.x) + threadIdx.x; g < n; g += size_t(gridDim.x) * blockDim.x) {
         double Q[MEQN];
@@ -82,9 +86,11 @@ __global__ void k_na_wave_spd_max(const double* q, int mx, int my, size_t plane,
         const double Qy[MEQN] = {Q[0], Q[2], Q[1], Q[3], Q[4]};
         const double sx = Euler::cell_speed(Euler::cell(gamma, Q));
         const double sy = Euler::cell_speed(Euler::cell(gamma, Qy));
+        if (!(sx <= 1e300) || !(sy <= 1e300)) nonfinite = true;
         if (sx <= 1e300) ax = Max(ax, sx);
         if (sy <= 1e300) ay = Max(ay, sy);
     }
+    if (nonfinite) atomicOr(status, 1u);
     for (int o = 16; o > 0; o >>= 1) {
         ax = Max(ax, __shfl_xor_sync(0xffffffffu, ax, o));
         ay = Max(ay, __shfl_xor_sync(0xffffffffu, ay, o));
@@ -139,7 +145,8 @@ void na_launch_stage(const StageArgs& a, cudaStream_t st)
 
 }  // namespace
 
-extern "C" int fin_construct_l_noalloc(const fin_params* p, const double* q_dev, double* L_dev, void* stream)
+extern "C" int fin_construct_l_noalloc(const fin_params* p, const double* q_dev, double* L_dev, void* stream,
+                                       int check)
 {
     if (!p || !q_dev || !L_dev) return FIN_ERR_ARG;
     if (p->physics != FIN_PHYS_EULER || p->meqn != 5 || p->space_order != 5) return FIN_ERR_UNSUPPORTED;
@@ -158,6 +165,9 @@ extern "C" int fin_construct_l_noalloc(const fin_params* p, const double* q_dev,
     const size_t n = size_t(p->mx) * size_t(p->my);
     if (n > NA_MAX_CELLS) return FIN_ERR_SIZE;
 
+    // An error left pending by the caller's earlier CUDA work stays where it
+    // is (peeked, not cleared) and this call launches nothing.
+    if (cudaPeekAtLastError() != cudaSuccess) return FIN_ERR_CUDA;
     double* scratch = nullptr;
     int rc = na_setup(&scratch);
     if (rc) return rc;
@@ -171,9 +181,13 @@ extern "C" int fin_construct_l_noalloc(const fin_params* p, const double* q_dev,
     if (cudaMemsetAsync(slots, 0, NA_SLOTS * sizeof(double), st) != cudaSuccess) return FIN_ERR_CUDA;
     int blocks = int((n + 255) / 256);
     if (blocks > 148 * 16) blocks = 148 * 16;
+    unsigned int* status = reinterpret_cast<unsigned int*>(slots + 4);
     k_na_aos_to_planes<<<blocks, 256, 0, st>>>(q_dev, in_planes, p->mx, p->my, p->mbc, plane);
-    if (p->global_alpha)
-        k_na_wave_spd_max<<<blocks, 256, 0, st>>>(in_planes, p->mx, p->my, plane, p->gamma, slots);
+    if (cudaGetLastError() != cudaSuccess) return FIN_ERR_CUDA;
+    if (p->global_alpha) {
+        k_na_wave_spd_max<<<blocks, 256, 0, st>>>(in_planes, p->mx, p->my, plane, p->gamma, slots, status);
+        if (cudaGetLastError() != cudaSuccess) return FIN_ERR_CUDA;
+    }
 
     StageArgs a;
     memset(&a, 0, sizeof(a));
@@ -194,7 +208,7 @@ extern "C" int fin_construct_l_noalloc(const fin_params* p, const double* q_dev,
     a.pw_f = float(a.pw);
     a.alpha_scaling_f = float(a.alpha_scaling);
     a.alpha_in = p->global_alpha ? slots : nullptr;
-    a.status = reinterpret_cast<unsigned int*>(slots + 4);
+    a.status = status;
     a.bc[0] = p->bc_xlow; a.bc[1] = p->bc_xhigh; a.bc[2] = p->bc_ylow; a.bc[3] = p->bc_yhigh;
     const bool p2 = p->power_param == 2.0;
     if (p->weno_version == FIN_WENO_JS) {
@@ -204,6 +218,16 @@ extern "C" int fin_construct_l_noalloc(const fin_params* p, const double* q_dev,
     } else {
         na_launch_stage<FIN_WENO_FD, true>(a, st);
     }
+    if (cudaGetLastError() != cudaSuccess) return FIN_ERR_CUDA;
     k_na_planes_to_aos<<<blocks, 256, 0, st>>>(out_planes, L_dev, p->mx, p->my, p->mbc, plane);
-    return cudaGetLastError() == cudaSuccess ? FIN_OK : FIN_ERR_CUDA;
+    if (cudaGetLastError() != cudaSuccess) return FIN_ERR_CUDA;
+    if (!check) return FIN_OK;
+    // The caller asked for the status: wait for the stream and read the
+    // status word (a 4-byte copy into this stack variable; the driver stages
+    // it, nothing is allocated).
+    unsigned int hst = 0;
+    if (cudaMemcpyAsync(&hst, status, sizeof(hst), cudaMemcpyDeviceToHost, st) != cudaSuccess) return FIN_ERR_CUDA;
+    if (cudaStreamSynchronize(st) != cudaSuccess) return FIN_ERR_CUDA;
+    if (hst & 1u) return FIN_ERR_NONFINITE;
+    return FIN_OK;
 }

@@ -6,16 +6,14 @@ frame's steps run while the previous frame is formatted and written); with
 --sync each frame waits for its files, as the reference's loop does.
 
     python -m finess_b200.frames --problem riemann --n 4096 --nout 4 --tfinal 0.02 --outdir /tmp/out [--sync]
-        [--precision fp64|fp32|hybrid] [--ref-output]
+        [--precision fp64|fp32|hybrid]
 
---ref-output also times the reference's own Output (lib/2d/Output.cpp,
-oracle/_ref/libfinref_io.so, where it was built) on the last frame's state,
-on the host, for comparison.
+run_frames returns the last frame's state (``q_last``, ``t_last``) beside the
+figures, so a checker can write the same frame with another implementation.
 """
 import argparse
 import json
 import os
-import sys
 import time
 
 import numpy as np
@@ -41,8 +39,7 @@ def problem(name, n):
     raise ValueError(name)
 
 
-def run_frames(name="riemann", n=4096, nout=4, tfinal=0.02, outdir="output", precision="fp64", sync=False,
-               ref_output=False):
+def run_frames(name="riemann", n=4096, nout=4, tfinal=0.02, outdir="output", precision="fp64", sync=False):
     p, q0 = problem(name, n)
     p.precision = PRECISIONS[precision]
     p.nout, p.tfinal = nout, tfinal
@@ -79,18 +76,7 @@ def run_frames(name="riemann", n=4096, nout=4, tfinal=0.02, outdir="output", pre
     out.update({"steps": steps, "wall_s": wall, "device_s": device_ms * 1e-3, "output_wait_s": wait_s,
                 "frames_written": nout + 1, "frame_file_bytes": frame_bytes,
                 "cell_updates_per_s_wall": float(p.mx) * p.my * steps / wall})
-    if ref_output:
-        sys.path.insert(0, os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "oracle"))
-        from oracle import IoRefLib
-        if IoRefLib.available():
-            refdir = os.path.join(outdir, "reference")
-            os.makedirs(refdir, exist_ok=True)
-            w = time.perf_counter()
-            IoRefLib().output(p, refdir, q_last, t_last, nout)
-            out["reference_output_s"] = time.perf_counter() - w
-            with open(os.path.join(outdir, "q%04d.dat" % nout), "rb") as a, \
-                    open(os.path.join(refdir, "q%04d.dat" % nout), "rb") as b:
-                out["reference_frame_identical"] = a.read() == b.read()
+    out["q_last"], out["t_last"] = q_last, t_last
     return out
 
 
@@ -103,9 +89,10 @@ def main():
     ap.add_argument("--outdir", default="output")
     ap.add_argument("--precision", default="fp64", choices=sorted(PRECISIONS))
     ap.add_argument("--sync", action="store_true", help="wait for each frame's files before the next frame")
-    ap.add_argument("--ref-output", action="store_true", help="also time the reference's Output on the last frame")
     a = ap.parse_args()
-    print(json.dumps(run_frames(a.problem, a.n, a.nout, a.tfinal, a.outdir, a.precision, a.sync, a.ref_output)))
+    out = run_frames(a.problem, a.n, a.nout, a.tfinal, a.outdir, a.precision, a.sync)
+    out.pop("q_last")
+    print(json.dumps(out))
 
 
 if __name__ == "__main__":

@@ -3,9 +3,10 @@
  * 2D finite-difference WENO right-hand side and time steppers.
  *
  * Every entry point is extern "C", takes plain pointers and sizes, returns an
- * int status (FIN_OK == 0) and never exits the process.  The C++ relink shim
- * (finess_b200/csrc/shim/finess_relink.cpp) maps these statuses back onto the
- * reference's own conventions (printf + exit(1), std::logic_error).
+ * int status (FIN_OK == 0) and never exits the process.  The C++ relink shims
+ * (finess_b200/csrc/shim/*.cpp, one file per reference symbol) map these
+ * statuses back onto the reference's own conventions (printf + exit(1),
+ * std::logic_error).
  *
  * Array layout at this boundary is the reference's own dTensorBC3 layout
  * (lib/tensors.h:267-273, lib/tensors.cpp:650-667): a ghosted array
@@ -335,9 +336,15 @@ const char* fin_batch_last_error(void);
  *     stream capture.
  *   - Calls share the one array: calls that overlap on the GPU (other
  *     streams, other threads) race; serialise them.
+ *   - check == 0: the call returns once its kernels are enqueued, and a
+ *     non-finite wave speed or state goes unreported.  check != 0: the call
+ *     waits for `stream` and returns FIN_ERR_NONFINITE when the stage met a
+ *     non-finite speed (what fin_construct_l reports).
+ *   - An error already pending from the caller's own CUDA work is left in
+ *     place and the call returns FIN_ERR_CUDA without launching anything.
  *   - Errors are reported by the return code only (fin_last_error does not
- *     describe them); non-finite speeds are not reported. */
-int fin_construct_l_noalloc(const fin_params* p, const double* q_dev, double* L_dev, void* stream);
+ *     describe them). */
+int fin_construct_l_noalloc(const fin_params* p, const double* q_dev, double* L_dev, void* stream, int check);
 
 /* ---- ideal MHD (physics FIN_PHYS_MHD) ---------------------------------- */
 /* The reference's apps/2d/mhd application path: lib/2d's ConstructL with the

@@ -237,7 +237,9 @@ class RefLib:
         lib.ref_construct_integrated_r.argtypes = [C.c_double, _dp, _dp, _dp]
         lib.ref_finsolve.argtypes = [C.c_int, _dp, C.POINTER(C.c_double), C.c_double, _dp]
         lib.ref_finsolve.restype = C.c_int
+        lib.ref_last_steps.restype = C.c_longlong
         self.lib = lib
+        self.last_steps = None
 
     def setup(self, p):
         self.lib.ref_setup(C.byref(p))
@@ -276,6 +278,7 @@ class RefLib:
         tt = C.c_double(t)
         dtv = np.array([0.0, dt, p.max_dt])
         rc = self.lib.ref_finsolve(p.time_stepping_method, q, C.byref(tt), tend, dtv)
+        self.last_steps = int(self.lib.ref_last_steps())   # accepted steps of this run
         return rc, q, tt.value, dtv[1]
 
 

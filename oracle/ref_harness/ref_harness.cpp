@@ -80,7 +80,11 @@ void BeforeFullTimeStep(double, StateVars&, StateVars&) {}
 void AfterFullTimeStep(double, StateVars&, StateVars&) {}
 void BeforeStep(double, StateVars&) {}
 void AfterStep(double, StateVars&) {}
-void ConSoln(const StateVars&) {}
+// FinSolveRK / FinSolveMD / FinSolveLxW call ConSoln once per accepted step
+// (FinSolveRK.cpp:362): the harness counts the calls instead of writing
+// conservation.dat, which gives the number of accepted steps of a run.
+static long long g_accepted_steps = 0;
+void ConSoln(const StateVars&) { ++g_accepted_steps; }
 
 // ---- helpers -------------------------------------------------------------
 static void load(dTensorBC3& t, const double* src)
@@ -180,6 +184,7 @@ int ref_finsolve(int method, double* q, double* t, double tend, double* dtv)
 {
     StateVars* Q = make_state(q, *t);
     int rc = 0;
+    g_accepted_steps = 0;
     try {
         if (method == FIN_TS_RK) FinSolveRK(*Q, tend, dtv);
         else if (method == FIN_TS_MD) FinSolveMD(*Q, tend, dtv);
@@ -191,6 +196,9 @@ int ref_finsolve(int method, double* q, double* t, double tend, double* dtv)
     delete Q;
     return rc;
 }
+
+// Accepted steps of the last ref_finsolve call.
+long long ref_last_steps(void) { return g_accepted_steps; }
 
 // Jacobian and Hessian of the application's flux at one state (DFluxFunc,
 // D2FluxFunc): A[(d*5+m)*5+k], H[((d*5+m)*5+k1)*5+k2], d = 0 (f) or 1 (g).

@@ -57,6 +57,18 @@ def test_oracle_live_vs_reference(oracle, reflib):
         assert np.array_equal(s1, s2)
 
 
+def test_reference_step_count_matches_oracle(oracle, reflib):
+    """The harness counts the reference's accepted steps (one ConSoln call
+    each, FinSolveRK.cpp:362); a whole adaptive frame gives the oracle's count."""
+    p = P.riemann_params(n=24, weno=FIN_WENO_Z)
+    q = oracle.set_bnd(p, P.riemann_init(p))
+    rc, q1, t1, dt1, n = oracle.finsolve(p, q, 0.0, 0.05, 1e-3)
+    rr, qr, tr, dtr = reflib.finsolve(p, q, 0.0, 0.05, 1e-3)
+    assert rc == 0 and rr == 0
+    assert n > 5 and reflib.last_steps == n
+    assert np.array_equal(interior(p, q1), interior(p, qr))
+
+
 def test_conservation_periodic(oracle):
     """Periodic runs keep sum(q dx dy) to round-off (flux form telescopes)."""
     p = P.vortex_params(n=24)
