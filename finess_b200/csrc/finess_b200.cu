@@ -128,6 +128,7 @@ struct fin_solver {
     double* mpp_fy;                 // [m][mx][my+1]
     double* mpp_amin;               // [4][mx][my]
     int timed_stages;               // stage launches timed in the current step (at most 3)
+    double* d_upd;                  // fin_update_soln(5)'s four ghosted arrays (made on first use)
 };
 
 // ---------------------------------------------------------------------------
@@ -152,6 +153,60 @@ __global__ void k_face_samples(const double* q, size_t plane, int mx, int my, in
         for (int k = 0; k < ind::NFEAT; k++) X[s * ind::NFEAT + k] = x[k];
         const double ag = alpha_g ? alpha_g[isx ? 0 : 1] : 0.0;
         y[s] = ind::face_label(q, plane, mx, my, bc, gamma, eps, pw, ascale, ag, isx, i, j);
+    }
+}
+
+// UpdateSoln.cpp:29-35 element by element: ((a1 q*) + (a2 q)) + (b L) with
+// b = beta*dt, every product and sum rounded on its own (no contraction).
+__global__ void k_update_soln(const double* qstar, const double* L, double* qnew, size_t n, double a1, double a2,
+                              double b)
+{
+    for (size_t k = blockIdx.x * size_t(blockDim.x) + threadIdx.x; k < n; k += size_t(gridDim.x) * blockDim.x)
+        qnew[k] = __dadd_rn(__dadd_rn(__dmul_rn(a1, qstar[k]), __dmul_rn(a2, qnew[k])), __dmul_rn(b, L[k]));
+}
+
+// UpdateSoln.cpp:43-80 (the fifth-order stepper's form) element by element:
+// q2 = q2 + delta q1, then q1 = ((g1 q1 + g2 q2) + g3 qold) + b L with
+// b = beta*dt, every operation rounded on its own.
+__global__ void k_update_soln5(const double* qold, const double* L, double* q1, double* q2, size_t n, double g1,
+                               double g2, double g3, double delta, double b)
+{
+    for (size_t k = blockIdx.x * size_t(blockDim.x) + threadIdx.x; k < n; k += size_t(gridDim.x) * blockDim.x) {
+        const double s1 = q1[k];
+        const double s2 = __dadd_rn(q2[k], __dmul_rn(delta, s1));
+        q2[k] = s2;
+        const double s3 = qold[k];
+        q1[k] = __dadd_rn(__dadd_rn(__dadd_rn(__dmul_rn(g1, s1), __dmul_rn(g2, s2)), __dmul_rn(g3, s3)),
+                          __dmul_rn(b, L[k]));
+    }
+}
+
+// GetCFL.cpp:54-59's maxima: smax(i, j, 1) and smax(i, j, 2) over i <= mx,
+// j <= my of a ghosted (mx+1, my+1, 2) array; NaN entries skipped.
+__global__ void k_smax_max(const double* smax, int mx, int my, int mbc, double* out)
+{
+    __shared__ double red[2][32];
+    double a = 0.0, b = 0.0;
+    const size_t n = size_t(mx) * my;
+    const int sy = my + 1 + 2 * mbc;
+    for (size_t g = blockIdx.x * size_t(blockDim.x) + threadIdx.x; g < n; g += size_t(gridDim.x) * blockDim.x) {
+        const int i = int(g / my), j = int(g - size_t(i) * my);
+        const size_t e = (size_t(i + mbc) * sy + (j + mbc)) * 2;
+        const double v1 = smax[e], v2 = smax[e + 1];
+        if (v1 == v1) a = v1 > a ? v1 : a;
+        if (v2 == v2) b = v2 > b ? v2 : b;
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+        a = Max(a, __shfl_xor_sync(0xffffffffu, a, o));
+        b = Max(b, __shfl_xor_sync(0xffffffffu, b, o));
+    }
+    const int w = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    if ((threadIdx.x & 31) == 0) { red[0][w] = a; red[1][w] = b; }
+    __syncthreads();
+    if (threadIdx.x < 2) {
+        double v = 0.0;
+        for (int k = 0; k < nw; k++) v = Max(v, red[threadIdx.x][k]);
+        atomic_max_nonneg(out + threadIdx.x, v);
     }
 }
 
@@ -1164,6 +1219,7 @@ int fin_destroy(fin_solver* s)
     cudaFree(s->Gg);
     cudaFree(s->d_face_x);
     cudaFree(s->d_face_y);
+    cudaFree(s->d_upd);
     if (s->h_slots) cudaFreeHost(s->h_slots);
     if (s->ev0) cudaEventDestroy(s->ev0);
     if (s->ev1) cudaEventDestroy(s->ev1);
@@ -1241,6 +1297,8 @@ int fin_global_wave_spd(fin_solver* s, const double* q_host, double* alpha1, dou
     return check_status(s);
 }
 
+static int download_l_smax(fin_solver* s, int outb, double* L_host, double* smax_host);
+
 int fin_construct_l(fin_solver* s, const double* q_host, double* L_host, double* smax_host)
 {
     if (!s || !q_host || !L_host) return set_err(FIN_ERR_ARG, "null argument");
@@ -1261,8 +1319,15 @@ int fin_construct_l(fin_solver* s, const double* q_host, double* L_host, double*
     a.face_alpha_x = smax_host ? s->d_face_x : nullptr;
     a.face_alpha_y = smax_host ? s->d_face_y : nullptr;
     if ((rc = launch_stage(s, a))) return rc;
-    // L: interior of the ghosted output, ghosts untouched (the reference
-    // leaves Lstar's ghost entries uninitialised).
+    return download_l_smax(s, outb, L_host, smax_host);
+}
+
+// L (interior of the ghosted output, ghosts untouched: the reference leaves
+// Lstar's ghost entries uninitialised) from q[outb], and smax max-accumulated
+// from the per-face speeds, then the status word.
+static int download_l_smax(fin_solver* s, int outb, double* L_host, double* smax_host)
+{
+    const fin_params& p = s->p;
     const size_t n = size_t(p.mx) * p.my;
     std::vector<double> hl(MEQN * n);
     for (int m = 0; m < MEQN; m++)
@@ -1371,6 +1436,8 @@ int fin_face_samples(fin_solver* s, long long offset, long long stride, long lon
     return FIN_OK;
 }
 
+static int download_fg(fin_solver* s, double* F_host, double* G_host);
+
 // ConstructIntegratedR, 1-state (lib/2d/ConstructIntegratedR.cpp:59-296).
 int fin_construct_integrated_r(fin_solver* s, double dt, const double* q_host, double* F_host, double* G_host)
 {
@@ -1381,6 +1448,13 @@ int fin_construct_integrated_r(fin_solver* s, double dt, const double* q_host, d
     int rc = upload(s, q_host, buf);
     if (rc) return rc;
     if ((rc = launch_intflux(s, p.time_order > 2 ? 1 : 0, s->q[buf], nullptr, dt, 0, 0, 0, 0))) return rc;
+    return download_fg(s, F_host, G_host);
+}
+
+// s->Fg, s->Gg -> the interior and 3-cell ghost frame of ghosted host arrays.
+static int download_fg(fin_solver* s, double* F_host, double* G_host)
+{
+    const fin_params& p = s->p;
     std::vector<double> hf(MEQN * s->gplane), hg(MEQN * s->gplane);
     CK(cudaMemcpyAsync(hf.data(), s->Fg, hf.size() * sizeof(double), cudaMemcpyDeviceToHost, s->stream));
     CK(cudaMemcpyAsync(hg.data(), s->Gg, hg.size() * sizeof(double), cudaMemcpyDeviceToHost, s->stream));
@@ -1394,6 +1468,213 @@ int fin_construct_integrated_r(fin_solver* s, double dt, const double* q_host, d
                 F_host[dst] = hf[src];
                 G_host[dst] = hg[src];
             }
+    return FIN_OK;
+}
+
+// The 2-state and three-coefficient forms (ConstructIntegratedR.cpp:525-606,
+// 608-700): q1 into the first scratch buffer, q2 into the second.
+static int construct_integrated_r_two(fin_solver* s, int mode, double dt, double a1, double b1, double c1,
+                                      const double* q1_host, double a2, double b2, double c2,
+                                      const double* q2_host, double* F_host, double* G_host)
+{
+    if (!s || !q1_host || !q2_host || !F_host || !G_host) return set_err(FIN_ERR_ARG, "null argument");
+    if (!s->Fg) return set_err(FIN_ERR_ARG, "the solver was created for Runge-Kutta stepping (no F, G buffers)");
+    const int b1f = (s->cur + 3) % 4, b2f = (s->cur + 2) % 4;
+    int rc = upload(s, q1_host, b1f);
+    if (rc) return rc;
+    if ((rc = upload(s, q2_host, b2f))) return rc;
+    if ((rc = launch_intflux(s, mode, s->q[b1f], s->q[b2f], dt, a1, b1, a2, b2, c1, c2))) return rc;
+    return download_fg(s, F_host, G_host);
+}
+
+int fin_construct_integrated_r2(fin_solver* s, double dt, double alpha1, double beta1, const double* q1_host,
+                                double alpha2, double beta2, const double* q2_host, double* F_host, double* G_host)
+{
+    return construct_integrated_r_two(s, 2, dt, alpha1, beta1, 0.0, q1_host, alpha2, beta2, 0.0, q2_host, F_host,
+                                      G_host);
+}
+
+int fin_construct_integrated_r3(fin_solver* s, double dt, double alpha1, double beta1, double charlie1,
+                                const double* q1_host, double alpha2, double beta2, double charlie2,
+                                const double* q2_host, double* F_host, double* G_host)
+{
+    return construct_integrated_r_two(s, 3, dt, alpha1, beta1, charlie1, q1_host, alpha2, beta2, charlie2, q2_host,
+                                      F_host, G_host);
+}
+
+// ConstructLxWL (lib/2d/ConstructLxWL.cpp:30-414): the stage kernel in its
+// F, G mode (the sampled time-integrated fluxes split in place of FluxFunc of
+// q, ConstructLxWL.cpp:150-155) with no update (L alone), the per-face speeds
+// for smax, and, when asked, the face fluxes Fhat / Ghat.
+int fin_construct_lxwl(fin_solver* s, const double* q_host, const double* F_host, const double* G_host,
+                       double* L_host, double* smax_host, double* Fhat_host, double* Ghat_host)
+{
+    if (!s || !q_host || !F_host || !G_host || !L_host) return set_err(FIN_ERR_ARG, "null argument");
+    if (!s->Fg) return set_err(FIN_ERR_ARG, "the solver was created for Runge-Kutta stepping (no F, G buffers)");
+    const fin_params& p = s->p;
+    if (p.space_order != 5) return set_err(FIN_ERR_UNSUPPORTED, "ConstructLxWL is built for space_order 5");
+    const int buf = (s->cur + 3) % 4, outb = (s->cur + 2) % 4;
+    int rc = upload(s, q_host, buf);
+    if (rc) return rc;
+    if (p.global_alpha && (rc = compute_alpha(s, buf))) return rc;
+    // F, G: ghosted host layout -> the (mx+6) x (my+6) frame planes
+    {
+        const int sy = p.my + 2 * p.mbc;
+        std::vector<double> hf(MEQN * s->gplane, 0.0), hg(MEQN * s->gplane, 0.0);
+        for (int i = -3; i < p.mx + 3; i++)
+            for (int j = -3; j < p.my + 3; j++)
+                for (int m = 0; m < MEQN; m++) {
+                    const size_t src = (size_t(i + p.mbc) * sy + (j + p.mbc)) * MEQN + m;
+                    const size_t dst = m * s->gplane + size_t(i + 3) * (p.my + 6) + (j + 3);
+                    hf[dst] = F_host[src];
+                    hg[dst] = G_host[src];
+                }
+        CK(cudaMemcpyAsync(s->Fg, hf.data(), hf.size() * sizeof(double), cudaMemcpyHostToDevice, s->stream));
+        CK(cudaMemcpyAsync(s->Gg, hg.data(), hg.size() * sizeof(double), cudaMemcpyHostToDevice, s->stream));
+        CK(cudaStreamSynchronize(s->stream));
+    }
+    const size_t nx = size_t(p.mx + 1) * p.my, ny = size_t(p.mx) * (p.my + 1);
+    if (smax_host) {
+        if (!s->d_face_x) CK(cudaMalloc(&s->d_face_x, nx * sizeof(double)));
+        if (!s->d_face_y) CK(cudaMalloc(&s->d_face_y, ny * sizeof(double)));
+    }
+    const bool fluxes = Fhat_host || Ghat_host;
+    if (fluxes) {
+        if (!s->mpp_fx) CK(cudaMalloc(&s->mpp_fx, MEQN * nx * sizeof(double)));
+        if (!s->mpp_fy) CK(cudaMalloc(&s->mpp_fy, MEQN * ny * sizeof(double)));
+    }
+    StageArgs a = base_args(s);
+    a.Fg = s->Fg; a.Gg = s->Gg; a.gplane = s->gplane;
+    a.qin = s->q[buf];
+    a.A = nullptr; a.B = nullptr; a.qout = s->q[outb];
+    a.a1 = 0.0; a.a2 = 0.0; a.bdt = 1.0;
+    a.alpha_in = p.global_alpha ? alpha_slot(s, buf) : nullptr;
+    a.face_alpha_x = smax_host ? s->d_face_x : nullptr;
+    a.face_alpha_y = smax_host ? s->d_face_y : nullptr;
+    a.flux_x = fluxes ? s->mpp_fx : nullptr;
+    a.flux_y = fluxes ? s->mpp_fy : nullptr;
+    if ((rc = launch_stage(s, a))) return rc;
+    if (fluxes) {
+        std::vector<double> fx(MEQN * nx), fy(MEQN * ny);
+        CK(cudaMemcpyAsync(fx.data(), s->mpp_fx, fx.size() * sizeof(double), cudaMemcpyDeviceToHost, s->stream));
+        CK(cudaMemcpyAsync(fy.data(), s->mpp_fy, fy.size() * sizeof(double), cudaMemcpyDeviceToHost, s->stream));
+        CK(cudaStreamSynchronize(s->stream));
+        // Fhat: dTensorBC3(mx+1, my, meqn, mbc), Ghat: dTensorBC3(mx, my+1, meqn, mbc)
+        // (ConstructLxWL.cpp:63-70); faces 1..mx+1 x 1..my and 1..mx x 1..my+1
+        if (Fhat_host) {
+            const int sy = p.my + 2 * p.mbc;
+            for (int i = 0; i <= p.mx; i++)
+                for (int j = 0; j < p.my; j++)
+                    for (int m = 0; m < MEQN; m++)
+                        Fhat_host[(size_t(i + p.mbc) * sy + (j + p.mbc)) * MEQN + m] =
+                            fx[(size_t(m) * (p.mx + 1) + i) * p.my + j];
+        }
+        if (Ghat_host) {
+            const int sy = p.my + 1 + 2 * p.mbc;
+            for (int i = 0; i < p.mx; i++)
+                for (int j = 0; j <= p.my; j++)
+                    for (int m = 0; m < MEQN; m++)
+                        Ghat_host[(size_t(i + p.mbc) * sy + (j + p.mbc)) * MEQN + m] =
+                            fy[(size_t(m) * p.mx + i) * (p.my + 1) + j];
+        }
+    }
+    return download_l_smax(s, outb, L_host, smax_host);
+}
+
+// UpdateSoln (lib/2d/UpdateSoln.cpp:14-38) on ghosted host arrays: every
+// element, in the reference's order ((alpha1 q* + alpha2 q) + (beta dt) L),
+// each product and sum rounded on its own.
+int fin_update_soln(fin_solver* s, double alpha1, double alpha2, double beta, double dt, const double* qstar_host,
+                    double t_star, const double* L_host, double* qnew_host, double* t_new)
+{
+    if (!s || !qstar_host || !L_host || !qnew_host || !t_new) return set_err(FIN_ERR_ARG, "null argument");
+    const size_t n = s->aos_elems;
+    if (!s->d_upd) CK(cudaMalloc(&s->d_upd, 4 * n * sizeof(double)));
+    double* dqs = s->d_upd;
+    double* dL = s->d_upd + n;
+    double* dqn = s->d_upd + 2 * n;
+    CK(cudaMemcpyAsync(dqs, qstar_host, n * sizeof(double), cudaMemcpyHostToDevice, s->stream));
+    CK(cudaMemcpyAsync(dL, L_host, n * sizeof(double), cudaMemcpyHostToDevice, s->stream));
+    CK(cudaMemcpyAsync(dqn, qnew_host, n * sizeof(double), cudaMemcpyHostToDevice, s->stream));
+    k_update_soln<<<grid_blocks(n), 256, 0, s->stream>>>(dqs, dL, dqn, n, alpha1, alpha2, beta * dt);
+    s->launches++;
+    CK(cudaGetLastError());
+    CK(cudaMemcpyAsync(qnew_host, dqn, n * sizeof(double), cudaMemcpyDeviceToHost, s->stream));
+    CK(cudaStreamSynchronize(s->stream));
+    // UpdateSoln.cpp:27
+    *t_new = alpha1 * t_star + alpha2 * *t_new + beta * dt;
+    return FIN_OK;
+}
+
+// The fifth-order stepper's UpdateSoln (lib/2d/UpdateSoln.cpp:43-80) on
+// ghosted host arrays; the reference leaves the times alone.
+int fin_update_soln5(fin_solver* s, double g1, double g2, double g3, double delta, double beta, double dt,
+                     const double* qold_host, const double* L_host, double* q1_host, double* q2_host)
+{
+    if (!s || !qold_host || !L_host || !q1_host || !q2_host) return set_err(FIN_ERR_ARG, "null argument");
+    const size_t n = s->aos_elems;
+    if (!s->d_upd) CK(cudaMalloc(&s->d_upd, 4 * n * sizeof(double)));
+    double* dqo = s->d_upd;
+    double* dL = s->d_upd + n;
+    double* dq1 = s->d_upd + 2 * n;
+    double* dq2 = s->d_upd + 3 * n;
+    CK(cudaMemcpyAsync(dqo, qold_host, n * sizeof(double), cudaMemcpyHostToDevice, s->stream));
+    CK(cudaMemcpyAsync(dL, L_host, n * sizeof(double), cudaMemcpyHostToDevice, s->stream));
+    CK(cudaMemcpyAsync(dq1, q1_host, n * sizeof(double), cudaMemcpyHostToDevice, s->stream));
+    CK(cudaMemcpyAsync(dq2, q2_host, n * sizeof(double), cudaMemcpyHostToDevice, s->stream));
+    k_update_soln5<<<grid_blocks(n), 256, 0, s->stream>>>(dqo, dL, dq1, dq2, n, g1, g2, g3, delta, beta * dt);
+    s->launches++;
+    CK(cudaGetLastError());
+    CK(cudaMemcpyAsync(q1_host, dq1, n * sizeof(double), cudaMemcpyDeviceToHost, s->stream));
+    CK(cudaMemcpyAsync(q2_host, dq2, n * sizeof(double), cudaMemcpyDeviceToHost, s->stream));
+    CK(cudaStreamSynchronize(s->stream));
+    return FIN_OK;
+}
+
+// GetCFL (lib/2d/GetCFL.cpp:31-73) on a ghosted smax array: the maxima of
+// smax(i,j,1) and smax(i,j,2) over i <= mx, j <= my on the device (NaN
+// entries skipped: the reference's Max(a, b) = a > b ? a : b drops them),
+// then max(dt S1/dx, dt S2/dy), which equals the reference's per-entry
+// maximum because the rounded product and quotient are monotone in S.
+int fin_get_cfl(fin_solver* s, double dt, double dtmax, const double* smax_host, double* cfl)
+{
+    if (!s || !smax_host || !cfl) return set_err(FIN_ERR_ARG, "null argument");
+    if (dt > dtmax) return set_err(FIN_ERR_DT_BOUNDS, "dt is out of bounds");
+    const fin_params& p = s->p;
+    const size_t n = size_t(p.mx + 1 + 2 * p.mbc) * (p.my + 1 + 2 * p.mbc) * 2;
+    int rc = ensure_aos(s);
+    if (rc) return rc;
+    if (n > s->aos_elems) return set_err(FIN_ERR_ARG, "smax larger than the staging buffer");
+    CK(cudaMemcpyAsync(s->d_aos, smax_host, n * sizeof(double), cudaMemcpyHostToDevice, s->stream));
+    CK(cudaMemsetAsync(s->slots + SLOT_SMAX_ALT, 0, 2 * sizeof(double), s->stream));
+    const size_t cells = size_t(p.mx) * p.my;
+    k_smax_max<<<grid_blocks(cells), 256, 0, s->stream>>>(s->d_aos, p.mx, p.my, p.mbc, s->slots + SLOT_SMAX_ALT);
+    s->launches++;
+    CK(cudaGetLastError());
+    double h[2];
+    CK(cudaMemcpyAsync(h, s->slots + SLOT_SMAX_ALT, sizeof(h), cudaMemcpyDeviceToHost, s->stream));
+    CK(cudaStreamSynchronize(s->stream));
+    double c = -100.0;
+    c = Max(dt * h[0] / s->dx, c);
+    c = Max(dt * h[1] / s->dy, c);
+    *cfl = c;
+    if (c > 1.0e8) return set_err(FIN_ERR_CFL_BOUNDS, "CFL number is out of bounds");
+    return FIN_OK;
+}
+
+// GetCFL from the global wave speeds (lib/2d/GetCFL.cpp:76-101).
+int fin_get_cfl_alpha(const fin_params* p, double dt, double dtmax, double alpha1, double alpha2, double* cfl)
+{
+    if (!p || !cfl) return set_err(FIN_ERR_ARG, "null argument");
+    if (p->mx < 1 || p->my < 1 || !(p->xhigh > p->xlow) || !(p->yhigh > p->ylow))
+        return set_err(FIN_ERR_ARG, "bad grid");
+    if (dt > dtmax) return set_err(FIN_ERR_DT_BOUNDS, "dt is out of bounds");
+    const double dx = (p->xhigh - p->xlow) / p->mx, dy = (p->yhigh - p->ylow) / p->my;
+    double c = -100.0;
+    c = Max(dt * alpha1 / dx, c);
+    c = Max(dt * alpha2 / dy, c);
+    *cfl = c;
+    if (c > 1.0e8) return set_err(FIN_ERR_CFL_BOUNDS, "CFL number is out of bounds");
     return FIN_OK;
 }
 

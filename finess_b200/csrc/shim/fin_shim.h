@@ -1,5 +1,7 @@
 // Relink shim: the reference's own C++ entry points (ConstructL,
-// GlobalWaveSpd, FinSolveRK) implemented over the C ABI of libfinb200.so, so
+// GlobalWaveSpd, FinSolveRK, FinSolveMD, FinSolveLxW, UpdateSoln, GetCFL,
+// ConstructIntegratedR, ConstructLxWL) implemented over the C ABI of
+// libfinb200.so, one object per reference object file, so
 // an unmodified FINESS application relinks against this library by naming
 // these objects in its Makefile (lib/2d/Makefile.defs:79-109 lists the names
 // an application may override).  Compiled inside the application's build,
@@ -30,5 +32,9 @@ void fin_shim_unpack_all(const std::vector<double>& buf, dTensorBC3& t);
 // Reference-style failure: print and exit(1), as lib/2d/GetCFL.cpp:43-48 and
 // FinSolveRK.cpp:84-92 do.
 void fin_shim_check(int rc, const char* where);
+
+// One FinSolveRK / FinSolveMD / FinSolveLxW call on the device; the solver's
+// stepper is the one global_ini_params names.
+void fin_shim_finsolve(StateVars& Qnew, double tend, double dtv[], const char* name);
 
 #endif

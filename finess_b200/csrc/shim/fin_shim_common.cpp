@@ -78,7 +78,12 @@ void fin_shim_params(fin_params* out)
     fin_params_default(&p);
     p.meqn = g.get_meqn(); p.maux = g.get_maux();
     p.space_order = g.get_space_order(); p.time_order = g.get_time_order();
-    p.time_stepping_method = FIN_TS_RK;
+    // the stepper the application chose (FinSolveRK, FinSolveMD or
+    // FinSolveLxW; RunFinpack.cpp:100-115 dispatches on the same key)
+    if (g.get_time_stepping_method() == IniParams::TimeSteppingMethod::MD) p.time_stepping_method = FIN_TS_MD;
+    else if (g.get_time_stepping_method() == IniParams::TimeSteppingMethod::LxW) p.time_stepping_method = FIN_TS_LXW;
+    else p.time_stepping_method = FIN_TS_RK;
+    p.mpp_limiter = g.get_mpp_limiter() ? 1 : 0;
     p.global_alpha = g.get_global_alpha() ? 1 : 0;
     p.source_term = g.get_source_term() ? 1 : 0;
     p.nv = g.get_nv(); p.verbosity = g.get_verbosity();
@@ -131,4 +136,28 @@ void fin_shim_unpack_interior(const std::vector<double>& buf, dTensorBC3& t)
         for (int j = 1; j <= my; j++)
             for (int m = 1; m <= meqn; m++)
                 t.set(i, j, m, buf[((size_t)(i + mbc - 1) * sy + (j + mbc - 1)) * meqn + (m - 1)]);
+}
+
+// FinSolveRK / FinSolveMD / FinSolveLxW (lib/2d/RunFinpack.h:18-20) over
+// fin_solve: the state goes to the device once per call (one output frame
+// of RunFinpack.cpp:95-130), every step runs there, and the frame's result
+// comes back with its ghost frame filled as SetBndValues would fill it.
+// conservation.dat gets its line after every accepted step (the reference's
+// steppers call ConSoln there) from totals summed on the device; where the
+// output directory does not exist the lines are dropped, as the reference's
+// ofstream drops them.  The per-stage hooks (BeforeStep/AfterStep, hooks.h)
+// are not called on the device path.
+void fin_shim_finsolve(StateVars& Qnew, double tend, double dtv[], const char* name)
+{
+    fin_solver* s = fin_shim_solver();
+    std::vector<double> q;
+    fin_shim_pack(Qnew.const_ref_q(), q);
+    fin_shim_check(fin_set_state(s, q.data(), Qnew.get_t()), name);
+    fin_set_conservation_file(s, global_ini_params.get_output_dir().c_str());
+    int nsteps = 0;
+    fin_shim_check(fin_solve(s, tend, dtv, &nsteps), name);
+    double t = 0.0;
+    fin_shim_check(fin_get_state(s, q.data(), &t), name);
+    fin_shim_unpack_all(q, Qnew.ref_q());
+    Qnew.set_t(t);
 }

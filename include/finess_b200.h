@@ -158,6 +158,59 @@ int fin_advance(fin_solver* s, double tend, double* dtv, int max_steps, int* nst
  * solver created with Lax-Wendroff or multiderivative stepping (mbc >= 5). */
 int fin_construct_integrated_r(fin_solver* s, double dt, const double* q_host, double* F_host, double* G_host);
 
+/* ConstructIntegratedR, 2-state form (lib/2d/ConstructIntegratedR.cpp:
+ * 525-606, declared lib/2d/constructs.h:19-24): F = alpha1 R(q1) + dt beta1
+ * f_t(q1) + alpha2 R(q2) + dt beta2 f_t(q2), and G alike; arrays as the
+ * 1-state form. */
+int fin_construct_integrated_r2(fin_solver* s, double dt, double alpha1, double beta1, const double* q1_host,
+                                double alpha2, double beta2, const double* q2_host, double* F_host, double* G_host);
+
+/* ConstructIntegratedR, three-coefficient form (lib/2d/ConstructIntegratedR.
+ * cpp:608-700, declared lib/2d/constructs.h:26-31), used by the fifth-order
+ * multiderivative stepper: adds charlie1 dt^2 f_tt(q1) + charlie2 dt^2
+ * f_tt(q2) to the 2-state sum. */
+int fin_construct_integrated_r3(fin_solver* s, double dt, double alpha1, double beta1, double charlie1,
+                                const double* q1_host, double alpha2, double beta2, double charlie2,
+                                const double* q2_host, double* F_host, double* G_host);
+
+/* ConstructLxWL (lib/2d/ConstructLxWL.cpp:30-414, declared lib/2d/
+ * constructs.h:44-51): ConstructL's split, reconstruction and projection
+ * applied to the sampled time-integrated fluxes F, G (ghosted host arrays
+ * whose interior and 3-cell ghost frame are read) instead of FluxFunc of q.
+ * L_host and smax_host as fin_construct_l.  Fhat_host, Ghat_host (may be
+ * NULL: the overload without them) receive the face fluxes in the ghosted
+ * (mx+1, my, meqn) and (mx, my+1, meqn) layouts, faces 1..mx+1 / 1..my+1
+ * written.  Needs a solver created with Lax-Wendroff or multiderivative
+ * stepping. */
+int fin_construct_lxwl(fin_solver* s, const double* q_host, const double* F_host, const double* G_host,
+                       double* L_host, double* smax_host, double* Fhat_host, double* Ghat_host);
+
+/* UpdateSoln, orders 1-4 (lib/2d/UpdateSoln.cpp:14-38, declared lib/2d/
+ * FinSolveRK.h:21-22): qnew = alpha1 qstar + alpha2 qnew + (beta dt) L over
+ * every element of the ghosted arrays (ghosts included, in the reference's
+ * operation order, correctly rounded), and *t_new = alpha1 t_star + alpha2
+ * *t_new + beta dt. */
+int fin_update_soln(fin_solver* s, double alpha1, double alpha2, double beta, double dt, const double* qstar_host,
+                    double t_star, const double* L_host, double* qnew_host, double* t_new);
+
+/* UpdateSoln, the fifth-order stepper's form (lib/2d/UpdateSoln.cpp:43-80,
+ * declared lib/2d/FinSolveRK.h:25-29): over every element, q2 = q2 + delta
+ * q1, then q1 = g1 q1 + g2 q2 + g3 qold + (beta dt) L; times untouched. */
+int fin_update_soln5(fin_solver* s, double g1, double g2, double g3, double delta, double beta, double dt,
+                     const double* qold_host, const double* L_host, double* q1_host, double* q2_host);
+
+/* GetCFL (lib/2d/GetCFL.cpp:31-73, declared lib/2d/misc2d.h:7): the maximum
+ * of dt smax(i,j,1)/dx and dt smax(i,j,2)/dy over i <= mx, j <= my of the
+ * ghosted (mx+1, my+1, 2) host array smax_host (NaN entries skipped, as the
+ * reference's Max does).  Returns FIN_ERR_DT_BOUNDS when dt > dtmax and
+ * FIN_ERR_CFL_BOUNDS when the CFL number exceeds 1e8 (*cfl is set then too);
+ * the relink shim turns these into the reference's message and exit(1). */
+int fin_get_cfl(fin_solver* s, double dt, double dtmax, const double* smax_host, double* cfl);
+
+/* GetCFL from the global wave speeds (lib/2d/GetCFL.cpp:76-101, declared
+ * lib/2d/misc2d.h:8): max(dt alpha1/dx, dt alpha2/dy), same errors. */
+int fin_get_cfl_alpha(const fin_params* p, double dt, double dtmax, double alpha1, double alpha2, double* cfl);
+
 /* One time step of exactly dt with no CFL control (benchmarking and
  * per-step parity); cfl_out (may be NULL) receives GetCFL's value for it. */
 int fin_step_fixed(fin_solver* s, double dt, double* cfl_out);

@@ -34,6 +34,8 @@ ORACLE_SO = os.path.join(HERE, "liboracle.so")
 REF_SO = os.path.join(HERE, "_ref", "libfinref.so")
 # the same reference objects relinked against libfinb200.so through the shim
 REF_SHIM_SO = os.path.join(HERE, "_ref", "libfinref_shim.so")
+# the reference's own steppers with their building blocks relinked against libfinb200.so
+REF_SHIM_PARTS_SO = os.path.join(HERE, "_ref", "libfinref_shim_parts.so")
 REF_MHD_SO = os.path.join(HERE, "_ref", "libfinref_mhd.so")
 # the MHD application's objects relinked against libfinb200.so (its FinSolveRK replaced)
 REF_MHD_SHIM_SO = os.path.join(HERE, "_ref", "libfinref_mhd_shim.so")

@@ -115,6 +115,9 @@ int ref_setup(const fin_params* p)
     g.epsilon = p->epsilon; g.power_param = p->power_param; g.alpha_scaling = p->alpha_scaling;
     g.gamma = p->gamma;
     g.mpp_limiter = p->mpp_limiter != 0;
+    g.time_stepping_method = p->time_stepping_method == FIN_TS_MD    ? IniParams::TimeSteppingMethod::MD
+                             : p->time_stepping_method == FIN_TS_LXW ? IniParams::TimeSteppingMethod::LxW
+                                                                     : IniParams::TimeSteppingMethod::RK;
     g_bc[0] = p->bc_xlow; g_bc[1] = p->bc_xhigh; g_bc[2] = p->bc_ylow; g_bc[3] = p->bc_yhigh;
     return 0;
 }

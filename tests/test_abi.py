@@ -93,3 +93,19 @@ def test_space_order_validation_without_gpu(lib):
         lib.fin_destroy(h)
     else:
         assert b"Requested WENO" not in lib.fin_last_error() and b"space order" not in lib.fin_last_error()
+
+
+def test_get_cfl_alpha_matches_reference_arithmetic(lib):
+    """GetCFL from the global wave speeds (lib/2d/GetCFL.cpp:76-101) is host
+    arithmetic: max(dt a1/dx, dt a2/dy) and the reference's two errors."""
+    from finess_b200._abi import FIN_ERR_CFL_BOUNDS, FIN_ERR_DT_BOUNDS, FIN_OK
+    p = default_params(mx=40, my=25, xlow=0.0, xhigh=2.0, ylow=-1.0, yhigh=1.5)
+    lib.fin_get_cfl_alpha.argtypes = [C.POINTER(FinParams), C.c_double, C.c_double, C.c_double, C.c_double,
+                                      C.POINTER(C.c_double)]
+    cfl = C.c_double()
+    dt, a1, a2 = 1e-3, 3.7, 2.9
+    assert lib.fin_get_cfl_alpha(C.byref(p), dt, 1.0, a1, a2, C.byref(cfl)) == FIN_OK
+    dx, dy = (2.0 - 0.0) / 40, (1.5 - -1.0) / 25
+    assert cfl.value == max(dt * a1 / dx, dt * a2 / dy, -100.0)
+    assert lib.fin_get_cfl_alpha(C.byref(p), 2.0, 1.0, a1, a2, C.byref(cfl)) == FIN_ERR_DT_BOUNDS
+    assert lib.fin_get_cfl_alpha(C.byref(p), dt, 1.0, 1e12, a2, C.byref(cfl)) == FIN_ERR_CFL_BOUNDS
