@@ -18,6 +18,8 @@ FIN_BC_PERIODIC, FIN_BC_TRANSMISSIVE = 0, 1
 FIN_PHYS_EULER = 0
 FIN_PHYS_MHD = 1
 FIN_PREC_FP64, FIN_PREC_FP32, FIN_PREC_HYBRID = 0, 1, 2
+# initial data sampled on the device (fin_set_state_qinit)
+FIN_QINIT_VORTEX, FIN_QINIT_RIEMANN4, FIN_QINIT_SHOCK_ENTROPY, FIN_QINIT_SHOCK_TUBE, FIN_QINIT_VORTEX_EXACT2 = 1, 2, 3, 4, 5
 
 WENO_NAMES = {"FD": FIN_WENO_FD, "JS": FIN_WENO_JS, "Z": FIN_WENO_Z}
 

@@ -25,6 +25,7 @@
 #include "fin_mpp.cuh"
 #include "fin_rk.cuh"
 #include "fin_weno_hi.cuh"
+#include "fin_sample.cuh"
 
 using namespace fin;
 
@@ -1260,6 +1261,61 @@ int fin_set_state(fin_solver* s, const double* q_host, double t)
     s->ind_since = -1;
     CK(cudaMemsetAsync(s->slots + SLOT_STATUS, 0, sizeof(double), s->stream));
     if ((rc = compute_alpha(s, s->cur))) return rc;
+    s->alpha_valid = true;
+    return check_status(s);
+}
+
+// Initial data sampled on the device (SampleFunction with a QinitFunc
+// functor, fin_sample.cuh) straight into q^n: no host array, no upload.
+int fin_set_state_qinit(fin_solver* s, int problem, const double* prm, int nprm, double t)
+{
+    if (!s) return set_err(FIN_ERR_ARG, "null solver");
+    if (nprm > 0 && !prm) return set_err(FIN_ERR_ARG, "null parameters");
+    const fin_params& p = s->p;
+    double* q = s->q[s->cur];
+    const double g = p.gamma;
+    cudaError_t e = cudaSuccess;
+    switch (problem) {
+    case FIN_QINIT_VORTEX: {
+        if (nprm != 0 && nprm != 3) return set_err(FIN_ERR_ARG, "vortex: parameters are eps, xc, yc");
+        const qinit::Vortex f{g, nprm ? prm[0] : 5.0, nprm ? prm[1] : 5.0, nprm ? prm[2] : 5.0};
+        e = launch_sample(f, p.xlow, p.ylow, s->dx, s->dy, p.mx, p.my, q, s->plane, s->stream);
+        break;
+    }
+    case FIN_QINIT_RIEMANN4: {
+        if (nprm != 0 && nprm != 18) return set_err(FIN_ERR_ARG, "riemann4: parameters are xc, yc, 4 x (rho, u, v, p)");
+        static const double def[18] = {0.8, 0.8, 1.5, 0.0, 0.0, 1.5, 0.5323, 1.206, 0.0, 0.3,
+                                       0.138, 1.206, 1.206, 0.029, 0.5323, 0.0, 1.206, 0.3};
+        const double* v = nprm ? prm : def;
+        qinit::Riemann4 f;
+        f.gamma = g; f.xc = v[0]; f.yc = v[1];
+        for (int k = 0; k < 4; k++)
+            for (int c = 0; c < 4; c++) f.s[k][c] = v[2 + 4 * k + c];
+        e = launch_sample(f, p.xlow, p.ylow, s->dx, s->dy, p.mx, p.my, q, s->plane, s->stream);
+        break;
+    }
+    case FIN_QINIT_SHOCK_ENTROPY:
+        e = launch_sample(qinit::ShockEntropy{g}, p.xlow, p.ylow, s->dx, s->dy, p.mx, p.my, q, s->plane, s->stream);
+        break;
+    case FIN_QINIT_SHOCK_TUBE: {
+        if (nprm != 1) return set_err(FIN_ERR_ARG, "shock tube: one parameter, OPT");
+        e = launch_sample(qinit::ShockTube{g, int(prm[0])}, p.xlow, p.ylow, s->dx, s->dy, p.mx, p.my, q, s->plane,
+                          s->stream);
+        break;
+    }
+    case FIN_QINIT_VORTEX_EXACT2:
+        e = launch_sample(qinit::VortexExact2{g}, p.xlow, p.ylow, s->dx, s->dy, p.mx, p.my, q, s->plane, s->stream);
+        break;
+    default:
+        return set_err(FIN_ERR_ARG, "unknown initial-data problem");
+    }
+    if (e != cudaSuccess) return set_err(FIN_ERR_CUDA, std::string("k_sample: ") + cudaGetErrorString(e));
+    s->launches++;
+    s->t = t;
+    s->ind_since = -1;
+    CK(cudaMemsetAsync(s->slots + SLOT_STATUS, 0, sizeof(double), s->stream));
+    int rc = compute_alpha(s, s->cur);
+    if (rc) return rc;
     s->alpha_valid = true;
     return check_status(s);
 }

@@ -83,6 +83,8 @@ def load_library(path=LIB_PATH):
     lib.fin_set_conservation_file.argtypes = [vp, C.c_char_p]
     lib.fin_write_conservation.argtypes = [vp]
     lib.fin_write_qhelp.argtypes = [P, C.c_char_p]
+    lib.fin_set_state_qinit.argtypes = [vp, C.c_int, C.c_void_p, C.c_int, C.c_double]
+    lib.fin_set_state_qinit.restype = C.c_int
     for name in ("fin_output_frame", "fin_output_wait", "fin_read_frame", "fin_set_conservation_file",
                  "fin_write_conservation", "fin_write_qhelp"):
         getattr(lib, name).restype = C.c_int
@@ -155,6 +157,13 @@ class Solver:
         q = np.ascontiguousarray(q, dtype=np.float64)
         assert q.shape == ghosted_shape(self.p), (q.shape, ghosted_shape(self.p))
         _check(self.lib.fin_set_state(self.h, q, t))
+
+    def set_state_qinit(self, problem, prm=(), t=0.0):
+        """Initial data sampled on the device (SampleFunction with a built-in
+        QinitFunc functor; problem = FIN_QINIT_*, prm its parameters)."""
+        a = np.ascontiguousarray(prm, dtype=np.float64)
+        _check(self.lib.fin_set_state_qinit(self.h, int(problem), a.ctypes.data_as(C.c_void_p) if a.size else None,
+                                            int(a.size), t))
 
     def get_state(self, out=None):
         """(q, t): the state in the reference's ghosted layout, into `out`

@@ -121,6 +121,30 @@ int fin_destroy(fin_solver* s);
 /* Copies a host state (reference ghosted layout, interior used) to the device
  * and sets t.  Replaces StateVars construction + QinitFunc sampling. */
 int fin_set_state(fin_solver* s, const double* q_host, double t);
+/* Initial data sampled on the device into the state and t set: SampleFunction
+ * (lib/2d/SampleFunction.cpp:62-125) with a QinitFunc (lib/2d/app_defined.h:7)
+ * evaluated at the interior cell centres xlow + (i - 1/2) dx,
+ * ylow + (j - 1/2) dy, as RunFinpack.cpp:80 does before the first frame.
+ * Replaces StateVars construction + host sampling + fin_set_state.
+ * problem / prm (nprm values; 0 = the defaults in brackets):
+ *   FIN_QINIT_VORTEX         isentropic vortex on the background (1, 1, 1, 1):
+ *                            eps, xc, yc [5, 5, 5]
+ *   FIN_QINIT_RIEMANN4       four-quadrant Riemann problem: xc, yc, then
+ *                            (rho, u, v, p) of the upper-right, upper-left,
+ *                            lower-left, lower-right quadrants [interface
+ *                            (0.8, 0.8), the benchmark's states]
+ *   FIN_QINIT_SHOCK_ENTROPY  shock / entropy-wave interaction on [-5,5]x[0,1]
+ *   FIN_QINIT_SHOCK_TUBE     apps/2d/euler/riemann_test/QinitFunc.cpp: OPT
+ *   FIN_QINIT_VORTEX_EXACT2  apps/2d/euler/test_exact2/QinitFunc.cpp
+ * Applications with their own initial data instantiate the device template
+ * fin::launch_sample<Functor> of finess_b200/csrc/fin_sample.cuh. */
+#define FIN_QINIT_VORTEX 1
+#define FIN_QINIT_RIEMANN4 2
+#define FIN_QINIT_SHOCK_ENTROPY 3
+#define FIN_QINIT_SHOCK_TUBE 4
+#define FIN_QINIT_VORTEX_EXACT2 5
+int fin_set_state_qinit(fin_solver* s, int problem, const double* prm, int nprm, double t);
+
 /* Copies the device state back (interior written; ghosts filled by the BC
  * remap, as SetBndValues would). */
 int fin_get_state(fin_solver* s, double* q_host, double* t);

@@ -10,6 +10,8 @@
   The MHD arrays are q (mx+2mbc, my+2mbc, 8) and aux (mx+2mbc, my+2mbc, 1).
 * ``IoRefLib``: oracle/_ref/libfinref_io.so, the reference's output routines
   (lib/2d/Output.cpp, WriteQhelp.cpp, ConSoln.cpp) writing their files.
+* ``RefQinit``: oracle/_ref/libfinref_qinit_<app>.so, the reference's
+  SampleFunction with an application's own QinitFunc.
 
 All take and return numpy arrays in the reference's ghosted dTensorBC3 layout
 (lib/tensors.h:267-273), shape (mx+2mbc, my+2mbc, meqn).  Only tests/,
@@ -357,6 +359,34 @@ class MhdRefLib:
         dtv = np.array([0.0, dt, p.max_dt])
         rc = self.lib.ref_mhd_finsolve(q, aux, C.byref(tt), tend, dtv)
         return rc, q, aux, tt.value, dtv[1]
+
+
+class RefQinit:
+    """The reference's SampleFunction with one application's own QinitFunc
+    (app "riemann_test" or "test_exact2"); available where oracle/_ref was
+    built.  sample(p, opt) returns the ghosted (mx+2mbc, my+2mbc, 5) array
+    RunFinpack.cpp:80 fills (ghosts sampled too)."""
+
+    @staticmethod
+    def path(app):
+        return os.path.join(HERE, "_ref", f"libfinref_qinit_{app}.so")
+
+    @staticmethod
+    def available(app):
+        return os.path.exists(RefQinit.path(app))
+
+    def __init__(self, app):
+        lib = C.CDLL(RefQinit.path(app))
+        lib.ref_qinit.argtypes = [C.POINTER(FinParams), C.c_int, _dp]
+        lib.ref_qinit.restype = C.c_int
+        self.lib = lib
+
+    def sample(self, p, opt=1):
+        q = np.zeros(ghosted_shape(p))
+        rc = self.lib.ref_qinit(C.byref(p), opt, q)
+        if rc:
+            raise ValueError(f"ref_qinit failed: {rc}")
+        return q
 
 
 REF_IO_SO = os.path.join(HERE, "_ref", "libfinref_io.so")

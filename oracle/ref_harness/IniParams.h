@@ -34,6 +34,9 @@ public:
     // [euler] / [mhd]
     double gamma = 1.4;
     bool constrained_transport = true;
+    // [initial] of apps/2d/euler/riemann_test (its this_app_params.py): the
+    // shock tube's direction
+    int OPT = 1;
 
     int get_ndims() const { return ndims; }
     int get_nout() const { return nout; }
@@ -70,6 +73,7 @@ public:
     double get_epsilon() const { return epsilon; }
     double get_gamma() const { return gamma; }
     bool get_constrained_transport() const { return constrained_transport; }
+    int get_OPT() const { return OPT; }
 };
 
 extern IniParams global_ini_params;

@@ -187,3 +187,18 @@ def test_space_order_frame_bar_is_tight(path):
     if "_fd_" in name or "finsolverk1_" in name:
         assert 10.0 * sens < 1e-11
     assert np.isfinite(interior(g["p"], g["q1"])).all()
+
+
+def test_reference_sampling_harness():
+    """The reference's SampleFunction with its riemann_test QinitFunc (the
+    checker of the device sampling) fills the whole ghosted grid, split at
+    x = 0.5 (OPT 1) or y = 0.5 (OPT 2)."""
+    from oracle import RefQinit
+    if not RefQinit.available("riemann_test"):
+        pytest.skip("oracle/_ref not built")
+    p = P.riemann_params(n=8)
+    x, y = P.cell_centres(p)
+    for opt, c in ((1, x), (2, y)):
+        q = RefQinit("riemann_test").sample(p, opt)
+        assert np.array_equal(q[..., 0], np.where(c > 0.5, 1.0, 3.0))
+        assert np.array_equal(q[..., 4], np.where(c > 0.5, 1.0, 3.0) / (p.gamma - 1.0))
