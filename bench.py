@@ -12,6 +12,7 @@ than the 126 MB L2, so no L2 flush is needed between steps.
     python bench.py --space-orders [--n N] [--steps K]    # LLF, WENO7/9/11 beside WENO5 (FP64)
     python bench.py --mpp [--n N] [--steps K]             # Lax-Wendroff with / without the MPP limiter
     python bench.py --frames [--n N]                      # frame files, and the reference's Output beside them
+    python bench.py --sweep [--gpus N]                    # the 1024-problem uneven sweep split across N GPUs
 
 The headline form is the hybrid (FP32 bulk + troubled-face network run every
 HYB_EVERY accepted steps, judge step every HYB_JUDGE_EVERY steps) when trained
@@ -465,6 +466,30 @@ def run_frames_bench(args):
     print(json.dumps(out), flush=True)
 
 
+def run_sweep_bench(args):
+    """The batched uneven sweep (1024 four-quadrant Riemann problems, N
+    log-uniform in [64, 1024], FP32, SSP-RK3 to t = 0.25) with its problems
+    split across the ranks by estimated work (finess_b200/sweep_ranks.py):
+    no exchange between ranks; whole-job cell-updates/s over the slowest
+    rank's device time (strong scaling)."""
+    ws, rank, local = dist_env()
+    import torch
+    torch.cuda.set_device(local)
+    from finess_b200 import replicas
+    from finess_b200.batch import PRECISIONS
+    from finess_b200.sweep_ranks import batch_solve, run_sweep_ranks
+    replicas.init(ws, backend="nccl", timeout_s=300)
+    out = run_sweep_ranks(1024, 0, rank, ws, batch_solve(0, PRECISIONS["fp32"], 0.25))
+    if rank == 0:
+        print(json.dumps({"metric": "2D Euler batched uneven sweep cell-updates/s (1024 problems, FP32)",
+                          "value": out["cell_updates_per_s"], "unit": UNIT, "n_gpus": ws, "scaling": "strong",
+                          "higher_is_better": True, "data": "synthetic", "dtype": "f32 (f64 state)",
+                          "config": {"workload": "euler2d_riemann_sweep1024_rk3", "tend": 0.25, "seed": 0,
+                                     "parallelism": f"problems split over {ws} ranks"},
+                          "detail": out}), flush=True)
+    replicas.finish()
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -486,6 +511,8 @@ def main():
                     help="every form to t = 0.8 at full size, with the errors against the FP64 run")
     ap.add_argument("--frames", action="store_true",
                     help="frame files from device state, and the reference's Output on the last frame")
+    ap.add_argument("--sweep", action="store_true",
+                    help="the uneven 1024-problem sweep (FP32, to t = 0.25), its problems split across the ranks")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     if args.mpp:
@@ -503,6 +530,9 @@ def main():
         return
     if args.frames:
         run_frames_bench(args)
+        return
+    if args.sweep:
+        run_sweep_bench(args)
         return
     if args.impl == "reference":
         run_reference_arm(args)

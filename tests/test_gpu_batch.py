@@ -111,3 +111,23 @@ def test_batch_rejects_mixed_forms():
     b.precision = FIN_PREC_FP32
     with pytest.raises(FinError):
         Batch([a, b])
+
+
+def test_sweep_split_across_ranks_equals_one_batch():
+    """The sweep split for two GPUs (finess_b200/sweep_ranks.py): each share
+    run as its own batch, as each rank would on its own GPU (the ranks share
+    nothing, so running the shares one after the other on one GPU is the same
+    computation), gives every problem's single-batch result and steps."""
+    from finess_b200._abi import FIN_PREC_FP64
+    from finess_b200.sweep_ranks import batch_solve, partition, problem_sizes
+    seed, n, nmin, nmax, tend = 5, 9, 24, 72, 0.05
+    sizes = problem_sizes(n, seed, nmin, nmax)
+    solve = batch_solve(seed, FIN_PREC_FP64, tend, nmin, nmax)
+    _, steps_all, states_all = solve(list(range(n)), keep_states=True)
+    parts, _ = partition([float(N) ** 3 for N in sizes], 2)
+    assert all(parts)
+    for part in parts:
+        _, steps, states = solve(part, keep_states=True)
+        for k, st, q in zip(part, steps, states):
+            assert st == steps_all[k]
+            assert np.max(np.abs(q - states_all[k])) <= 1e-12 * np.max(np.abs(states_all[k]))
