@@ -78,5 +78,22 @@ def build(force=False, verbose=False):
     return OUT
 
 
+def build_app(src, out, force=False):
+    """An application's own .cu file (its physics policy and hooks, its
+    extern "C" entry points) compiled against this library's device headers
+    (fin_physics.cuh, fin_physics_host.h, fin_sample.cuh) into a shared
+    library, as an application links its callbacks."""
+    headers = _newest((".cuh", ".h"))
+    if not force and os.path.exists(out) and os.path.getmtime(out) >= max(headers, os.path.getmtime(src)):
+        return out
+    nvcc = os.environ.get("NVCC", "nvcc")
+    cmd = [nvcc] + NVCC_FLAGS + ["-shared", "-I" + os.path.join(ROOT, "include"), "-I" + CSRC, "-o", out, src]
+    res = subprocess.run(cmd, capture_output=True, text=True)
+    if res.returncode != 0:
+        sys.stderr.write(res.stdout + res.stderr)
+        raise RuntimeError("nvcc failed on " + src)
+    return out
+
+
 if __name__ == "__main__":
     print(build(force="--force" in sys.argv, verbose=True))
