@@ -98,9 +98,43 @@ struct App : AppBase {
     int step_fixed(double dt, double* cfl) override { return d.step_fixed(dt, cfl); }
 };
 
+// The library's reciprocal (fin_device.cuh: Newton-Raphson refinement of
+// rcp.approx) beside CUDA's correctly rounded division, for a sweep of
+// arguments.
+__global__ void k_rcp_probe(const double* x, double* r64, double* div64, float* r32, int n)
+{
+    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
+        r64[k] = fin::rcp(x[k]);
+        div64[k] = __ddiv_rn(1.0, x[k]);
+        r32[k] = fin::rcp(float(x[k]));
+    }
+}
+
 }  // namespace
 
 extern "C" {
+
+// rcp(x) (FP64 and FP32) and 1/x of n host values through the device.
+int app_rcp_probe(const double* x, double* r64, double* div64, float* r32, int n)
+{
+    double *dx = nullptr, *d64 = nullptr, *dd = nullptr;
+    float* d32 = nullptr;
+    if (cudaMalloc(&dx, n * sizeof(double)) != cudaSuccess || cudaMalloc(&d64, n * sizeof(double)) != cudaSuccess ||
+        cudaMalloc(&dd, n * sizeof(double)) != cudaSuccess || cudaMalloc(&d32, n * sizeof(float)) != cudaSuccess)
+        return FIN_ERR_CUDA;
+    cudaMemcpy(dx, x, n * sizeof(double), cudaMemcpyHostToDevice);
+    k_rcp_probe<<<(n + 255) / 256, 256>>>(dx, d64, dd, d32, n);
+    int rc = cudaGetLastError() == cudaSuccess ? FIN_OK : FIN_ERR_CUDA;
+    cudaMemcpy(r64, d64, n * sizeof(double), cudaMemcpyDeviceToHost);
+    cudaMemcpy(div64, dd, n * sizeof(double), cudaMemcpyDeviceToHost);
+    cudaMemcpy(r32, d32, n * sizeof(float), cudaMemcpyDeviceToHost);
+    if (cudaDeviceSynchronize() != cudaSuccess) rc = FIN_ERR_CUDA;
+    cudaFree(dx);
+    cudaFree(d64);
+    cudaFree(dd);
+    cudaFree(d32);
+    return rc;
+}
 
 // kind 0: advection-acoustics, prm = (K, rho0, ax, ay); kind 1: the same with
 // the hooks, prm = (K, rho0, ax, ay, h0, h1); kind 2: EulerPhys (gamma of p).

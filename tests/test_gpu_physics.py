@@ -178,3 +178,39 @@ def test_euler_policy_steps_equal_the_specialised_kernel(app, oracle):
         qo, _ = oracle.step_fixed(p, qo, dt)
     assert rel_linf(interior(p, qg), interior(p, qo)) <= TOL
     assert rel_linf(interior(p, qg), interior(p, qs)) <= TOL
+
+
+def test_reciprocal_error_bounds(app):
+    """fin_device.cuh's rcp (Newton-Raphson refinement of rcp.approx, two
+    steps in FP64): within 1 ulp of the correctly rounded 1/x, and equal to
+    CUDA's __ddiv_rn(1, x) for most x, over normal magnitudes 2^-1000 ..
+    2^1000 of both signs; x = 0 and subnormal x give NaN and results below
+    the normal range flush to 0, as its comment states (no use divides by
+    such values: a zero or subnormal density is already a failed state).
+    FP32: rcp.approx alone, within 1 ulp of 1/x."""
+    f64 = np.ctypeslib.ndpointer(dtype=np.float64, flags="C_CONTIGUOUS")
+    f32 = np.ctypeslib.ndpointer(dtype=np.float32, flags="C_CONTIGUOUS")
+    app.app_rcp_probe.argtypes = [f64, f64, f64, f32, C.c_int]
+    app.app_rcp_probe.restype = C.c_int
+    rng = np.random.default_rng(8)
+    e = rng.uniform(-1000, 1000, 200000)
+    x = np.ldexp(rng.uniform(1.0, 2.0, e.size), e.astype(np.int64)) * rng.choice([-1.0, 1.0], e.size)
+    x = np.concatenate([x, [1.0, 3.0, 0.1, 1.4, 1e-300, 7e300, 2.0 ** -1022, 2.0 ** 1021 * 1.5]])
+    edge = np.array([0.0, 1e-310, -2.0 ** -1070, 2.0 ** 1023])
+    allx = np.ascontiguousarray(np.concatenate([x, edge]))
+    n = allx.size
+    r64, d64, r32 = np.zeros(n), np.zeros(n), np.zeros(n, dtype=np.float32)
+    assert app.app_rcp_probe(allx, r64, d64, r32, n) == FIN_OK
+    exact = 1.0 / x
+    k = x.size
+    ulp_err = np.abs(r64[:k] - exact) / np.spacing(np.abs(exact))
+    assert np.max(ulp_err) <= 1.0
+    assert np.array_equal(d64[:k], exact)                      # CUDA's division is correctly rounded
+    assert np.mean(r64[:k] == exact) > 0.99
+    assert np.isnan(r64[k]) and np.isnan(r64[k + 1]) and np.isnan(r64[k + 2])   # 0 and subnormal x
+    assert r64[k + 3] == 0.0                                   # 1/2^1023 is subnormal: flushed
+    x32 = x[(np.abs(x) > 1e-30) & (np.abs(x) < 1e30)].astype(np.float32)
+    sel = (np.abs(allx[:k]) > 1e-30) & (np.abs(allx[:k]) < 1e30)
+    ex32 = (np.float32(1.0) / x32).astype(np.float32)
+    err32 = np.abs(r32[:k][sel].astype(np.float64) - ex32) / np.spacing(np.abs(ex32))
+    assert np.max(err32) <= 1.0
