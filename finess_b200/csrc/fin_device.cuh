@@ -67,6 +67,51 @@ __device__ __forceinline__ float rcp(float x)
     asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
     return r;
 }
+// Packed pairs of FP32 values for sm_100's f32x2 arithmetic (PTX add / mul /
+// fma .rn.f32x2): one instruction computes two independent lanes, each
+// rounded exactly as the scalar operation would be, so code written on pairs
+// gives the bits of the same scalar code with half the instructions.
+struct f2 {
+    unsigned long long v;
+};
+__device__ __forceinline__ f2 f2_make(float a, float b)
+{
+    f2 r;
+    asm("mov.b64 %0, {%1, %2};" : "=l"(r.v) : "f"(a), "f"(b));
+    return r;
+}
+__device__ __forceinline__ f2 f2_of(float2 a) { return f2_make(a.x, a.y); }
+__device__ __forceinline__ float f2_lo(f2 a)
+{
+    float lo, hi;
+    asm("mov.b64 {%0, %1}, %2;" : "=f"(lo), "=f"(hi) : "l"(a.v));
+    return lo;
+}
+__device__ __forceinline__ float f2_hi(f2 a)
+{
+    float lo, hi;
+    asm("mov.b64 {%0, %1}, %2;" : "=f"(lo), "=f"(hi) : "l"(a.v));
+    return hi;
+}
+__device__ __forceinline__ f2 f2_fma(f2 a, f2 b, f2 c)   // a b + c per lane
+{
+    f2 r;
+    asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(r.v) : "l"(a.v), "l"(b.v), "l"(c.v));
+    return r;
+}
+__device__ __forceinline__ f2 f2_mul(f2 a, f2 b)
+{
+    f2 r;
+    asm("mul.rn.f32x2 %0, %1, %2;" : "=l"(r.v) : "l"(a.v), "l"(b.v));
+    return r;
+}
+__device__ __forceinline__ f2 f2_add(f2 a, f2 b)
+{
+    f2 r;
+    asm("add.rn.f32x2 %0, %1, %2;" : "=l"(r.v) : "l"(a.v), "l"(b.v));
+    return r;
+}
+
 __device__ __forceinline__ double fsqrt(double x) { return sqrt(x); }
 __device__ __forceinline__ float fsqrt(float x)
 {
@@ -320,6 +365,68 @@ __device__ __forceinline__ R weno5(const R* u, R eps, R pw)
         }
     }
     return (w0 * c0 + w1 * c1 + w2 * c2) * rcp(w0 + w1 + w2);
+}
+
+// The two WENO5 reconstructions of a face's split (u = gp, the points of
+// the + split; the pair's second lane gm) in FP32 as f32x2 pairs, with power
+// 2 (or the linear FD5 weights): the operations of weno5<float, VER, true>,
+// each product and sum written out (explicit fma where the scalar form
+// contracts), both lanes in one instruction; the weight normalisation's
+// maxima and reciprocals per lane.  Returns WENO(gp) + WENO(gm).
+__device__ __forceinline__ f2 f2_splat(float a) { return f2_make(a, a); }
+__device__ __forceinline__ f2 f2_abs(f2 a)
+{
+    f2 r;
+    r.v = a.v & 0x7fffffff7fffffffull;
+    return r;
+}
+template <int VER>
+__device__ __forceinline__ float weno5_pair_x2(const float* up, const float* um, float eps)
+{
+    f2 u[5];
+#pragma unroll
+    for (int k = 0; k < 5; k++) u[k] = f2_make(up[k], um[k]);
+    const f2 uim2 = u[0], uim1 = u[1], ui = u[2], uip1 = u[3], uip2 = u[4];
+    const f2 k1312 = f2_splat(13.0f / 12.0f), k025 = f2_splat(0.25f);
+    auto beta = [&](f2 t, f2 s) { return f2_fma(k1312, f2_mul(t, t), f2_mul(k025, f2_mul(s, s))); };
+    const f2 b0 = beta(f2_add(f2_fma(f2_splat(-2.0f), uim1, uim2), ui),
+                       f2_fma(f2_splat(3.0f), ui, f2_fma(f2_splat(-4.0f), uim1, uim2)));
+    const f2 b1 = beta(f2_add(f2_fma(f2_splat(-2.0f), ui, uim1), uip1), f2_fma(f2_splat(-1.0f), uip1, uim1));
+    const f2 b2 = beta(f2_add(f2_fma(f2_splat(-2.0f), uip1, ui), uip2),
+                       f2_add(f2_fma(f2_splat(-4.0f), uip1, f2_mul(f2_splat(3.0f), ui)), uip2));
+    const f2 c0 = f2_fma(f2_splat(11.0f / 6.0f), ui, f2_fma(f2_splat(-7.0f / 6.0f), uim1, f2_mul(f2_splat(1.0f / 3.0f), uim2)));
+    const f2 c1 = f2_fma(f2_splat(1.0f / 3.0f), uip1, f2_fma(f2_splat(5.0f / 6.0f), ui, f2_mul(f2_splat(-1.0f / 6.0f), uim1)));
+    const f2 c2 = f2_fma(f2_splat(-1.0f / 6.0f), uip2, f2_fma(f2_splat(5.0f / 6.0f), uip1, f2_mul(f2_splat(1.0f / 3.0f), ui)));
+    f2 r;
+    if (VER == FIN_WENO_FD) {
+        r = f2_fma(f2_splat(0.3f), c2, f2_fma(f2_splat(0.6f), c1, f2_mul(f2_splat(0.1f), c0)));
+    } else {
+        const f2 e = f2_splat(eps);
+        const f2 d0 = f2_add(e, b0), d1 = f2_add(e, b1), d2 = f2_add(e, b2);
+        f2 D0 = f2_mul(d0, d0), D1 = f2_mul(d1, d1), D2 = f2_mul(d2, d2);
+        const float sl = rcp(Max(f2_lo(D0), Max(f2_lo(D1), f2_lo(D2))));
+        const float sh = rcp(Max(f2_hi(D0), Max(f2_hi(D1), f2_hi(D2))));
+        const f2 sc = f2_make(sl, sh);
+        D0 = f2_mul(D0, sc);
+        D1 = f2_mul(D1, sc);
+        D2 = f2_mul(D2, sc);
+        f2 w0, w1, w2;
+        if (VER == FIN_WENO_JS) {
+            w0 = f2_mul(f2_splat(0.1f), f2_mul(D1, D2));
+            w1 = f2_mul(f2_splat(0.6f), f2_mul(D0, D2));
+            w2 = f2_mul(f2_splat(0.3f), f2_mul(D0, D1));
+        } else {
+            const f2 tau = f2_abs(f2_fma(f2_splat(-1.0f), b2, b0));
+            const f2 T = f2_mul(f2_mul(tau, tau), sc);
+            w0 = f2_mul(f2_splat(0.1f), f2_mul(f2_add(D0, T), f2_mul(D1, D2)));
+            w1 = f2_mul(f2_splat(0.6f), f2_mul(f2_add(D1, T), f2_mul(D0, D2)));
+            w2 = f2_mul(f2_splat(0.3f), f2_mul(f2_add(D2, T), f2_mul(D0, D1)));
+        }
+        const f2 num = f2_fma(w2, c2, f2_fma(w1, c1, f2_mul(w0, c0)));
+        const f2 den = f2_add(f2_add(w0, w1), w2);
+        r = f2_mul(num, f2_make(rcp(f2_lo(den)), rcp(f2_hi(den))));
+    }
+    return f2_lo(r) + f2_hi(r);
 }
 
 }  // namespace fin

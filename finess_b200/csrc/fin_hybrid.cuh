@@ -60,6 +60,12 @@ __device__ __forceinline__ float gelu2(float x)
 {
     return fmaf(x, mlp::tanh_approx(x * fmaf(mlp::GK1, x * x, mlp::GK0)), x);
 }
+// gelu2 of two values as f32x2 pairs: lane by lane the same operations.
+__device__ __forceinline__ f2 gelu2_x2(f2 x)
+{
+    const f2 a = f2_mul(x, f2_fma(f2_make(mlp::GK1, mlp::GK1), f2_mul(x, x), f2_make(mlp::GK0, mlp::GK0)));
+    return f2_fma(x, f2_make(mlp::tanh_approx(f2_lo(a)), mlp::tanh_approx(f2_hi(a))), x);
+}
 
 // D (TMEM columns at tmem_d) = A (128 x 32, K-major) * B (32 x 32, K-major)^T,
 // issued by one thread, no commit.
@@ -177,7 +183,11 @@ __device__ __forceinline__ void indicator_tile(IndTile<Cfg>& S, const int mx, co
         float v[32];
         tc::tmem_ld32(tmem + lane_base + 32 * mt, v);
 #pragma unroll
-        for (int o = 0; o < NH; o++) v[o] = ind::gelu2(v[o]);
+        for (int o = 0; o < NH; o += 2) {
+            const f2 g = ind::gelu2_x2(f2_make(v[o], v[o + 1]));
+            v[o] = f2_lo(g);
+            v[o + 1] = f2_hi(g);
+        }
         store_row32(S.X + mt * 128 * KIN, row, v);
     }
     tc::fence_smem_to_async();
@@ -201,7 +211,11 @@ __device__ __forceinline__ void indicator_tile(IndTile<Cfg>& S, const int mx, co
         tc::tmem_ld32(tmem + lane_base + 32 * mt, v);
         float zz = S.w.b3;
 #pragma unroll
-        for (int o = 0; o < NH; o++) zz = fmaf(S.w.w3h[o], ind::gelu2(v[o] + S.w.b2[o]), zz);
+        for (int o = 0; o < NH; o += 2) {
+            const f2 g = ind::gelu2_x2(f2_add(f2_make(v[o], v[o + 1]), f2_make(S.w.b2[o], S.w.b2[o + 1])));
+            zz = fmaf(S.w.w3h[o], f2_lo(g), zz);
+            zz = fmaf(S.w.w3h[o + 1], f2_hi(g), zz);
+        }
         const bool fl = fword[h] >= 0 && zz > zthr;
         if (fl) atomicOr(flags + fword[h], fbit[h]);
         const unsigned bal = __ballot_sync(0xffffffffu, fl);

@@ -315,7 +315,11 @@ __global__ void __launch_bounds__(Cfg::NT, 2) k_mhd_indicator(const __grid_const
             float v[32];
             tc::tmem_ld32(tmem + lane_base + 32 * mt, v);
 #pragma unroll
-            for (int o = 0; o < NH; o++) v[o] = ind::gelu2(v[o]);
+            for (int o = 0; o < NH; o += 2) {
+                const f2 g = ind::gelu2_x2(f2_make(v[o], v[o + 1]));
+                v[o] = f2_lo(g);
+                v[o + 1] = f2_hi(g);
+            }
             store_row32(S.X + mt * 128 * KIN, row, v);
         }
         tc::fence_smem_to_async();
@@ -339,7 +343,11 @@ __global__ void __launch_bounds__(Cfg::NT, 2) k_mhd_indicator(const __grid_const
             tc::tmem_ld32(tmem + lane_base + 32 * mt, v);
             float zz = S.w.b3;
 #pragma unroll
-            for (int o = 0; o < NH; o++) zz = fmaf(S.w.w3h[o], ind::gelu2(v[o] + S.w.b2[o]), zz);
+            for (int o = 0; o < NH; o += 2) {
+                const f2 g = ind::gelu2_x2(f2_add(f2_make(v[o], v[o + 1]), f2_make(S.w.b2[o], S.w.b2[o + 1])));
+                zz = fmaf(S.w.w3h[o], f2_lo(g), zz);
+                zz = fmaf(S.w.w3h[o + 1], f2_hi(g), zz);
+            }
             const bool fl = fword[h] >= 0 && zz > ia.zthr;
             if (fl) atomicOr(ia.flags + fword[h], fbit[h]);
             const unsigned bal = __ballot_sync(0xffffffffu, fl);

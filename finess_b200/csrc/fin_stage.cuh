@@ -243,7 +243,9 @@ __device__ __forceinline__ R weno_pair(R* up, R* um, R eps, R pw)
 {
     fence5(up);
     fence5(um);
-    R g = weno5<R, VER, P2>(up, eps, pw) + weno5<R, VER, P2>(um, eps, pw);
+    R g;
+    if constexpr (sizeof(R) == 4 && (P2 || VER == FIN_WENO_FD)) g = weno5_pair_x2<VER>(up, um, eps);   // f32x2 pairs
+    else g = weno5<R, VER, P2>(up, eps, pw) + weno5<R, VER, P2>(um, eps, pw);
     fence(g);
     return g;
 }

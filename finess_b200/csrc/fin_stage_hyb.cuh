@@ -57,13 +57,19 @@ struct HybSmem {
     static_assert(!SHARE || FHGH <= Cfg::STG_BYTES, "the face fluxes fit the staging tile");
 };
 
-// linear_face on (0.5 f, q) pairs: P points at stencil point 3.
+// linear_face on (0.5 f, q) pairs: P points at stencil point 3.  The f sums
+// and q differences run as f32x2 pairs, lane by lane the operations of
+//   sf = 37 (f2 + f3) + (-8 (f1 + f4) + (f0 + f5)),
+//   sq = 10 (q2 - q3) + (-5 (q1 - q4) + (q0 - q5)),
+// (x + y and x - y as fma(y, +-1, x): the same rounding).
 __device__ __forceinline__ float linear_face2(const float2* P, int str, float lah)
 {
-    const float2 a0 = P[-3 * str], a1 = P[-2 * str], a2 = P[-str], a3 = P[0], a4 = P[str], a5 = P[2 * str];
-    const float sf = fmaf(37.0f, a2.x + a3.x, fmaf(-8.0f, a1.x + a4.x, a0.x + a5.x));
-    const float sq = fmaf(10.0f, a2.y - a3.y, fmaf(-5.0f, a1.y - a4.y, a0.y - a5.y));
-    return fmaf(lah, sq, sf) * float(1.0 / 30.0);
+    const f2 pm = f2_make(1.0f, -1.0f), k1 = f2_make(-8.0f, -5.0f), k2 = f2_make(37.0f, 10.0f);
+    const f2 s05 = f2_fma(f2_of(P[2 * str]), pm, f2_of(P[-3 * str]));
+    const f2 s14 = f2_fma(f2_of(P[str]), pm, f2_of(P[-2 * str]));
+    const f2 s23 = f2_fma(f2_of(P[0]), pm, f2_of(P[-str]));
+    const f2 t = f2_fma(k2, s23, f2_fma(k1, s14, s05));
+    return fmaf(lah, f2_hi(t), f2_lo(t)) * float(1.0 / 30.0);
 }
 
 // Pass B of k_stage_hyb for one troubled face w (work-list index): the
@@ -107,7 +113,8 @@ __device__ __forceinline__ void hyb_troubled_face(int w, const float2* fqx, cons
     const float s1 = Min(unl - PL.w, ua - ca), s2 = Max(unr + PR.w, ua + ca);
     const float alpha = Max(isx ? ag1 : ag2, Max(fabsf(s1), fabsf(s2)));
     float fh[MEQN];
-    weno_char_flux<float, VER, P2>(ev, ash * alpha, eps, pw, pt, fh);
+    if constexpr (P2 || VER == FIN_WENO_FD) weno_char_flux_x2<VER>(ev, ash * alpha, pt, eps, fh);   // f32x2 pairs
+    else weno_char_flux<float, VER, P2>(ev, ash * alpha, eps, pw, pt, fh);
     if (isx) {
 #pragma unroll
         for (int m = 0; m < MEQN; m++) Fh[m * (TI + 1) * TJ + fi * TJ + fj] = fh[m];
