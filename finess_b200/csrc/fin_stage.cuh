@@ -31,6 +31,7 @@
 #pragma once
 #include "fin_device.cuh"
 #include "fin_tc.cuh"
+#include "fin_weno_face.cuh"
 
 namespace fin {
 
@@ -424,6 +425,18 @@ __device__ __forceinline__ void stage_tile(const StageArgs& a, const int i0, con
         const R lah = R(0.5) * Par<R>::ascale(a) * alpha;
         const typename Euler::Rows<R> rw = Euler::rows(ev);
         R fh[MEQN] = {R(0), R(0), R(0), R(0), R(0)};
+        if constexpr (sizeof(R) == 4 && (P2 || VER == FIN_WENO_FD)) {
+            // FP32: the split pairs and the paired reconstructions of
+            // weno_char_flux_x2 (f32x2), the same passes over the fields
+            auto pt = [&](int s, float* q, float* f) {
+                const int oq = qbase + (s - 3) * qstr, of = fbase + (s - 3) * fstr;
+                q[0] = qs[oq]; q[1] = qs[cn * PQ + oq]; q[2] = qs[ct * PQ + oq]; q[3] = qs[3 * PQ + oq];
+                q[4] = qs[4 * PQ + oq];
+                f[0] = fl[of]; f[1] = fl[cn * fplane + of]; f[2] = fl[ct * fplane + of]; f[3] = fl[3 * fplane + of];
+                f[4] = fl[4 * fplane + of];
+            };
+            weno_char_flux_x2<VER>(ev, lah, pt, eps, fh);
+        } else {
         {
             // pass 1: characteristic fields 0 and 4 (acoustic rows, shared tail)
             R p0[5], p4[5], m0[5], m4[5];
@@ -513,6 +526,7 @@ __device__ __forceinline__ void stage_tile(const StageArgs& a, const int i0, con
                 }
                 right_add<R>(ev, k == 0 ? 2 : 3, weno_pair<R, VER, P2>(up, um, eps, pw), fh);
             }
+        }
         }
         // Back to (rho, rho u, rho v, rho w, E) and store.
         if (isx) {
