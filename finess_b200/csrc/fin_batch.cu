@@ -477,7 +477,7 @@ __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wai
 template <class Cfg>
 __global__ void __launch_bounds__(Cfg::NT, 3)
 k_indicator_batch(BProb* pr, const int* act, const long long* tile0, const int* nact, const float* P, float gamma,
-                  float zthr, unsigned long long* count, unsigned long long* queue)
+                  float zthr, unsigned long long* count, unsigned long long* queue, int skip_const)
 {
     const int na = *nact;
     const long long total = tile0[na];
@@ -536,7 +536,7 @@ k_indicator_batch(BProb* pr, const int* act, const long long* tile0, const int* 
             prefetch(pn, in0, jn0);
         }
         BProb& b = pr[p];
-        indicator_tile<Cfg>(S, b.mx, b.my, gamma, zthr, b.flags, i0, j0, tmem, mma_phase);
+        indicator_tile<Cfg>(S, b.mx, b.my, gamma, zthr, b.flags, i0, j0, tmem, mma_phase, skip_const != 0);
         if (S.abort) {
             if (tid == 0) atomicOr(&b.status, 4u);
             break;
@@ -632,6 +632,7 @@ struct fin_batch {
     bool hyb;                   // created in the hybrid form with WENO-JS or WENO-Z
     float* mlpP;                // network parameters (null: none given yet, the plain FP32 form runs)
     float zthr;
+    bool ind_skip_const;
     BHyb hs;
     unsigned* dflags;           // every problem's flag masks
     unsigned long long* dcount; // troubled faces and faces the indicator ran on
@@ -779,7 +780,7 @@ int launch_indicator(fin_batch* b, QueueRef q, unsigned long long* counter)
         grid = 3 * nsm;
     }
     kern<<<grid, HybCfg::NT, smem, b->stream>>>(b->db, q.act, q.tile0, q.nact, b->mlpP, float(b->tmpl_p.gamma),
-                                                b->zthr, b->dcount, counter);
+                                                b->zthr, b->dcount, counter, b->ind_skip_const ? 1 : 0);
     BCK(cudaGetLastError());
     return FIN_OK;
 }
@@ -1219,6 +1220,7 @@ int fin_batch_set_indicator(fin_batch* b, const float* params, float z_threshold
     if (!b->mlpP) BCK(cudaMalloc(&b->mlpP, mlp::NPARAM * sizeof(float)));
     BCK(cudaMemcpyAsync(b->mlpP, params, mlp::NPARAM * sizeof(float), cudaMemcpyHostToDevice, b->stream));
     b->zthr = z_threshold;
+    b->ind_skip_const = ind::zero_row_logit(params) < double(z_threshold) - 0.05;   // as fin_set_indicator
     b->hs.judge_every = judge_every;
     b->hs.judge_tol = judge_tol;
     BCK(cudaMemcpyAsync(b->hb.data(), b->db, b->n * sizeof(BProb), cudaMemcpyDeviceToHost, b->stream));

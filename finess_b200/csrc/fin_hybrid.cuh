@@ -2,6 +2,8 @@
 // tcgen05 tensor cores -> a bit mask of troubled faces.  (The training-sample
 // extractor and the judge step's state comparison are in finess_b200.cu.)
 #pragma once
+#include <cmath>
+#include <cstring>
 #include "fin_indicator.cuh"
 #include "fin_mlp.cuh"
 #include "fin_stage.cuh"
@@ -21,6 +23,8 @@ struct IndicatorArgs {
     unsigned long long* count; // troubled faces (accumulated)
     int tma;                   // tm maps q (box (TJ+8) x (TI+6) x 5, as the stage kernel's)
     CUtensorMap tm;
+    int skip_const;            // the network's output for an all-zero feature row is known to be
+                               // "not troubled" (ind::zero_row_logit): constant stencils skip it
 };
 
 namespace ind {
@@ -81,6 +85,38 @@ __device__ __forceinline__ void mma_128x32x32(uint32_t tmem_d, const __nv_bfloat
     }
 }
 
+// The network's logit for an all-zero feature row (the features of a face
+// whose six stencil states are equal: every undivided difference is exactly
+// 0), restated on the host with the kernel's roundings: layer 1 is the BF16
+// bias alone, 2 gelu in BF16, layer 2 with the halved BF16 W2 in FP32, + b2,
+// 2 gelu, the halved output weights.  The host's tanh and the tensor core's
+// summation order differ from the device's by far less than the margin the
+// caller demands.
+inline float bf16_host(float x)
+{
+    uint32_t u;
+    memcpy(&u, &x, 4);
+    u += 0x7fffu + ((u >> 16) & 1u);
+    u &= 0xffff0000u;
+    float r;
+    memcpy(&r, &u, 4);
+    return r;
+}
+inline double zero_row_logit(const float* P)
+{
+    using namespace mlp;
+    auto g2 = [](double x) { return x * (1.0 + std::tanh(x * (double(GK0) + double(GK1) * x * x))); };
+    double a1[NH];
+    for (int o = 0; o < NH; o++) a1[o] = bf16_host(float(g2(bf16_host(P[OFF_B1 + o]))));
+    double z = P[OFF_B3];
+    for (int o = 0; o < NH; o++) {
+        double h = 0.0;
+        for (int i = 0; i < NH; i++) h += double(bf16_host(0.5f * bf16_host(P[OFF_W2 + o * NH + i]))) * a1[i];
+        z += double(0.5f * bf16_host(P[OFF_W3 + o])) * g2(h + P[OFF_B2 + o]);
+    }
+    return z;
+}
+
 }  // namespace ind
 
 // Shared memory of the indicator kernel for the stage kernel's tile shape.
@@ -113,10 +149,17 @@ struct IndTile {
 // warps 0-3 take matrices 0 and 1, warps 4-7 matrices 2 and 3.  Flagged
 // faces set their bits (the words are cleared before the run).  Sets S.abort
 // when a tensor-core wait ran out (uniform across the CTA on return).
+//
+// With skip_const, a warp whose 32 faces of a matrix all have six equal
+// stencil states (or are not owned) skips their features, activations and
+// output: their features are exactly 0, and the network's output for a zero
+// row is known to be "not troubled" (the caller checked
+// ind::zero_row_logit against the threshold with a margin), so the flags
+// are the same as with the network evaluated.
 template <class Cfg>
 __device__ __forceinline__ void indicator_tile(IndTile<Cfg>& S, const int mx, const int my, const float gamma,
                                                const float zthr, unsigned* flags, const int i0, const int j0,
-                                               const uint32_t tmem, uint32_t& mma_phase)
+                                               const uint32_t tmem, uint32_t& mma_phase, const bool skip_const = false)
 {
     using namespace mlp;
     constexpr int TI = Cfg::TI, TJ = Cfg::TJ, H = Cfg::H, RJ = Cfg::RJ, PQ = Cfg::RI * Cfg::RJ;
@@ -125,6 +168,7 @@ __device__ __forceinline__ void indicator_tile(IndTile<Cfg>& S, const int mx, co
     // ---- 2. features of the thread's two slots ----
     long long fword[2];   // flag word of the slot's face (-1: not owned)
     unsigned fbit[2];
+    bool wconst[2];       // the warp's 32 slots of matrix h are all constant stencils (or unowned)
     const int wx = flag_wx(my), wy = flag_wy(my);
 #pragma unroll 1
     for (int h = 0; h < 2; h++) {
@@ -142,13 +186,14 @@ __device__ __forceinline__ void indicator_tile(IndTile<Cfg>& S, const int mx, co
         bool own;
         if (isx) own = gj < my && gi <= mx && (fi < TI || gi == mx);
         else own = sl < 511 && gi < mx && gj <= my && (fj < TJ || gj == my);
+        float Q[6][MEQN];
+        bool cst = skip_const;   // an unowned slot counts as constant
         if (own) {
             fword[h] = isx ? (long long)gi * wx + (gj >> 5) : (long long)(mx + 1) * wx + (long long)gi * wy + (gj >> 5);
             fbit[h] = 1u << (gj & 31);
             const int cn = isx ? 1 : 2, ct = isx ? 2 : 1;
             const int base = isx ? (H + fi - 3) * RJ + (H + fj) : (H + fi) * RJ + (H + fj - 3);
             const int str = isx ? RJ : 1;
-            float Q[6][MEQN];
 #pragma unroll
             for (int st = 0; st < 6; st++) {
                 const int o = base + st * str;
@@ -158,7 +203,14 @@ __device__ __forceinline__ void indicator_tile(IndTile<Cfg>& S, const int mx, co
                 Q[st][3] = S.qs[3 * PQ + o];
                 Q[st][4] = S.qs[4 * PQ + o];
             }
-            ind::stencil_features<float>(Q, gamma, xr);
+#pragma unroll
+            for (int st = 1; st < 6; st++)
+#pragma unroll
+                for (int m = 0; m < MEQN; m++) cst = cst && Q[st][m] == Q[0][m];
+        }
+        wconst[h] = __all_sync(0xffffffffu, cst);   // every lane takes part
+        if (own) {
+            if (!wconst[h]) ind::stencil_features<float>(Q, gamma, xr);
             xr[NIN] = 1.0f;   // the layer-1 bias input
         }
         store_row32(S.X + mt * 128 * KIN, row, xr);
@@ -180,6 +232,7 @@ __device__ __forceinline__ void indicator_tile(IndTile<Cfg>& S, const int mx, co
 #pragma unroll 1
     for (int h = 0; h < 2; h++) {
         const int mt = 2 * (warp >> 2) + h, row = 32 * (warp & 3) + lane;
+        if (wconst[h]) continue;   // rows whose output is known: layer 2 sees their zero features
         float v[32];
         tc::tmem_ld32(tmem + lane_base + 32 * mt, v);
 #pragma unroll
@@ -207,6 +260,7 @@ __device__ __forceinline__ void indicator_tile(IndTile<Cfg>& S, const int mx, co
 #pragma unroll 1
     for (int h = 0; h < 2; h++) {
         const int mt = 2 * (warp >> 2) + h;
+        if (wconst[h]) continue;   // not troubled (the zero row's known output)
         float v[32];
         tc::tmem_ld32(tmem + lane_base + 32 * mt, v);
         float zz = S.w.b3;
@@ -287,7 +341,7 @@ __global__ void __launch_bounds__(Cfg::NT, 3) k_indicator(const __grid_constant_
         __syncthreads();
         if (S.abort) { pending = false; break; }
         pending = t + gridDim.x < ntiles ? issue(t + gridDim.x) : false;
-        indicator_tile<Cfg>(S, mx, my, a.gamma, a.zthr, a.flags, i0, j0, tmem, mma_phase);
+        indicator_tile<Cfg>(S, mx, my, a.gamma, a.zthr, a.flags, i0, j0, tmem, mma_phase, a.skip_const != 0);
         if (S.abort) break;
     }
     // a copy still in flight lands before the shared memory is released

@@ -101,6 +101,7 @@ struct fin_solver {
     unsigned* flags;        // troubled-face flag masks of the current step
     unsigned long long* ind_count;
     float zthr;
+    bool ind_skip_const;    // the network's zero-row output is "not troubled": constant stencils skip it
     int judge_every;
     double judge_tol;
     long long hstep, judges, reverts, troubled_last, faces;
@@ -640,6 +641,7 @@ int launch_indicator(fin_solver* s, int buf)
     ia.flags = s->flags;
     ia.status = s->status;
     ia.count = s->ind_count;
+    ia.skip_const = s->ind_skip_const ? 1 : 0;
     ia.tma = 0;
     if (s->tma_ok) {
         ia.tma = 1;
@@ -1430,6 +1432,10 @@ int fin_set_indicator(fin_solver* s, const float* params, float z_threshold, int
     CK(cudaMemcpyAsync(s->mlpP, params, mlp::NPARAM * sizeof(float), cudaMemcpyHostToDevice, s->stream));
     CK(cudaStreamSynchronize(s->stream));
     s->zthr = z_threshold;
+    // A face whose six stencil states are equal has all-zero features; when
+    // the network's output for that row lies clearly below the threshold,
+    // the indicator skips such faces (the same flags, less work).
+    s->ind_skip_const = ind::zero_row_logit(params) < double(z_threshold) - 0.05;
     s->judge_every = judge_every;
     s->judge_tol = judge_tol;
     s->hyb_off = 0;
