@@ -1469,6 +1469,17 @@ int fin_hybrid_stats(fin_solver* s, long long* troubled_faces, long long* faces,
     return FIN_OK;
 }
 
+int fin_hybrid_flags(fin_solver* s, unsigned* words_host, size_t nwords)
+{
+    if (!s || !words_host) return set_err(FIN_ERR_ARG, "null argument");
+    if (!s->flags) return set_err(FIN_ERR_ARG, "the solver holds no indicator flags");
+    const size_t n = flag_words(s->p.mx, s->p.my);
+    if (nwords < n) return set_err(FIN_ERR_SIZE, "flag buffer too small");
+    CK(cudaMemcpyAsync(words_host, s->flags, n * sizeof(unsigned), cudaMemcpyDeviceToHost, s->stream));
+    CK(cudaStreamSynchronize(s->stream));
+    return FIN_OK;
+}
+
 int fin_face_samples(fin_solver* s, long long offset, long long stride, long long max_n, float* X_host,
                      unsigned char* y_host, long long* n_out)
 {

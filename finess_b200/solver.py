@@ -223,6 +223,22 @@ class Solver:
         _check(self.lib.fin_hybrid_stats(self.h, *[C.byref(x) for x in v]))
         return {"troubled_faces": v[0].value, "faces": v[1].value, "judges": v[2].value, "reverts": v[3].value}
 
+    def hybrid_flags(self):
+        """Troubled-face flags of the last indicator pass, one bool per face:
+        x faces (mx+1) x my (i-major), then y faces mx x (my+1)."""
+        p = self.p
+        wx, wy = (p.my + 31) >> 5, (p.my + 32) >> 5
+        n = (p.mx + 1) * wx + p.mx * wy
+        w = np.zeros(n, dtype=np.uint32)
+        self.lib.fin_hybrid_flags.argtypes = [C.c_void_p, np.ctypeslib.ndpointer(np.uint32, flags="C_CONTIGUOUS"),
+                                              C.c_size_t]
+        self.lib.fin_hybrid_flags.restype = C.c_int
+        _check(self.lib.fin_hybrid_flags(self.h, w, n))
+        bits = np.unpackbits(w.view(np.uint8), bitorder="little")
+        fx = bits[:(p.mx + 1) * wx * 32].reshape(p.mx + 1, wx * 32)[:, :p.my]
+        fy = bits[(p.mx + 1) * wx * 32:].reshape(p.mx, wy * 32)[:, :p.my + 1]
+        return np.concatenate([fx.ravel(), fy.ravel()]).astype(bool)
+
     def face_samples(self, offset=0, stride=1, max_n=None):
         """Indicator features (n x 20) and WENO-JS labels of the current state's faces."""
         p = self.p

@@ -346,6 +346,11 @@ int fin_set_indicator_every(fin_solver* s, int every);
 /* Troubled faces flagged in the last indicator pass, faces per pass, judge
  * steps run and steps reverted. */
 int fin_hybrid_stats(fin_solver* s, long long* troubled_faces, long long* faces, long long* judges, long long* reverts);
+/* The troubled-face bit masks of the last indicator pass (no reference
+ * counterpart): x faces (rows 0..mx, ceil(my/32) words per row, bit b of word
+ * k = column 32k+b), then y faces (rows 0..mx-1, ceil((my+1)/32) words per
+ * row); nwords must be at least that total. */
+int fin_hybrid_flags(fin_solver* s, unsigned* words_host, size_t nwords);
 /* Training samples of the current state: features (20 floats) and labels of
  * faces offset, offset + stride, ... (x faces, then y faces), at most max_n. */
 int fin_face_samples(fin_solver* s, long long offset, long long stride, long long max_n, float* X_host,

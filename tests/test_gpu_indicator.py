@@ -136,6 +136,42 @@ def test_indicator_flags_match_oracle_network(oracle, case):
     assert abs(st["troubled_faces"] - n_oracle) <= max(near, 2), (st, n_oracle, near)
 
 
+@pytest.mark.parametrize("kind", ["riemann_init", "random"])
+def test_indicator_flags_face_by_face(oracle, kind):
+    """Face by face, the device's flags equal the oracle network's decisions
+    on the oracle's FP64 features, except faces within rounding of the
+    threshold; faces whose stencil is constant (features exactly 0, which the
+    kernel skips when the network's zero-row output is below the threshold)
+    are never flagged."""
+    from finess_b200.indicator import DEFAULT_WEIGHTS
+    from finess_b200.solver import Solver
+    import mlp_oracle as M
+    W = np.load(DEFAULT_WEIGHTS)
+    params, zthr = W["params"], float(W["z_threshold"])
+    if kind == "riemann_init":
+        p = P.riemann_params(n=70, weno=FIN_WENO_JS)
+        p.my = 53
+        q = P.riemann_init(p)
+    else:
+        p, q = _cases()[0]
+    q = oracle.set_bnd(p, q)
+    Xo, _ = oracle.face_samples(p, q)
+    zo = M.forward_emulated(params, Xo)
+    ph = p.copy(); ph.precision = FIN_PREC_HYBRID
+    with Solver(ph) as a:
+        a.set_indicator(params, zthr, judge_every=0)
+        a.set_state(q)
+        a.step_fixed(1e-5)
+        fl = a.hybrid_flags()
+    assert fl.size == len(Xo)
+    const = np.all(Xo == 0.0, axis=1)
+    if kind == "riemann_init":
+        assert const.mean() > 0.5
+    assert not np.any(fl[const])
+    sure = np.abs(zo - zthr) >= 0.05
+    assert np.array_equal(fl[sure], (zo > zthr)[sure])
+
+
 def test_hybrid_after_revert_continues_on_the_right_buffers():
     """A revert swaps the hybrid attempt's buffer with the full-WENO one; the
     hybrid steps after it must read the swapped buffers (their TMA maps travel
