@@ -570,13 +570,13 @@ def main():
             raise RuntimeError(f"{tag}: only {nst} steps taken")
         dev_ms = max_over_ranks(dev_ms)
         kms, kl = s.kernel_time()
+        ims, il = s.indicator_time() if tag == "hybrid" else (0.0, 0)
         s.set_kernel_timing(False)
         r = {"value": ws * cells * args.steps / (dev_ms * 1e-3), "ms_per_step": dev_ms / args.steps,
              "stage_kernel_ms": kms / kl, "launches": s.launch_count() - l0, "kernel_stats": (kms, kl),
              "warmup_steps": nw, "warmup_ms": warm_ms}
         if tag == "hybrid":
             st = s.hybrid_stats()
-            ims, il = s.indicator_time()
             r["indicator"] = {**st, "kernel_ms": ims / il if il else None, "launches_in_window": il,
                               "every": HYB_EVERY, "judge_every": HYB_JUDGE_EVERY,
                               "judges_in_window": st["judges"] - st0["judges"]}
