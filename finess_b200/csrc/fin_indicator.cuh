@@ -17,6 +17,7 @@
 // normalised up to O(1).
 #pragma once
 #include "fin_device.cuh"
+#include "fin_weno_face.cuh"
 
 namespace fin {
 namespace ind {
@@ -59,14 +60,31 @@ __device__ __forceinline__ void stencil_features(const R (&Q)[6][MEQN], R gamma,
     const typename Euler::Eig<R> e = Euler::eig(gamma, Qa);
     const typename Euler::Rows<R> rw = Euler::rows(e);
     R w[4][6];
+    if constexpr (sizeof(R) == 4) {
+        // FP32: two stencil points per f32x2 pair (the same rows lane by lane)
 #pragma unroll
-    for (int s = 0; s < 6; s++) {
-        R w0, w4;
-        Euler::left04(e, rw, Q[s], w0, w4);
-        w[0][s] = w0;
-        w[1][s] = Euler::left1(e, rw, Q[s]);
-        w[2][s] = Q[s][2] - e.u2 * Q[s][0];
-        w[3][s] = w4;
+        for (int s = 0; s < 6; s += 2) {
+            f2 v[MEQN], w0, w4;
+#pragma unroll
+            for (int m = 0; m < MEQN; m++) v[m] = f2_make(Q[s][m], Q[s + 1][m]);
+            left04_x2(e, rw, v, w0, w4);
+            const f2 w1 = left1_x2(e, rw, v);
+            const f2 w2 = f2_fma(f2_splat(-e.u2), v[0], v[2]);
+            w[0][s] = f2_lo(w0); w[0][s + 1] = f2_hi(w0);
+            w[1][s] = f2_lo(w1); w[1][s + 1] = f2_hi(w1);
+            w[2][s] = f2_lo(w2); w[2][s + 1] = f2_hi(w2);
+            w[3][s] = f2_lo(w4); w[3][s + 1] = f2_hi(w4);
+        }
+    } else {
+#pragma unroll
+        for (int s = 0; s < 6; s++) {
+            R w0, w4;
+            Euler::left04(e, rw, Q[s], w0, w4);
+            w[0][s] = w0;
+            w[1][s] = Euler::left1(e, rw, Q[s]);
+            w[2][s] = Q[s][2] - e.u2 * Q[s][0];
+            w[3][s] = w4;
+        }
     }
 #pragma unroll
     for (int k = 0; k < 4; k++) {
