@@ -894,9 +894,14 @@ __global__ void __launch_bounds__(Cfg::NT, Cfg::MINB) k_mhd_stage(const __grid_c
             if (sx <= 1e300) cs_x = Max(cs_x, sx);
             if (sy <= 1e300) cs_y = Max(cs_y, sy);
         }
-        const double ax = fabs(u1), ay = fabs(u2);
-        if (ax <= 1e300) hx = Max(hx, ax); else nonfinite = true;
-        if (ay <= 1e300) hy = Max(hy, ay); else nonfinite = true;
+        if (a.hj_out) {
+            // the HJ speeds of q_out, only where a stage produces a state (a
+            // right-hand-side evaluation writes L there, whose density
+            // entry may be exactly 0)
+            const double ax = fabs(u1), ay = fabs(u2);
+            if (ax <= 1e300) hx = Max(hx, ax); else nonfinite = true;
+            if (ay <= 1e300) hy = Max(hy, ay); else nonfinite = true;
+        }
     }
 
     // ---- block reductions, one atomic per maximum ----
