@@ -60,7 +60,10 @@ __device__ __forceinline__ void stencil_features(const R (&Q)[6][MEQN], R gamma,
     const typename Euler::Eig<R> e = Euler::eig(gamma, Qa);
     const typename Euler::Rows<R> rw = Euler::rows(e);
     R w[4][6];
-    if constexpr (sizeof(R) == 4) {
+#ifndef FIN_X2_FEAT
+#define FIN_X2_FEAT 1
+#endif
+    if constexpr (sizeof(R) == 4 && FIN_X2_FEAT) {
         // FP32: two stencil points per f32x2 pair (the same rows lane by lane)
 #pragma unroll
         for (int s = 0; s < 6; s += 2) {

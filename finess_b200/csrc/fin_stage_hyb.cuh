@@ -62,8 +62,17 @@ struct HybSmem {
 //   sf = 37 (f2 + f3) + (-8 (f1 + f4) + (f0 + f5)),
 //   sq = 10 (q2 - q3) + (-5 (q1 - q4) + (q0 - q5)),
 // (x + y and x - y as fma(y, +-1, x): the same rounding).
+#ifndef FIN_X2_LINEAR
+#define FIN_X2_LINEAR 1
+#endif
 __device__ __forceinline__ float linear_face2(const float2* P, int str, float lah)
 {
+#if !FIN_X2_LINEAR
+    const float2 a0 = P[-3 * str], a1 = P[-2 * str], a2 = P[-str], a3 = P[0], a4 = P[str], a5 = P[2 * str];
+    const float sf = fmaf(37.0f, a2.x + a3.x, fmaf(-8.0f, a1.x + a4.x, a0.x + a5.x));
+    const float sq = fmaf(10.0f, a2.y - a3.y, fmaf(-5.0f, a1.y - a4.y, a0.y - a5.y));
+    return fmaf(lah, sq, sf) * float(1.0 / 30.0);
+#endif
     const f2 pm = f2_make(1.0f, -1.0f), k1 = f2_make(-8.0f, -5.0f), k2 = f2_make(37.0f, 10.0f);
     const f2 s05 = f2_fma(f2_of(P[2 * str]), pm, f2_of(P[-3 * str]));
     const f2 s14 = f2_fma(f2_of(P[str]), pm, f2_of(P[-2 * str]));
