@@ -84,10 +84,29 @@ __device__ __forceinline__ float linear_face2(const float2* P, int str, float la
 // Pass B of k_stage_hyb for one troubled face w (work-list index): the
 // LLF speed again, the face-average eigensystem and the full characteristic
 // WENO flux, stored into Fh / Gh.
+// With parts < 3 (the face split over two threads) fh receives the partial
+// flux of the selected fields (weno_char_flux_x2's parts) and nothing is
+// stored; the caller adds the halves and stores them (hyb_store_face).
+template <class Cfg>
+__device__ __forceinline__ void hyb_store_face(int w, const float* fh, float* Fh, float* Gh)
+{
+    constexpr int TI = Cfg::TI, TJ = Cfg::TJ;
+    if (w < Cfg::NFX) {
+        const int fi = w / TJ, fj = w - fi * TJ;
+#pragma unroll
+        for (int m = 0; m < MEQN; m++) Fh[m * (TI + 1) * TJ + fi * TJ + fj] = fh[m];
+    } else {
+        const int v = w - Cfg::NFX, fi = v / (TJ + 1), fj = v - fi * (TJ + 1);
+        const float o[MEQN] = {fh[0], fh[2], fh[1], fh[3], fh[4]};
+#pragma unroll
+        for (int m = 0; m < MEQN; m++) Gh[m * TI * (TJ + 1) + fi * (TJ + 1) + fj] = o[m];
+    }
+}
+
 template <int VER, bool P2, class Cfg>
 __device__ __forceinline__ void hyb_troubled_face(int w, const float2* fqx, const float2* fqy, const float4* prim4,
                                                float* Fh, float* Gh, float gam, float eps, float pw, float ash,
-                                               float ag1, float ag2)
+                                               float ag1, float ag2, int parts = 3, float* fh_part = nullptr)
 {
     constexpr int TI = Cfg::TI, TJ = Cfg::TJ, H = Cfg::H, RI = Cfg::RI, RJ = Cfg::RJ;
     constexpr int XPL = RI * TJ, YPL = TI * RJ;
@@ -122,8 +141,13 @@ __device__ __forceinline__ void hyb_troubled_face(int w, const float2* fqx, cons
     const float s1 = Min(unl - PL.w, ua - ca), s2 = Max(unr + PR.w, ua + ca);
     const float alpha = Max(isx ? ag1 : ag2, Max(fabsf(s1), fabsf(s2)));
     float fh[MEQN];
-    if constexpr (P2 || VER == FIN_WENO_FD) weno_char_flux_x2<VER>(ev, ash * alpha, pt, eps, fh);   // f32x2 pairs
+    if constexpr (P2 || VER == FIN_WENO_FD) weno_char_flux_x2<VER>(ev, ash * alpha, pt, eps, fh, parts);   // f32x2
     else weno_char_flux<float, VER, P2>(ev, ash * alpha, eps, pw, pt, fh);
+    if (parts != 3) {
+#pragma unroll
+        for (int m = 0; m < MEQN; m++) fh_part[m] = fh[m];
+        return;
+    }
     if (isx) {
 #pragma unroll
         for (int m = 0; m < MEQN; m++) Fh[m * (TI + 1) * TJ + fi * TJ + fj] = fh[m];
@@ -324,9 +348,34 @@ __device__ __forceinline__ void stage_hyb_tile(const StageArgs& a, const int i0,
         {
             const int nt = *ntrb;
             const float agx[2] = {ag1, ag2};
+            if constexpr (P2 || VER == FIN_WENO_FD) {
+                // two adjacent lanes per troubled face: the even lane takes
+                // fields 0 and 4, the odd lane fields 1, 2 and 3; the halves
+                // are added (even + odd, the same order in both lanes) and
+                // the even lane stores the face.  The loop bound is uniform
+                // over the warp, so every lane reaches the shuffles.
 #pragma unroll 1
-            for (int k = tid; k < nt; k += NT)
-                hyb_troubled_face<VER, P2, Cfg>(tlist[k], fqx, fqy, prim4, Fh, Gh, gam, eps, pw, ash, agx[0], agx[1]);
+                for (int base = tid & ~31; base < 2 * nt; base += NT) {
+                    const int k2 = base + lane;
+                    const bool act = k2 < 2 * nt;
+                    float fh[MEQN] = {0.0f, 0.0f, 0.0f, 0.0f, 0.0f};
+                    const int w = act ? tlist[k2 >> 1] : 0;
+                    if (act)
+                        hyb_troubled_face<VER, P2, Cfg>(w, fqx, fqy, prim4, Fh, Gh, gam, eps, pw, ash, agx[0], agx[1],
+                                                        (k2 & 1) ? 2 : 1, fh);
+#pragma unroll
+                    for (int m = 0; m < MEQN; m++) {
+                        const float o = __shfl_xor_sync(0xffffffffu, fh[m], 1);
+                        fh[m] = (k2 & 1) ? o + fh[m] : fh[m] + o;
+                    }
+                    if (act && !(k2 & 1)) hyb_store_face<Cfg>(w, fh, Fh, Gh);
+                }
+            } else {
+#pragma unroll 1
+                for (int k = tid; k < nt; k += NT)
+                    hyb_troubled_face<VER, P2, Cfg>(tlist[k], fqx, fqy, prim4, Fh, Gh, gam, eps, pw, ash, agx[0],
+                                                    agx[1]);
+            }
         }
         __syncthreads();
         // ---- phase 3: flux difference (ConstructL.cpp:396-398), update

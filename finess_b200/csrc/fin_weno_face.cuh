@@ -168,9 +168,12 @@ __device__ __forceinline__ f2 left1_x2(const Euler::Eig<float>& e, const Euler::
     return f2_mul(a, f2_splat(e.inv_d2));
 }
 
+// parts: bit 0 = pass 1 (fields 0 and 4), bit 1 = passes 2 and 3 (fields 1,
+// 2, 3); fh receives the sum of the selected fields' right projections (a
+// face split over two threads adds the two partial fluxes afterwards).
 template <int VER, class Pt>
 __device__ __forceinline__ void weno_char_flux_x2(const Euler::Eig<float>& ev, float lah, const Pt& pt, float eps,
-                                                  float* fh)
+                                                  float* fh, int parts = 3)
 {
     const Euler::Rows<float> rw = Euler::rows(ev);
     const f2 pmla = f2_make(lah, -lah);
@@ -183,7 +186,7 @@ __device__ __forceinline__ void weno_char_flux_x2(const Euler::Eig<float>& ev, f
 #pragma unroll
         for (int m = 0; m < MEQN; m++) v[m] = f2_fma(pmla, f2_splat(q[m]), f2_splat(f[m]));
     };
-    {
+    if (parts & 1) {
         // pass 1: fields 0 and 4
         float p0[5], p4[5], m0[5], m4[5];
 #pragma unroll
@@ -206,7 +209,7 @@ __device__ __forceinline__ void weno_char_flux_x2(const Euler::Eig<float>& ev, f
             right_add_f<float>(ev, k == 0 ? 0 : 4, weno_pair_f<float, VER, true>(up, um, eps, 2.0f), fh);
         }
     }
-    {
+    if (parts & 2) {
         // pass 2: field 1
         float p1[5], m1[5];
 #pragma unroll
@@ -220,7 +223,7 @@ __device__ __forceinline__ void weno_char_flux_x2(const Euler::Eig<float>& ev, f
         }
         right_add_f<float>(ev, 1, weno_pair_f<float, VER, true>(p1, m1, eps, 2.0f), fh);
     }
-    {
+    if (parts & 2) {
         // pass 3: fields 2 and 3 (v_t - u2 v0, v_w - u3 v0)
         float p2[5], p3[5], m2[5], m3[5];
 #pragma unroll

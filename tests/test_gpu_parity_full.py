@@ -14,13 +14,17 @@ built.
   x and periodic in y: one ConstructL and one SSP-RK3 step at 1e-12;
 * ideal MHD Orszag-Tang, 2048^2, WENO5-JS, periodic, from the reference's own
   QinitFunc: one ConstructL (with the A3 Hamilton-Jacobi right-hand side) and
-  one SSP-RK3 step with constrained transport at 1e-12.
+  one SSP-RK3 step with constrained transport at 1e-12 (ConstructL: at 1e-12
+  or the reference's own one-ulp sensitivity at this size, whichever is
+  larger).
 
 Each test records its measured error: with FIN_PARITY_REPORT set to a file
 path, one JSON line per measurement is appended there.
 """
 import json
 import os
+
+import numpy as np
 
 import pytest
 
@@ -135,8 +139,21 @@ def test_orszag_tang2048_construct_l_and_step():
     ea = rel_linf(interior(p, Lag), interior(p, Lar))
     eq = rel_linf(interior(p, q1g), interior(p, q1r))
     eaux = rel_linf(interior(p, a1g), interior(p, a1r))
-    _report("orszag_tang2048_js", construct_l_rel_linf=eL, hj_rel_linf=ea, smax_rel_linf=rel_linf(smg, smr),
-            step_rel_linf=eq, step_aux_rel_linf=eaux, dt=dt)
-    assert eL <= TOL_STEP and ea <= TOL_STEP
+    # The reference's own sensitivity at this size: its ConstructL of the
+    # state with every interior value moved by one ulp (up or down at
+    # random).  The initial density is uniform, so rho's right-hand side is
+    # rounding noise and the 8 x 8 projections meet degenerate states on
+    # whole grid lines; one ulp of input moves the reference's L by ~2e-12.
+    rng = np.random.default_rng(1)
+    qp = q.copy()
+    I = qp[p.mbc:p.mbc + p.mx, p.mbc:p.mbc + p.my]
+    I[...] = np.where(rng.random(I.shape) < 0.5, np.nextafter(I, np.inf), np.nextafter(I, -np.inf))
+    qp, auxp = ref.set_bnd(p, qp, aux)
+    Lp, _ = ref.construct_l(p, qp, auxp)
+    sens = rel_linf(interior(p, Lp), interior(p, Lr))
+    _report("orszag_tang2048_js", construct_l_rel_linf=eL, reference_one_ulp_sensitivity=sens, hj_rel_linf=ea,
+            smax_rel_linf=rel_linf(smg, smr), step_rel_linf=eq, step_aux_rel_linf=eaux, dt=dt)
+    assert eL <= max(TOL_STEP, sens)
+    assert ea <= TOL_STEP
     assert rel_linf(smg, smr) <= TOL_STEP
     assert eq <= TOL_STEP and eaux <= TOL_STEP

@@ -92,8 +92,13 @@ def test_reference_steppers_over_device_parts(partslib, path):
 
 @pytest.mark.parametrize("path", golden_cases("intr_"))
 def test_relinked_construct_integrated_r(partslib, path):
+    from finess_b200._abi import FIN_TS_LXW, FIN_TS_MD
     g = load_golden(path)
-    p = g["p"]
+    p = g["p"].copy()
+    # the relinked application's stepper: Lax-Wendroff for time_order 2 or 3
+    # (FinSolveMD takes orders 4 and 5); the integrated flux depends on the
+    # order alone
+    p.time_stepping_method = FIN_TS_LXW if p.time_order <= 3 else FIN_TS_MD
     F, G = partslib.construct_integrated_r(p, float(g["dt"]), g["q"])
     mb = p.mbc
     fr = (slice(mb - 3, mb + p.mx + 3), slice(mb - 3, mb + p.my + 3))
