@@ -207,6 +207,11 @@ __device__ __forceinline__ R linear_face(const R* f, int fstr, const R* q, int q
 #define FIN_MINB_F32 3
 #endif
 template <class R> struct MinBlocks { static constexpr int value = FIN_MINB_F64; };
+// FP64 face body: fields 0, 4 and 1 in one sweep of the stencil (1) or the
+// three passes of the register-lean form (0).
+#ifndef FIN_F64_MERGE
+#define FIN_F64_MERGE 0
+#endif
 template <> struct MinBlocks<float> { static constexpr int value = FIN_MINB_F32; };
 
 // Scalar parameters read from kernel-parameter space where they are used
@@ -436,6 +441,68 @@ __device__ __forceinline__ void stage_tile(const StageArgs& a, const int i0, con
                 f[4] = fl[4 * fplane + of];
             };
             weno_char_flux_x2<VER>(ev, lah, pt, eps, fh);
+        } else if (FIN_F64_MERGE && sizeof(R) == 8) {
+            // fields 0, 4 and 1 in one sweep of the stencil (left014 shares
+            // the acoustic rows' tail), then fields 2 and 3; the right
+            // projections are added in the same order as the three passes below
+            R p0[5], p4[5], m0[5], m4[5], p1[5], m1[5];
+#pragma unroll
+            for (int s = 0; s < 6; s++) {
+                asm volatile("" ::: "memory");
+                const int oq = qbase + (s - 3) * qstr, of = fbase + (s - 3) * fstr;
+                const R q0 = qs[oq], qn = qs[cn * PQ + oq], qt = qs[ct * PQ + oq], qw = qs[3 * PQ + oq], qe = qs[4 * PQ + oq];
+                const R f0 = fl[of], fn = fl[cn * fplane + of], ft = fl[ct * fplane + of], fw = fl[3 * fplane + of],
+                        fe = fl[4 * fplane + of];
+                if (s < 5) {
+                    const R v[MEQN] = {f0 + lah * q0, fn + lah * qn, ft + lah * qt, fw + lah * qw, fe + lah * qe};
+                    Euler::left014(ev, rw, v, p0[s], p1[s], p4[s]);
+                }
+                if (s > 0) {
+                    const R v[MEQN] = {f0 - lah * q0, fn - lah * qn, ft - lah * qt, fw - lah * qw, fe - lah * qe};
+                    Euler::left014(ev, rw, v, m0[5 - s], m1[5 - s], m4[5 - s]);
+                }
+            }
+#pragma unroll 1
+            for (int k = 0; k < 3; k++) {
+                R up[5], um[5];
+#pragma unroll
+                for (int t = 0; t < 5; t++) {
+                    up[t] = k == 0 ? p0[t] : (k == 1 ? p4[t] : p1[t]);
+                    um[t] = k == 0 ? m0[t] : (k == 1 ? m4[t] : m1[t]);
+                }
+                right_add<R>(ev, k == 0 ? 0 : (k == 1 ? 4 : 1), weno_pair<R, VER, P2>(up, um, eps, pw), fh);
+            }
+            {
+                // fields 2 and 3 (rows v_t - u2 v0 and v_w - u3 v0)
+                R p2[5], p3[5], m2[5], m3[5];
+#pragma unroll
+                for (int s = 0; s < 6; s++) {
+                    asm volatile("" ::: "memory");
+                    const int oq = qbase + (s - 3) * qstr, of = fbase + (s - 3) * fstr;
+                    const R q0 = qs[oq], qt = qs[ct * PQ + oq], qw = qs[3 * PQ + oq];
+                    const R f0 = fl[of], ft = fl[ct * fplane + of], fw = fl[3 * fplane + of];
+                    if (s < 5) {
+                        const R v0 = f0 + lah * q0;
+                        p2[s] = (ft + lah * qt) - ev.u2 * v0;
+                        p3[s] = (fw + lah * qw) - ev.u3 * v0;
+                    }
+                    if (s > 0) {
+                        const R v0 = f0 - lah * q0;
+                        m2[5 - s] = (ft - lah * qt) - ev.u2 * v0;
+                        m3[5 - s] = (fw - lah * qw) - ev.u3 * v0;
+                    }
+                }
+#pragma unroll 1
+                for (int k = 0; k < 2; k++) {
+                    R up[5], um[5];
+#pragma unroll
+                    for (int t = 0; t < 5; t++) {
+                        up[t] = k == 0 ? p2[t] : p3[t];
+                        um[t] = k == 0 ? m2[t] : m3[t];
+                    }
+                    right_add<R>(ev, k == 0 ? 2 : 3, weno_pair<R, VER, P2>(up, um, eps, pw), fh);
+                }
+            }
         } else {
         {
             // pass 1: characteristic fields 0 and 4 (acoustic rows, shared tail)
