@@ -62,51 +62,35 @@ struct HybSmem {
 //   sf = 37 (f2 + f3) + (-8 (f1 + f4) + (f0 + f5)),
 //   sq = 10 (q2 - q3) + (-5 (q1 - q4) + (q0 - q5)),
 // (x + y and x - y as fma(y, +-1, x): the same rounding).
+// The f32x2 form measured 1 % slower than the scalar one (B200, 4096^2,
+// mid-run state), so the scalar form is built.
 #ifndef FIN_X2_LINEAR
-#define FIN_X2_LINEAR 1
+#define FIN_X2_LINEAR 0
 #endif
 __device__ __forceinline__ float linear_face2(const float2* P, int str, float lah)
 {
-#if !FIN_X2_LINEAR
-    const float2 a0 = P[-3 * str], a1 = P[-2 * str], a2 = P[-str], a3 = P[0], a4 = P[str], a5 = P[2 * str];
-    const float sf = fmaf(37.0f, a2.x + a3.x, fmaf(-8.0f, a1.x + a4.x, a0.x + a5.x));
-    const float sq = fmaf(10.0f, a2.y - a3.y, fmaf(-5.0f, a1.y - a4.y, a0.y - a5.y));
-    return fmaf(lah, sq, sf) * float(1.0 / 30.0);
-#endif
+#if FIN_X2_LINEAR
     const f2 pm = f2_make(1.0f, -1.0f), k1 = f2_make(-8.0f, -5.0f), k2 = f2_make(37.0f, 10.0f);
     const f2 s05 = f2_fma(f2_of(P[2 * str]), pm, f2_of(P[-3 * str]));
     const f2 s14 = f2_fma(f2_of(P[str]), pm, f2_of(P[-2 * str]));
     const f2 s23 = f2_fma(f2_of(P[0]), pm, f2_of(P[-str]));
     const f2 t = f2_fma(k2, s23, f2_fma(k1, s14, s05));
     return fmaf(lah, f2_hi(t), f2_lo(t)) * float(1.0 / 30.0);
+#else
+    const float2 a0 = P[-3 * str], a1 = P[-2 * str], a2 = P[-str], a3 = P[0], a4 = P[str], a5 = P[2 * str];
+    const float sf = fmaf(37.0f, a2.x + a3.x, fmaf(-8.0f, a1.x + a4.x, a0.x + a5.x));
+    const float sq = fmaf(10.0f, a2.y - a3.y, fmaf(-5.0f, a1.y - a4.y, a0.y - a5.y));
+    return fmaf(lah, sq, sf) * float(1.0 / 30.0);
+#endif
 }
 
 // Pass B of k_stage_hyb for one troubled face w (work-list index): the
 // LLF speed again, the face-average eigensystem and the full characteristic
 // WENO flux, stored into Fh / Gh.
-// With parts < 3 (the face split over two threads) fh receives the partial
-// flux of the selected fields (weno_char_flux_x2's parts) and nothing is
-// stored; the caller adds the halves and stores them (hyb_store_face).
-template <class Cfg>
-__device__ __forceinline__ void hyb_store_face(int w, const float* fh, float* Fh, float* Gh)
-{
-    constexpr int TI = Cfg::TI, TJ = Cfg::TJ;
-    if (w < Cfg::NFX) {
-        const int fi = w / TJ, fj = w - fi * TJ;
-#pragma unroll
-        for (int m = 0; m < MEQN; m++) Fh[m * (TI + 1) * TJ + fi * TJ + fj] = fh[m];
-    } else {
-        const int v = w - Cfg::NFX, fi = v / (TJ + 1), fj = v - fi * (TJ + 1);
-        const float o[MEQN] = {fh[0], fh[2], fh[1], fh[3], fh[4]};
-#pragma unroll
-        for (int m = 0; m < MEQN; m++) Gh[m * TI * (TJ + 1) + fi * (TJ + 1) + fj] = o[m];
-    }
-}
-
 template <int VER, bool P2, class Cfg>
 __device__ __forceinline__ void hyb_troubled_face(int w, const float2* fqx, const float2* fqy, const float4* prim4,
                                                float* Fh, float* Gh, float gam, float eps, float pw, float ash,
-                                               float ag1, float ag2, int parts = 3, float* fh_part = nullptr)
+                                               float ag1, float ag2)
 {
     constexpr int TI = Cfg::TI, TJ = Cfg::TJ, H = Cfg::H, RI = Cfg::RI, RJ = Cfg::RJ;
     constexpr int XPL = RI * TJ, YPL = TI * RJ;
@@ -141,13 +125,8 @@ __device__ __forceinline__ void hyb_troubled_face(int w, const float2* fqx, cons
     const float s1 = Min(unl - PL.w, ua - ca), s2 = Max(unr + PR.w, ua + ca);
     const float alpha = Max(isx ? ag1 : ag2, Max(fabsf(s1), fabsf(s2)));
     float fh[MEQN];
-    if constexpr (P2 || VER == FIN_WENO_FD) weno_char_flux_x2<VER>(ev, ash * alpha, pt, eps, fh, parts);   // f32x2
+    if constexpr (P2 || VER == FIN_WENO_FD) weno_char_flux_x2<VER>(ev, ash * alpha, pt, eps, fh);   // f32x2 pairs
     else weno_char_flux<float, VER, P2>(ev, ash * alpha, eps, pw, pt, fh);
-    if (parts != 3) {
-#pragma unroll
-        for (int m = 0; m < MEQN; m++) fh_part[m] = fh[m];
-        return;
-    }
     if (isx) {
 #pragma unroll
         for (int m = 0; m < MEQN; m++) Fh[m * (TI + 1) * TJ + fi * TJ + fj] = fh[m];
@@ -348,34 +327,9 @@ __device__ __forceinline__ void stage_hyb_tile(const StageArgs& a, const int i0,
         {
             const int nt = *ntrb;
             const float agx[2] = {ag1, ag2};
-            if constexpr (P2 || VER == FIN_WENO_FD) {
-                // two adjacent lanes per troubled face: the even lane takes
-                // fields 0 and 4, the odd lane fields 1, 2 and 3; the halves
-                // are added (even + odd, the same order in both lanes) and
-                // the even lane stores the face.  The loop bound is uniform
-                // over the warp, so every lane reaches the shuffles.
 #pragma unroll 1
-                for (int base = tid & ~31; base < 2 * nt; base += NT) {
-                    const int k2 = base + lane;
-                    const bool act = k2 < 2 * nt;
-                    float fh[MEQN] = {0.0f, 0.0f, 0.0f, 0.0f, 0.0f};
-                    const int w = act ? tlist[k2 >> 1] : 0;
-                    if (act)
-                        hyb_troubled_face<VER, P2, Cfg>(w, fqx, fqy, prim4, Fh, Gh, gam, eps, pw, ash, agx[0], agx[1],
-                                                        (k2 & 1) ? 2 : 1, fh);
-#pragma unroll
-                    for (int m = 0; m < MEQN; m++) {
-                        const float o = __shfl_xor_sync(0xffffffffu, fh[m], 1);
-                        fh[m] = (k2 & 1) ? o + fh[m] : fh[m] + o;
-                    }
-                    if (act && !(k2 & 1)) hyb_store_face<Cfg>(w, fh, Fh, Gh);
-                }
-            } else {
-#pragma unroll 1
-                for (int k = tid; k < nt; k += NT)
-                    hyb_troubled_face<VER, P2, Cfg>(tlist[k], fqx, fqy, prim4, Fh, Gh, gam, eps, pw, ash, agx[0],
-                                                    agx[1]);
-            }
+            for (int k = tid; k < nt; k += NT)
+                hyb_troubled_face<VER, P2, Cfg>(tlist[k], fqx, fqy, prim4, Fh, Gh, gam, eps, pw, ash, agx[0], agx[1]);
         }
         __syncthreads();
         // ---- phase 3: flux difference (ConstructL.cpp:396-398), update

@@ -10,7 +10,7 @@ void SetBndValues(StateVars& Q);   // the application's own (app_defined.h:10)
 namespace {
 
 fin_solver* g_solver = nullptr;
-fin_params g_key;   // parameters g_solver was created with (before the BC probe)
+fin_params g_key;   // parameters g_solver was created with (boundary conditions included)
 
 // Reads the boundary condition of one side off the application's
 // SetBndValues: the probe's interior cell (i, j) holds the value
@@ -103,12 +103,16 @@ fin_solver* fin_shim_solver()
 {
     fin_params p;
     fin_shim_params(&p);
-    // The solver is kept while the grid and method stay the same.
-    if (g_solver && memcmp(&p, &g_key, sizeof(p)) == 0) return g_solver;
-    g_key = p;
+    // The boundary conditions are read off SetBndValues on every call (a
+    // host pass over one grid-sized probe, the order of the packing each
+    // call does anyway), so a process that changes them between calls gets
+    // a solver with the right ones.  The solver is kept while the grid, the
+    // method and the boundary conditions stay the same.
     int bc[4];
     fin_shim_probe_bc(p.mx, p.my, p.mbc, p.meqn, p.maux, bc);
     p.bc_xlow = bc[0]; p.bc_xhigh = bc[1]; p.bc_ylow = bc[2]; p.bc_yhigh = bc[3];
+    if (g_solver && memcmp(&p, &g_key, sizeof(p)) == 0) return g_solver;
+    g_key = p;
     if (g_solver) fin_destroy(g_solver);
     g_solver = nullptr;
     fin_shim_check(fin_create(&p, &g_solver), "fin_create");
