@@ -168,12 +168,15 @@ __device__ __forceinline__ f2 left1_x2(const Euler::Eig<float>& e, const Euler::
     return f2_mul(a, f2_splat(e.inv_d2));
 }
 
-// parts: bit 0 = pass 1 (fields 0 and 4), bit 1 = passes 2 and 3 (fields 1,
-// 2, 3); fh receives the sum of the selected fields' right projections (a
-// face split over two threads adds the two partial fluxes afterwards).
+// FIN_X2_MERGE: fields 0, 4 and 1 in one sweep of the stencil (one load of
+// each point instead of two), at the price of six live reconstruction
+// stencils instead of four.
+#ifndef FIN_X2_MERGE
+#define FIN_X2_MERGE 0
+#endif
 template <int VER, class Pt>
 __device__ __forceinline__ void weno_char_flux_x2(const Euler::Eig<float>& ev, float lah, const Pt& pt, float eps,
-                                                  float* fh, int parts = 3)
+                                                  float* fh)
 {
     const Euler::Rows<float> rw = Euler::rows(ev);
     const f2 pmla = f2_make(lah, -lah);
@@ -186,7 +189,34 @@ __device__ __forceinline__ void weno_char_flux_x2(const Euler::Eig<float>& ev, f
 #pragma unroll
         for (int m = 0; m < MEQN; m++) v[m] = f2_fma(pmla, f2_splat(q[m]), f2_splat(f[m]));
     };
-    if (parts & 1) {
+#if FIN_X2_MERGE
+    {
+        // fields 0, 4 and 1 in one sweep; the right projections are added
+        // in the order 0, 4, 1 as the separate passes add them
+        float p0[5], p4[5], m0[5], m4[5], p1[5], m1[5];
+#pragma unroll
+        for (int s = 0; s < 6; s++) {
+            asm volatile("" ::: "memory");
+            f2 v[MEQN], w0, w4;
+            split(s, v);
+            left04_x2(ev, rw, v, w0, w4);
+            const f2 w1 = left1_x2(ev, rw, v);
+            if (s < 5) { p0[s] = f2_lo(w0); p4[s] = f2_lo(w4); p1[s] = f2_lo(w1); }
+            if (s > 0) { m0[5 - s] = f2_hi(w0); m4[5 - s] = f2_hi(w4); m1[5 - s] = f2_hi(w1); }
+        }
+#pragma unroll 1
+        for (int k = 0; k < 3; k++) {
+            float up[5], um[5];
+#pragma unroll
+            for (int t = 0; t < 5; t++) {
+                up[t] = k == 0 ? p0[t] : (k == 1 ? p4[t] : p1[t]);
+                um[t] = k == 0 ? m0[t] : (k == 1 ? m4[t] : m1[t]);
+            }
+            right_add_f<float>(ev, k == 0 ? 0 : (k == 1 ? 4 : 1), weno_pair_f<float, VER, true>(up, um, eps, 2.0f), fh);
+        }
+    }
+#else
+    {
         // pass 1: fields 0 and 4
         float p0[5], p4[5], m0[5], m4[5];
 #pragma unroll
@@ -209,7 +239,7 @@ __device__ __forceinline__ void weno_char_flux_x2(const Euler::Eig<float>& ev, f
             right_add_f<float>(ev, k == 0 ? 0 : 4, weno_pair_f<float, VER, true>(up, um, eps, 2.0f), fh);
         }
     }
-    if (parts & 2) {
+    {
         // pass 2: field 1
         float p1[5], m1[5];
 #pragma unroll
@@ -223,7 +253,8 @@ __device__ __forceinline__ void weno_char_flux_x2(const Euler::Eig<float>& ev, f
         }
         right_add_f<float>(ev, 1, weno_pair_f<float, VER, true>(p1, m1, eps, 2.0f), fh);
     }
-    if (parts & 2) {
+#endif
+    {
         // pass 3: fields 2 and 3 (v_t - u2 v0, v_w - u3 v0)
         float p2[5], p3[5], m2[5], m3[5];
 #pragma unroll
