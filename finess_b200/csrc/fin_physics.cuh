@@ -211,6 +211,13 @@ __global__ void __launch_bounds__(256, 1) k_phys_stage(const __grid_constant__ S
         const int gi = i0 + ci, gj = j0 + cj;
         if (gi >= mx || gj >= my) continue;
         const size_t g = size_t(gi) * my + gj;
+        // operand loads ahead of the first store (qout may alias A or B as
+        // far as the compiler knows)
+        double va[M], vb[M];
+        for (int m = 0; m < M; m++) {
+            va[m] = a.A ? a.A[m * a.plane + g] : 0.0;
+            vb[m] = a.B ? a.B[m * a.plane + g] : 0.0;
+        }
         double qn[M];
         for (int m = 0; m < M; m++) {
             const double f1 = Fh[m * (TI + 1) * TJ + (ci + 1) * TJ + cj], f0 = Fh[m * (TI + 1) * TJ + ci * TJ + cj];
@@ -219,8 +226,8 @@ __global__ void __launch_bounds__(256, 1) k_phys_stage(const __grid_constant__ S
             double L = __ddiv_rn(-__dsub_rn(f1, f0), a.dx);
             L = __dsub_rn(L, __ddiv_rn(__dsub_rn(g1, g0), a.dy));
             double v = 0.0;
-            if (a.A) v = __dmul_rn(a.a1, a.A[m * a.plane + g]);
-            if (a.B) v = __dadd_rn(v, __dmul_rn(a.a2, a.B[m * a.plane + g]));
+            if (a.A) v = __dmul_rn(a.a1, va[m]);
+            if (a.B) v = __dadd_rn(v, __dmul_rn(a.a2, vb[m]));
             v = __dadd_rn(v, __dmul_rn(a.bdt, L));
             qn[m] = v;
             a.qout[m * a.plane + g] = v;

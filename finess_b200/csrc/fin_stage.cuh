@@ -390,8 +390,11 @@ __device__ __forceinline__ void stage_tile(const StageArgs& a, const int i0, con
             qbase = (H + fi) * RJ + (H + fj); qstr = RJ;
             fl = fs; fbase = (H + fi) * TJ + fj; fstr = TJ; fplane = RI * TJ;
         } else {
+            // face between cols fj-1, fj; taken by rows of TJ, then the last
+            // column, so a half-warp reads one row of the staged tile
             const int v = w - Cfg::NFX;
-            fi = v / (TJ + 1); fj = v - fi * (TJ + 1);  // face between cols fj-1, fj
+            fi = v < TI * TJ ? v / TJ : v - TI * TJ;
+            fj = v < TI * TJ ? v - fi * TJ : TJ;
             qbase = (H + fi) * RJ + (H + fj); qstr = 1;
             fl = gs; fbase = fi * RJ + (H + fj); fstr = 1; fplane = TI * RJ;
         }
@@ -638,6 +641,15 @@ __device__ __forceinline__ void stage_tile(const StageArgs& a, const int i0, con
         const int gi = i0 + ci, gj = j0 + cj;
         if (gi >= mx || gj >= my) continue;
         const size_t g = size_t(gi) * my + gj;
+        // every operand load ahead of the first store: qout may alias A or
+        // B as far as the compiler knows, so loads interleaved with the
+        // stores would wait one memory round trip per component
+        double va[MEQN], vb[MEQN];
+#pragma unroll
+        for (int m = 0; m < MEQN; m++) {
+            va[m] = a.A ? a.A[m * a.plane + g] : 0.0;
+            vb[m] = a.B ? a.B[m * a.plane + g] : 0.0;
+        }
         double qn[MEQN];
 #pragma unroll
         for (int m = 0; m < MEQN; m++) {
@@ -651,8 +663,8 @@ __device__ __forceinline__ void stage_tile(const StageArgs& a, const int i0, con
             const double L = double(Lr);
             double v = 0.0;
             {
-                if (a.A) v = a.a1 * a.A[m * a.plane + g];
-                if (a.B) v = v + a.a2 * a.B[m * a.plane + g];
+                if (a.A) v = a.a1 * va[m];
+                if (a.B) v = v + a.a2 * vb[m];
             }
             v = v + a.bdt * L;
             qn[m] = v;

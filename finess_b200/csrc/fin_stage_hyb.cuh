@@ -317,10 +317,16 @@ __device__ __forceinline__ void stage_hyb_tile(const StageArgs& a, const int i0,
         }
 #pragma unroll 1
         for (int wb = 0; wb < Cfg::NFY; wb += NT) {
+            // y faces by rows of TJ, then the last column: a half-warp then
+            // reads one row of the staged pairs and primitives (rows of
+            // TJ + 1 faces straddled the half-warps and doubled some
+            // shared-memory wavefronts)
             const int v = wb + tid;
+            const int fi = v < TI * TJ ? v / TJ : v - TI * TJ;
+            const int fj = v < TI * TJ ? v - fi * TJ : TJ;
             bool push = false;
-            if (v < Cfg::NFY) push = face_a(std::false_type{}, v / (TJ + 1), v - (v / (TJ + 1)) * (TJ + 1));
-            append(push, Cfg::NFX + v);
+            if (v < Cfg::NFY) push = face_a(std::false_type{}, fi, fj);
+            append(push, Cfg::NFX + fi * (TJ + 1) + fj);
         }
         __syncthreads();
         // ---- phase 2, pass B: full characteristic WENO on the listed faces ----
@@ -352,14 +358,22 @@ __device__ __forceinline__ void stage_hyb_tile(const StageArgs& a, const int i0,
                 const double* se = ebuf + c;
                 const double* ge = ext ? ext + g : nullptr;
                 double* out = a.qout + g;
+                // every operand load ahead of the first store: out may alias
+                // them as far as the compiler knows, and loads interleaved
+                // with the stores would wait one L2 round trip per component
+                double qiv[MEQN], qev[MEQN];
+#pragma unroll
+                for (int m = 0; m < MEQN; m++) {
+                    qiv[m] = L::SHARE ? a.qin[m * plane + g] : si[m * RI * Cfg::SJ];
+                    qev[m] = (tt && !L::SHARE) ? se[m * TT] : (ge ? ge[m * plane] : 0.0);
+                }
                 float qf[MEQN];
 #pragma unroll
                 for (int m = 0; m < MEQN; m++) {
                     const float f1 = fh[m * (TI + 1) * TJ + TJ], f0 = fh[m * (TI + 1) * TJ];
                     const float g1 = gh[m * TI * (TJ + 1) + 1], g0 = gh[m * TI * (TJ + 1)];
                     const float Lr = -(f1 - f0) * rdx - (g1 - g0) * rdy;
-                    const double qi = L::SHARE ? a.qin[m * plane + g] : si[m * RI * Cfg::SJ];
-                    const double qe = (tt && !L::SHARE) ? se[m * TT] : (ge ? ge[m * plane] : 0.0);
+                    const double qi = qiv[m], qe = qev[m];
                     double v = hasA ? a1 * (Aq ? qi : qe) : 0.0;
                     if (hasB) v = v + a2 * (Bq ? qi : qe);
                     v = v + bdt * double(Lr);

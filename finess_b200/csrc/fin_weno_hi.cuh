@@ -302,6 +302,14 @@ __global__ void __launch_bounds__(256) k_hi_update(const double* __restrict__ fx
     bool nonfinite = false;
     for (size_t g = blockIdx.x * size_t(blockDim.x) + threadIdx.x; g < n; g += size_t(gridDim.x) * blockDim.x) {
         const int i = int(g / my), j = int(g - size_t(i) * my);
+        // operand loads ahead of the first store (qout may alias A or B as
+        // far as the compiler knows)
+        double va[MEQN], vb[MEQN];
+#pragma unroll
+        for (int m = 0; m < MEQN; m++) {
+            va[m] = a.A ? a.A[m * a.plane + g] : 0.0;
+            vb[m] = a.B ? a.B[m * a.plane + g] : 0.0;
+        }
         double qn[MEQN];
 #pragma unroll
         for (int m = 0; m < MEQN; m++) {
@@ -310,8 +318,8 @@ __global__ void __launch_bounds__(256) k_hi_update(const double* __restrict__ fx
             double L = -(f1 - f0) * a.rdx;
             L = L - (g1 - g0) * a.rdy;
             double v = 0.0;
-            if (a.A) v = a.a1 * a.A[m * a.plane + g];
-            if (a.B) v = v + a.a2 * a.B[m * a.plane + g];
+            if (a.A) v = a.a1 * va[m];
+            if (a.B) v = v + a.a2 * vb[m];
             v = v + a.bdt * L;
             qn[m] = v;
             a.qout[m * a.plane + g] = v;
