@@ -436,6 +436,83 @@ def run_whole_runs(args):
                       "runs": runs}), flush=True)
 
 
+def run_segments(args):
+    """The hybrid whole run to T_END in segments of 0.1 (one JSON line per
+    segment): steps, ms per step, the mean stage and indicator launch times
+    (CUDA events per launch), and the indicator's flagged fraction of the
+    faces at the segment's end, raw and after the stage kernel's 3 x 3
+    dilation of same-direction faces."""
+    import torch
+    torch.cuda.set_device(0)
+    from finess_b200 import problems as P
+    indicator = load_indicator()
+    p = P.riemann_params(n=args.n)
+    q0 = P.riemann_init(p)
+    s = make_solver(p, "hybrid", indicator)
+    s.set_state(q0, 0.0)
+    dtv = np.array([0.0, first_dt(p, s, q0), p.max_dt])
+
+    def dilate(a):
+        d = a.copy()
+        d[1:, :] |= a[:-1, :]
+        d[:-1, :] |= a[1:, :]
+        e = d.copy()
+        e[:, 1:] |= d[:, :-1]
+        e[:, :-1] |= d[:, 1:]
+        return e
+    nx = (p.mx + 1) * p.my
+    nseg = int(round(T_END / 0.1))
+    for k in range(1, nseg + 1):
+        s.set_kernel_timing(True)
+        dtv, m = s.advance(0.1 * k if k < nseg else T_END, dtv, 1 << 30)
+        ms = s.last_kernel_ms()
+        kms, kl = s.kernel_time()
+        ims, il = s.indicator_time()
+        s.set_kernel_timing(False)
+        f = s.hybrid_flags()
+        fx, fy = f[:nx].reshape(p.mx + 1, p.my), f[nx:].reshape(p.mx, p.my + 1)
+        st = s.hybrid_stats()
+        print(json.dumps({"t": round(0.1 * k, 3), "steps": m, "ms_per_step": ms / max(m, 1),
+                          "stage_kernel_ms": kms / max(kl, 1), "indicator_kernel_ms": ims / max(il, 1),
+                          "flagged_raw": float((fx.sum() + fy.sum()) / f.size),
+                          "flagged_dilated": float((dilate(fx).sum() + dilate(fy).sum()) / f.size),
+                          "judges": st["judges"], "reverts": st["reverts"]}), flush=True)
+    s.close()
+
+
+def run_small(args):
+    """Small single problems (config 1's isentropic vortex, FP64, WENO5-JS,
+    SSP-RK3, to t = 10) through fin_advance, whose step control reads the
+    CFL back to the host every step, and through a batch of one problem
+    (step control on the device, each step one CUDA graph replay, the host
+    polled every few steps); both must give the same state bit for bit."""
+    import torch
+    torch.cuda.set_device(0)
+    from finess_b200 import problems as P
+    from finess_b200.batch import Batch
+    from finess_b200._abi import FIN_PREC_FP64
+    for n in (64, 200, 512):
+        p = P.vortex_params(n=n)
+        p.precision = FIN_PREC_FP64
+        q0 = P.vortex_exact(p, 0.0)
+        s = make_solver(p, "fp64", None)
+        s.set_state(q0, 0.0)
+        dt0 = first_dt(p, s, q0)
+        dtv, k = s.advance(10.0, np.array([0.0, dt0, p.max_dt]), 1 << 30)
+        adv_ms = s.last_kernel_ms()
+        qa, _ = s.get_state()
+        s.close()
+        with Batch([p]) as b:
+            b.set_state(0, q0, 0.0)
+            _, steps = b.solve(10.0, np.array([dt0]))
+            bat_ms = b.stats()["device_ms"]
+            qb, _ = b.get_state(0)
+        print(json.dumps({"grid": f"{n}x{n}", "steps": int(k), "batch_steps": int(steps[0]),
+                          "fin_advance_ms": adv_ms, "fin_advance_us_per_step": 1e3 * adv_ms / k,
+                          "batch_of_one_ms": bat_ms, "batch_us_per_step": 1e3 * bat_ms / max(int(steps[0]), 1),
+                          "bitwise_equal": bool(np.array_equal(qa, qb))}), flush=True)
+
+
 def run_frames_bench(args):
     """RunFinpack's frame loop on the device (finess_b200.frames), then the
     reference's own Output (oracle/_ref/libfinref_io.so, one host thread) on
@@ -513,6 +590,16 @@ def main():
                     help="frame files from device state, and the reference's Output on the last frame")
     ap.add_argument("--sweep", action="store_true",
                     help="the uneven 1024-problem sweep (FP32, to t = 0.25), its problems split across the ranks")
+    ap.add_argument("--small", action="store_true",
+                    help="small single problems (200^2 vortex and others) through fin_advance and a batch of one")
+    ap.add_argument("--segments", action="store_true",
+                    help="the hybrid whole run in segments of 0.1: per-segment cost and flagged fractions")
+    ap.add_argument("--save-state", default=None, metavar="PATH",
+                    help="profiling case: run the headline problem (first form of --forms) from t = 0 to "
+                         "--window-t and save its state to PATH (.npz)")
+    ap.add_argument("--load-state", default=None, metavar="PATH",
+                    help="profiling case: W + K steps of the first form of --forms from the state saved at PATH "
+                         "(few launches before a captured one)")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     if args.mpp:
@@ -533,6 +620,15 @@ def main():
         return
     if args.sweep:
         run_sweep_bench(args)
+        return
+    if args.segments:
+        run_segments(args)
+        return
+    if args.small:
+        run_small(args)
+        return
+    if args.save_state or args.load_state:
+        run_state_case(args)
         return
     if args.impl == "reference":
         run_reference_arm(args)
@@ -738,6 +834,48 @@ def main():
         }
         print(json.dumps(line), flush=True)
     replicas.finish()
+
+
+def run_state_case(args):
+    """Profiling cases from a mid-run state: --save-state runs the headline
+    problem from t = 0 to --window-t in one form and saves the state;
+    --load-state takes W + K steps from such a state, so a profiler capture
+    of a stage or indicator launch at that state follows only a few launches
+    (the whole run to --window-t happens in another process)."""
+    import torch
+    torch.cuda.set_device(0)
+    from finess_b200 import problems as P
+    indicator = load_indicator()
+    form = (args.forms or "hybrid").split(",")[0]
+    p = P.riemann_params(n=args.n)
+    s = make_solver(p, form, indicator)
+    if args.save_state:
+        q0 = P.riemann_init(p)
+        s.set_state(q0, 0.0)
+        dtv, k = s.advance(args.window_t, np.array([0.0, first_dt(p, s, q0), p.max_dt]), 1 << 30)
+        q, t = s.get_state()
+        np.savez(args.save_state, q=q, t=t, n=args.n)
+        out = {"saved": args.save_state, "form": form, "grid": f"{p.mx}x{p.my}", "t": t, "steps": k}
+    else:
+        z = np.load(args.load_state)
+        if int(z["n"]) != args.n:
+            raise SystemExit(f"{args.load_state} holds a {int(z['n'])}^2 state; pass --n {int(z['n'])}")
+        q, t = z["q"], float(z["t"])
+        s.set_state(q, t)
+        dtv = np.array([0.0, first_dt(p, s, q), p.max_dt])
+        dtv, nw = s.advance(T_END + 1.0, dtv, args.warmup)
+        s.set_kernel_timing(True)
+        dtv, k = s.advance(T_END + 1.0, dtv, args.steps)
+        kms, kl = s.kernel_time()
+        out = {"loaded": args.load_state, "form": form, "grid": f"{p.mx}x{p.my}", "t_start": t, "steps": k,
+               "ms_per_step": s.last_kernel_ms() / max(k, 1), "stage_kernel_ms": kms / max(kl, 1)}
+        if form == "hybrid":
+            ims, il = s.indicator_time()
+            out["indicator_kernel_ms"] = ims / il if il else None
+            out["hybrid_stats"] = s.hybrid_stats()
+        s.set_kernel_timing(False)
+    s.close()
+    print(json.dumps(out), flush=True)
 
 
 if __name__ == "__main__":
