@@ -110,11 +110,21 @@ struct TileCfg {
     static constexpr int RI = TI + 2 * H, RJ = TJ + 2 * H;
     static constexpr int NFX = (TI + 1) * TJ, NFY = TI * (TJ + 1);
     static constexpr int NPRIM = 4;   // per-cell u, v, p, c of the cross region
+    // FP32 faces of a 15 x 16 tile go to threads so that the two half-warps
+    // of a warp take face rows 8 apart (XROW8): 8 rows of RJ = 22 words are
+    // 176 words, 16 modulo 32, so the two rows' words fall in opposite
+    // halves of the banks; the x-direction flux rows get a pitch of 18 for
+    // the same reason (8 x 18 = 144).  FP64 (a half-warp reads one row of
+    // 8-byte words) keeps the row-by-row order.
+    template <class R>
+    __host__ __device__ static constexpr bool XROW8() { return sizeof(R) == 4 && TI == 15 && TJ == 16; }
+    template <class R>
+    __host__ __device__ static constexpr int FSJ() { return XROW8<R>() ? TJ + 2 : TJ; }
     // byte offset of the reduction scratch (after the arrays, 16-B aligned)
     template <class R>
     __host__ __device__ static constexpr size_t red_offset()
     {
-        return (sizeof(R) * (size_t(MEQN) * (size_t(RI) * RJ + size_t(RI) * TJ + size_t(TI) * RJ +
+        return (sizeof(R) * (size_t(MEQN) * (size_t(RI) * RJ + size_t(RI) * FSJ<R>() + size_t(TI) * RJ +
                                              size_t(TI + 1) * TJ + size_t(TI) * (TJ + 1)) +
                              size_t(NPRIM) * RI * RJ) + 15) / 16 * 16;
     }
@@ -286,8 +296,9 @@ __device__ __forceinline__ void stage_tile(const StageArgs& a, const int i0, con
     extern __shared__ __align__(128) unsigned char smem_raw[];
     R* prim = reinterpret_cast<R*>(smem_raw);      // [4][RI][RJ]   u, v, p, c
     R* qs = prim + Cfg::NPRIM * PQ;                // [M][RI][RJ]
-    R* fs = qs + MEQN * PQ;                        // [M][RI][TJ]   0.5 * f
-    R* gs = fs + MEQN * RI * TJ;                   // [M][TI][RJ]   0.5 * g
+    constexpr int FS = Cfg::template FSJ<R>();
+    R* fs = qs + MEQN * PQ;                        // [M][RI][FS]   0.5 * f
+    R* gs = fs + MEQN * RI * FS;                   // [M][TI][RJ]   0.5 * g
     R* Fh = gs + MEQN * TI * RJ;                   // [M][TI+1][TJ]
     R* Gh = Fh + MEQN * (TI + 1) * TJ;             // [M][TI][TJ+1]
     double* red = reinterpret_cast<double*>(smem_raw + Cfg::template red_offset<R>());
@@ -340,9 +351,9 @@ __device__ __forceinline__ void stage_tile(const StageArgs& a, const int i0, con
             cj = cj < -3 ? -3 : (cj > my + 2 ? my + 2 : cj);
             const size_t o = size_t(ci + 3) * (my + 6) + (cj + 3);
             if (yin) {
-                const int d = ii * TJ + (jj - H);
+                const int d = ii * FS + (jj - H);
 #pragma unroll
-                for (int m = 0; m < MEQN; m++) fs[m * RI * TJ + d] = R(0.5 * __ldg(a.Fg + m * a.gplane + o));
+                for (int m = 0; m < MEQN; m++) fs[m * RI * FS + d] = R(0.5 * __ldg(a.Fg + m * a.gplane + o));
             }
             if (xin) {
                 const int d = (ii - H) * RJ + jj;
@@ -353,12 +364,12 @@ __device__ __forceinline__ void stage_tile(const StageArgs& a, const int i0, con
         }
         const R hr = R(0.5) * rho, hep = R(0.5) * (en + press);
         if (yin) {
-            const int o = ii * TJ + (jj - H);
+            const int o = ii * FS + (jj - H);
             fs[o] = hr * u1;
-            fs[RI * TJ + o] = hr * u1 * u1 + R(0.5) * press;
-            fs[2 * RI * TJ + o] = hr * u1 * u2;
-            fs[3 * RI * TJ + o] = hr * u1 * u3;
-            fs[4 * RI * TJ + o] = u1 * hep;
+            fs[RI * FS + o] = hr * u1 * u1 + R(0.5) * press;
+            fs[2 * RI * FS + o] = hr * u1 * u2;
+            fs[3 * RI * FS + o] = hr * u1 * u3;
+            fs[4 * RI * FS + o] = u1 * hep;
         }
         if (xin) {
             const int o = (ii - H) * RJ + jj;
@@ -386,15 +397,29 @@ __device__ __forceinline__ void stage_tile(const StageArgs& a, const int i0, con
         int fi, fj, qbase, qstr, fbase, fstr, fplane;
         const R* fl;
         if (isx) {
-            fi = w / TJ; fj = w - fi * TJ;            // face between rows fi-1, fi of the tile
+            // face between rows fi-1, fi of the tile
+            if constexpr (Cfg::template XROW8<R>()) {
+                fi = (w >> 5) + ((w >> 1) & 8); fj = w & 15;   // half-warps on rows r and r + 8
+            } else {
+                fi = w / TJ; fj = w - fi * TJ;
+            }
             qbase = (H + fi) * RJ + (H + fj); qstr = RJ;
-            fl = fs; fbase = (H + fi) * TJ + fj; fstr = TJ; fplane = RI * TJ;
+            fl = fs; fbase = (H + fi) * FS + fj; fstr = FS; fplane = RI * FS;
         } else {
             // face between cols fj-1, fj; taken by rows of TJ, then the last
-            // column, so a half-warp reads one row of the staged tile
+            // column, so a half-warp reads one row of the staged tile (FP32:
+            // half-warps on rows r and r + 8; the last warp takes row 7 and
+            // the last column)
             const int v = w - Cfg::NFX;
-            fi = v < TI * TJ ? v / TJ : v - TI * TJ;
-            fj = v < TI * TJ ? v - fi * TJ : TJ;
+            if constexpr (Cfg::template XROW8<R>()) {
+                const int wv = v >> 5, ln = v & 31;
+                if (wv < 7) { fi = wv + (ln & 16 ? 8 : 0); fj = ln & 15; }
+                else if (ln < 16) { fi = 7; fj = ln; }
+                else { fi = ln - 16; fj = TJ; }
+            } else {
+                fi = v < TI * TJ ? v / TJ : v - TI * TJ;
+                fj = v < TI * TJ ? v - fi * TJ : TJ;
+            }
             qbase = (H + fi) * RJ + (H + fj); qstr = 1;
             fl = gs; fbase = fi * RJ + (H + fj); fstr = 1; fplane = TI * RJ;
         }
