@@ -147,8 +147,8 @@ struct IndTile {
 // tcgen05 and the flags.  Per tile the CTA owns the x faces of rows i0 ..
 // i0+TI-1 and the y faces of columns j0 .. j0+TJ-1 (the last tile row /
 // column also the domain's last face row / column): at most 511 faces, laid
-// out as four 128-row matrices (slots 0..255 x faces (fi, fj) = (s / 16,
-// s % 16), slots 256..510 y faces (fi, fj) = ((s-256) / 17, (s-256) % 17)).
+// out as four 128-row matrices (slots 0..255 x faces, slots 256..510 y
+// faces, each warp's half-warps on face rows 8 apart).
 //   2. each thread: the features of its two slots from shared memory;
 //   3. layer 1 on tcgen05 (4 x two K=16 steps into TMEM columns 0..127);
 //   4. 2 gelu, BF16, back into the X matrices; layer 2 into the same columns;
@@ -171,6 +171,7 @@ __device__ __forceinline__ void indicator_tile(IndTile<Cfg>& S, const int mx, co
 {
     using namespace mlp;
     constexpr int TI = Cfg::TI, TJ = Cfg::TJ, H = Cfg::H, RJ = Cfg::RJ, PQ = Cfg::RI * Cfg::RJ;
+    static_assert(Cfg::NT == 256 && TI == 15 && TJ == 16, "face slots: 256 x faces, 255 y faces, rows 8 apart");
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const uint32_t lane_base = uint32_t((warp & 3) * 32) << 16;
     // ---- 2. features of the thread's two slots ----
@@ -188,8 +189,17 @@ __device__ __forceinline__ void indicator_tile(IndTile<Cfg>& S, const int mx, co
         fbit[h] = 0;
         bool isx = sl < 256;
         int fi, fj;
-        if (isx) { fi = sl >> 4; fj = sl & 15; }
-        else { const int v = sl - 256; fi = v / (TJ + 1); fj = v - fi * (TJ + 1); }
+        // half-warps on face rows r and r + 8: 8 rows of RJ = 22 words are
+        // 176 words, 16 modulo 32, so the two rows' stencil loads fall in
+        // opposite halves of the banks (the last warp of y slots takes row
+        // 7 and the last column)
+        if (isx) { fi = (sl >> 5) + ((sl >> 1) & 8); fj = sl & 15; }
+        else {
+            const int v = sl - 256, wv = v >> 5, ln = v & 31;
+            if (wv < 7) { fi = wv + (ln & 16 ? 8 : 0); fj = ln & 15; }
+            else if (ln < 16) { fi = 7; fj = ln; }
+            else { fi = ln - 16; fj = TJ; }
+        }
         const int gi = i0 + fi, gj = j0 + fj;
         bool own;
         if (isx) own = gj < my && gi <= mx && (fi < TI || gi == mx);
@@ -296,7 +306,7 @@ template <class Cfg>
 __global__ void __launch_bounds__(Cfg::NT, 3) k_indicator(const __grid_constant__ IndicatorArgs a)
 {
     constexpr int TI = Cfg::TI, TJ = Cfg::TJ, H = Cfg::H;
-    static_assert(Cfg::NT == 256 && (TI + 1) * TJ <= 256 && TI * (TJ + 1) <= 255 && TJ == 16, "face slots");
+    static_assert(Cfg::NT == 256 && TI == 15 && TJ == 16, "face slots: 256 x faces, 255 y faces, rows 8 apart");
     extern __shared__ __align__(128) unsigned char smem_raw[];
     IndTile<Cfg>& S = *reinterpret_cast<IndTile<Cfg>*>(smem_raw);
     const int tid = threadIdx.x, warp = tid >> 5;
