@@ -97,7 +97,10 @@ __device__ __forceinline__ void stencil_features(const R (&Q)[6][MEQN], R gamma,
             d[s] = w[k][s + 1] - w[k][s];
             mmax = Max(mmax, R(fabs(d[s])));
         }
-        const R inv = R(1) / mmax;
+        // FP32: the hardware reciprocal (rcp.approx, within 1 ulp; mmax >=
+        // FEAT_FLOOR is a normal number) instead of the IEEE division's
+        // instruction sequence; the features are rounded to BF16 next
+        const R inv = sizeof(R) == 4 ? rcp(mmax) : R(1) / mmax;
 #pragma unroll
         for (int s = 0; s < 5; s++) x[k * 5 + s] = float(d[s] * inv);
     }
