@@ -406,10 +406,22 @@ struct MhdCfg {
     // R arrays: qs [8][RI*RJ], fs [8][RI*TJ], gs [8][TI*RJ], pc [4][PI*PJ],
     // Fh [8][NFX], Gh [8][NFY], rec [MR_N][NT]; then FP64: as [AI*AJ],
     // an [NI*NJ], red [6][NT/32].
-    static constexpr size_t NR = size_t(MHD_NQ) * (RI * RJ + RI * TJ + TI * RJ + NFX + NFY) + 4 * PI * PJ +
-                                 size_t(MR_N) * NT;
+    // FP32 faces of a 15 x 16 tile go to threads so that the two half-warps
+    // of a warp take face rows 8 apart (ROW8): 8 rows of RJ = 22 (PJ = 18)
+    // words are 176 (144) words, 16 modulo 32, so the two rows' words fall
+    // in opposite halves of the banks; the x-direction flux rows get a pitch
+    // of FSJ = 18 for the same reason.  FP64 keeps the row-by-row order.
     template <class R>
-    __host__ __device__ static constexpr size_t dbl_offset() { return (NR * sizeof(R) + 15) / 16 * 16; }
+    __host__ __device__ static constexpr bool ROW8() { return sizeof(R) == 4 && TI == 15 && TJ == 16; }
+    template <class R>
+    __host__ __device__ static constexpr int FSJ() { return ROW8<R>() ? TJ + 2 : TJ; }
+    template <class R>
+    __host__ __device__ static constexpr size_t NR()
+    {
+        return size_t(MHD_NQ) * (RI * RJ + RI * FSJ<R>() + TI * RJ + NFX + NFY) + 4 * PI * PJ + size_t(MR_N) * NT;
+    }
+    template <class R>
+    __host__ __device__ static constexpr size_t dbl_offset() { return (NR<R>() * sizeof(R) + 15) / 16 * 16; }
     template <class R>
     __host__ __device__ static constexpr size_t smem_bytes()
     {
@@ -476,7 +488,8 @@ __global__ void __launch_bounds__(Cfg::NT, Cfg::MINB) k_mhd_stage(const __grid_c
     extern __shared__ __align__(128) unsigned char smem_raw[];
     R* qs = reinterpret_cast<R*>(smem_raw);          // [8][RI][RJ]
     R* fs = qs + MHD_NQ * PQ;                        // [8][RI][TJ]  0.5 f
-    R* gs = fs + MHD_NQ * RI * TJ;                   // [8][TI][RJ]  0.5 g
+    constexpr int FS = Cfg::template FSJ<R>();
+    R* gs = fs + MHD_NQ * RI * FS;                   // [8][TI][RJ]  0.5 g
     R* pc = gs + MHD_NQ * TI * RJ;                   // [4][PI][PJ]  u1, u2, p, cf
     R* Fh = pc + 4 * PP;                             // [8][TI+1][TJ]
     R* Gh = Fh + MHD_NQ * Cfg::NFX;                  // [8][TI][TJ+1]
@@ -551,8 +564,8 @@ __global__ void __launch_bounds__(Cfg::NT, Cfg::MINB) k_mhd_stage(const __grid_c
         const R Bu = u1 * B1 + u2 * B2 + u3 * B3;
         const R eb = en + press + Bm;
         if (yin) {
-            const int o = ii * TJ + (jj - H);
-            constexpr int S = RI * TJ;
+            const int o = ii * FS + (jj - H);
+            constexpr int S = RI * FS;
             fs[o] = R(0.5) * (rho * u1);
             fs[S + o] = R(0.5) * (rho * u1 * u1 + press + Bm - B1 * B1);
             fs[2 * S + o] = R(0.5) * (rho * u1 * u2 - B1 * B2);
@@ -649,13 +662,27 @@ __global__ void __launch_bounds__(Cfg::NT, Cfg::MINB) k_mhd_stage(const __grid_c
         Geom g;
         g.isx = w < Cfg::NFX;
         if (g.isx) {
-            g.fi = w / TJ; g.fj = w - g.fi * TJ;                  // between tile rows fi-1 and fi
+            // between tile rows fi-1 and fi
+            if constexpr (Cfg::template ROW8<R>()) {
+                g.fi = (w >> 5) + ((w >> 1) & 8); g.fj = w & 15;  // half-warps on rows r and r + 8
+            } else {
+                g.fi = w / TJ; g.fj = w - g.fi * TJ;
+            }
             g.qbase = (H + g.fi) * RJ + (H + g.fj); g.qstr = RJ;
-            g.fl = fs; g.fbase = (H + g.fi) * TJ + g.fj; g.fstr = TJ; g.fplane = RI * TJ;
+            g.fl = fs; g.fbase = (H + g.fi) * FS + g.fj; g.fstr = FS; g.fplane = RI * FS;
             g.pbase = (g.fi + 1) * PJ + (g.fj + 1); g.pstr = PJ;
         } else {
             const int v = w - Cfg::NFX;
-            g.fi = v / (TJ + 1); g.fj = v - g.fi * (TJ + 1);      // between tile columns fj-1 and fj
+            // between tile columns fj-1 and fj (FP32: half-warps on rows r and
+            // r + 8, the last warp on row 7 and the last column)
+            if constexpr (Cfg::template ROW8<R>()) {
+                const int wv = v >> 5, ln = v & 31;
+                if (wv < 7) { g.fi = wv + (ln & 16 ? 8 : 0); g.fj = ln & 15; }
+                else if (ln < 16) { g.fi = 7; g.fj = ln; }
+                else { g.fi = ln - 16; g.fj = TJ; }
+            } else {
+                g.fi = v / (TJ + 1); g.fj = v - g.fi * (TJ + 1);
+            }
             g.qbase = (H + g.fi) * RJ + (H + g.fj); g.qstr = 1;
             g.fl = gs; g.fbase = g.fi * RJ + (H + g.fj); g.fstr = 1; g.fplane = TI * RJ;
             g.pbase = (g.fi + 1) * PJ + (g.fj + 1); g.pstr = 1;
