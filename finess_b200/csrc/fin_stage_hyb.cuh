@@ -43,10 +43,14 @@ struct HybSmem {
     static constexpr size_t PRIM = 0;                                                    // float4 [RI][RJ]
     static constexpr size_t FQX = PRIM + size_t(RI) * RJ * 16;                          // float2 [M][RI][TJ]
     static constexpr size_t FQY = FQX + size_t(MEQN) * RI * TJ * 8;                     // float2 [M][TI][RJ]
-    static constexpr size_t FHGH = size_t(MEQN) * ((TI + 1) * TJ + TI * (TJ + 1)) * 4;  // Fh, Gh bytes
+    // face-flux rows of FP = TJ + 2 floats: the warps take face rows (and
+    // the update cell rows) 8 apart, 8 x 18 = 144 words, 16 modulo 32, so a
+    // warp's two rows fall in opposite halves of the banks
+    static constexpr int FP = TJ + 2;
+    static constexpr size_t FHGH = size_t(MEQN) * ((TI + 1) + TI) * FP * 4;             // Fh, Gh bytes
     static constexpr size_t STG = Cfg::pad128(FQY + size_t(MEQN) * TI * RJ * 8);        // double [M][RI][SJ]
-    static constexpr size_t FH = SHARE ? STG : STG + Cfg::pad128(Cfg::STG_BYTES);       // float [M][TI+1][TJ]
-    static constexpr size_t GH = FH + size_t(MEQN) * (TI + 1) * TJ * 4;                 // float [M][TI][TJ+1]
+    static constexpr size_t FH = SHARE ? STG : STG + Cfg::pad128(Cfg::STG_BYTES);       // float [M][TI+1][FP]
+    static constexpr size_t GH = FH + size_t(MEQN) * (TI + 1) * FP * 4;                 // float [M][TI][FP]
     static constexpr size_t EBUF = Cfg::pad128(SHARE ? STG + Cfg::STG_BYTES : FH + FHGH);   // double [M][TI][TJ]
     static constexpr size_t RED = SHARE ? EBUF : EBUF + Cfg::ABUF_BYTES;               // double [NT/32][4]
     static constexpr size_t MASK = RED + size_t(NT / 32) * 4 * 8;                       // unsigned [FXR + FYR]
@@ -93,7 +97,7 @@ __device__ __forceinline__ void hyb_troubled_face(int w, const float2* fqx, cons
                                                float ag1, float ag2)
 {
     constexpr int TI = Cfg::TI, TJ = Cfg::TJ, H = Cfg::H, RI = Cfg::RI, RJ = Cfg::RJ;
-    constexpr int XPL = RI * TJ, YPL = TI * RJ;
+    constexpr int XPL = RI * TJ, YPL = TI * RJ, FP = HybSmem<Cfg>::FP;
     const bool isx = w < Cfg::NFX;
     int fi, fj;
     if (isx) { fi = w / TJ; fj = w - fi * TJ; }
@@ -129,11 +133,11 @@ __device__ __forceinline__ void hyb_troubled_face(int w, const float2* fqx, cons
     else weno_char_flux<float, VER, P2>(ev, ash * alpha, eps, pw, pt, fh);
     if (isx) {
 #pragma unroll
-        for (int m = 0; m < MEQN; m++) Fh[m * (TI + 1) * TJ + fi * TJ + fj] = fh[m];
+        for (int m = 0; m < MEQN; m++) Fh[m * (TI + 1) * FP + fi * FP + fj] = fh[m];
     } else {
         const float o[MEQN] = {fh[0], fh[2], fh[1], fh[3], fh[4]};
 #pragma unroll
-        for (int m = 0; m < MEQN; m++) Gh[m * TI * (TJ + 1) + fi * (TJ + 1) + fj] = o[m];
+        for (int m = 0; m < MEQN; m++) Gh[m * TI * FP + fi * FP + fj] = o[m];
     }
 }
 
@@ -149,6 +153,8 @@ __device__ __forceinline__ void stage_hyb_tile(const StageArgs& a, const int i0,
     static_assert(Cfg::MASKS_FIT, "flag row masks are 32-bit words");
     constexpr int TI = Cfg::TI, TJ = Cfg::TJ, NT = Cfg::NT, H = Cfg::H, RI = Cfg::RI, RJ = Cfg::RJ;
     constexpr int XPL = RI * TJ, YPL = TI * RJ, TT = TI * TJ;   // component planes of fqx, fqy, ebuf
+    constexpr int FP = L::FP;                                    // face-flux row pitch
+    static_assert(TI == 15 && TJ == 16 && NT == 256 && NT >= TT, "one face / cell per thread, rows 8 apart");
     extern __shared__ __align__(128) unsigned char smem_raw[];
     float4* prim4 = reinterpret_cast<float4*>(smem_raw + L::PRIM);
     float2* fqx = reinterpret_cast<float2*>(smem_raw + L::FQX);
@@ -292,8 +298,8 @@ __device__ __forceinline__ void stage_hyb_tile(const StageArgs& a, const int i0,
             }
             if (!trb) {
                 const float lah = ash * alpha;
-                float* dst = isx ? Fh + fi * TJ + fj : Gh + fi * (TJ + 1) + fj;
-                constexpr int dplane = isx ? (TI + 1) * TJ : TI * (TJ + 1);
+                float* dst = (isx ? Fh : Gh) + fi * FP + fj;
+                constexpr int dplane = isx ? (TI + 1) * FP : TI * FP;
 #pragma unroll
                 for (int m = 0; m < MEQN; m++) dst[m * dplane] = linear_face2(P + m * pl, str, lah);
             }
@@ -308,22 +314,23 @@ __device__ __forceinline__ void stage_hyb_tile(const StageArgs& a, const int i0,
                 if (push) tlist[base + __popc(bal & ((1u << lane) - 1u))] = short(w);
             }
         };
-#pragma unroll 1
-        for (int wb = 0; wb < Cfg::NFX; wb += NT) {
-            const int w = wb + tid;
-            bool push = false;
-            if (w < Cfg::NFX) push = face_a(std::true_type{}, w / TJ, w - (w / TJ) * TJ);
-            append(push, w);
+        // One face per thread, x faces then y faces: a half-warp takes 16
+        // faces of one row (it reads one row of the pairs and primitives),
+        // the two half-warps of a warp rows 8 apart (the flux stores fall in
+        // opposite bank halves); the last warp of y faces takes row 7 and
+        // the last column.  The list holds face indices (fi (TJ+1) + fj for
+        // y faces after the NFX x faces, fi TJ + fj for x faces).
+        {
+            const int w = tid, fi = (w >> 5) + ((w >> 1) & 8), fj = w & 15;
+            const bool push = face_a(std::true_type{}, fi, fj);
+            append(push, fi * TJ + fj);
         }
-#pragma unroll 1
-        for (int wb = 0; wb < Cfg::NFY; wb += NT) {
-            // y faces by rows of TJ, then the last column: a half-warp then
-            // reads one row of the staged pairs and primitives (rows of
-            // TJ + 1 faces straddled the half-warps and doubled some
-            // shared-memory wavefronts)
-            const int v = wb + tid;
-            const int fi = v < TI * TJ ? v / TJ : v - TI * TJ;
-            const int fj = v < TI * TJ ? v - fi * TJ : TJ;
+        {
+            const int v = tid, wv = v >> 5, ln = v & 31;
+            int fi, fj;
+            if (wv < 7) { fi = wv + (ln & 16 ? 8 : 0); fj = ln & 15; }
+            else if (ln < 16) { fi = 7; fj = ln; }
+            else { fi = ln - 16; fj = TJ; }
             bool push = false;
             if (v < Cfg::NFY) push = face_a(std::false_type{}, fi, fj);
             append(push, Cfg::NFX + fi * (TJ + 1) + fj);
@@ -347,15 +354,18 @@ __device__ __forceinline__ void stage_hyb_tile(const StageArgs& a, const int i0,
             const double a1 = a.a1, a2 = a.a2, bdt = a.bdt;
             const float rdx = float(a.rdx), rdy = float(a.rdy);
             const size_t plane = a.plane;
+            // one cell per thread (NT >= TT), half-warps on cell rows 8
+            // apart (warp 7: row 7)
             for (int c = tid; c < TT; c += NT) {
-                const int ci = c / TJ, cj = c - ci * TJ;
+                const int wv = c >> 5, ln = c & 31;
+                const int ci = wv < 7 ? wv + (ln & 16 ? 8 : 0) : 7, cj = ln & 15;
                 const int gi = i0 + ci, gj = j0 + cj;
                 if (gi >= mx || gj >= my) continue;
                 const size_t g = size_t(gi) * my + gj;
-                const float* fh = Fh + ci * TJ + cj;
-                const float* gh = Gh + ci * (TJ + 1) + cj;
+                const float* fh = Fh + ci * FP + cj;
+                const float* gh = Gh + ci * FP + cj;
                 const double* si = stg + (H + ci) * Cfg::SJ + H + cj + 1;
-                const double* se = ebuf + c;
+                const double* se = ebuf + ci * TJ + cj;
                 const double* ge = ext ? ext + g : nullptr;
                 double* out = a.qout + g;
                 // every operand load ahead of the first store: out may alias
@@ -370,8 +380,8 @@ __device__ __forceinline__ void stage_hyb_tile(const StageArgs& a, const int i0,
                 float qf[MEQN];
 #pragma unroll
                 for (int m = 0; m < MEQN; m++) {
-                    const float f1 = fh[m * (TI + 1) * TJ + TJ], f0 = fh[m * (TI + 1) * TJ];
-                    const float g1 = gh[m * TI * (TJ + 1) + 1], g0 = gh[m * TI * (TJ + 1)];
+                    const float f1 = fh[m * (TI + 1) * FP + FP], f0 = fh[m * (TI + 1) * FP];
+                    const float g1 = gh[m * TI * FP + 1], g0 = gh[m * TI * FP];
                     const float Lr = -(f1 - f0) * rdx - (g1 - g0) * rdy;
                     const double qi = qiv[m], qe = qev[m];
                     double v = hasA ? a1 * (Aq ? qi : qe) : 0.0;
