@@ -656,7 +656,7 @@ int fin_mhd_create(const fin_params* p, fin_mhd** out)
     MCK(cudaGetDevice(&dev));
     cudaDeviceProp prop;
     MCK(cudaGetDeviceProperties(&prop, dev));
-    if (prop.major != 10) return merr(FIN_ERR_NO_DEVICE, "this build targets sm_100a (B200)");
+    if (prop.major != 10) return merr(FIN_ERR_NO_DEVICE, "libfinb200 is compiled for sm_100a (B200)");
     fin_mhd* s = new fin_mhd();
     memset(s, 0, sizeof(*s));
     s->p = *p;

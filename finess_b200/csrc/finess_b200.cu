@@ -1142,7 +1142,7 @@ int fin_create(const fin_params* p, fin_solver** out)
     CK(cudaGetDevice(&dev));
     cudaDeviceProp prop;
     CK(cudaGetDeviceProperties(&prop, dev));
-    if (prop.major != 10) return set_err(FIN_ERR_NO_DEVICE, "this build targets sm_100a (B200)");
+    if (prop.major != 10) return set_err(FIN_ERR_NO_DEVICE, "libfinb200 is compiled for sm_100a (B200)");
 
     fin_solver* s = new fin_solver();
     memset(s, 0, sizeof(*s));
