@@ -509,21 +509,49 @@ __global__ void __launch_bounds__(Cfg::NT, Cfg::MINB) k_mhd_stage(const __grid_c
 
     // ---- phase 0: q_in on the tile + 3-cell cross halo, A3 on the tile +
     // 5-cell frame (periodic remap) ----
-    for (int e = tid; e < PQ; e += NT) {
-        const int ii = e / RJ, jj = e - ii * RJ;
-        const bool xin = ii >= H && ii < H + TI, yin = jj >= H && jj < H + TJ;
-        if (!xin && !yin) continue;
-        const int gi = pwrap(i0 + ii - H, mx);
-        const int gj = pwrap(j0 + jj - H, my);
-        const size_t g = size_t(gi) * my + gj;
+    // All of a thread's loads (state and A3) are issued before its stores:
+    // one memory round trip per tile, not one per pass over the region.
+    {
+        constexpr int NQI = (PQ + NT - 1) / NT, NAI = (Cfg::AI * AJ + NT - 1) / NT;
+        double vq[NQI][MHD_NQ], va[NAI];
 #pragma unroll
-        for (int m = 0; m < MHD_NQ; m++) qs[m * PQ + e] = R(__ldg(a.qin + m * a.plane + g));
-    }
-    for (int e = tid; e < Cfg::AI * AJ; e += NT) {
-        const int ii = e / AJ, jj = e - ii * AJ;
-        const int gi = pwrap(i0 + ii - HA, mx);
-        const int gj = pwrap(j0 + jj - HA, my);
-        as[e] = __ldg(a.qin + 8 * a.plane + size_t(gi) * my + gj);
+        for (int it = 0; it < NQI; it++) {
+            const int e = tid + it * NT;
+            const int ii = e / RJ, jj = e - ii * RJ;
+            const bool xin = ii >= H && ii < H + TI, yin = jj >= H && jj < H + TJ;
+            if (e < PQ && (xin || yin)) {
+                const int gi = pwrap(i0 + ii - H, mx);
+                const int gj = pwrap(j0 + jj - H, my);
+                const size_t g = size_t(gi) * my + gj;
+#pragma unroll
+                for (int m = 0; m < MHD_NQ; m++) vq[it][m] = __ldg(a.qin + m * a.plane + g);
+            }
+        }
+#pragma unroll
+        for (int it = 0; it < NAI; it++) {
+            const int e = tid + it * NT;
+            if (e < Cfg::AI * AJ) {
+                const int ii = e / AJ, jj = e - ii * AJ;
+                const int gi = pwrap(i0 + ii - HA, mx);
+                const int gj = pwrap(j0 + jj - HA, my);
+                va[it] = __ldg(a.qin + 8 * a.plane + size_t(gi) * my + gj);
+            }
+        }
+#pragma unroll
+        for (int it = 0; it < NQI; it++) {
+            const int e = tid + it * NT;
+            const int ii = e / RJ, jj = e - ii * RJ;
+            const bool xin = ii >= H && ii < H + TI, yin = jj >= H && jj < H + TJ;
+            if (e < PQ && (xin || yin)) {
+#pragma unroll
+                for (int m = 0; m < MHD_NQ; m++) qs[m * PQ + e] = R(vq[it][m]);
+            }
+        }
+#pragma unroll
+        for (int it = 0; it < NAI; it++) {
+            const int e = tid + it * NT;
+            if (e < Cfg::AI * AJ) as[e] = va[it];
+        }
     }
     if (HYB) {
         // the flag windows, rows and columns wrapped (doubly periodic), each
