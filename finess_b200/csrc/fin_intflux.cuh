@@ -141,20 +141,34 @@ __global__ void __launch_bounds__(TI * TJ) k_intflux(const IntFluxArgs a)
     for (int st = 0; st < nstate; st++) {
         const double* q = st == 0 ? a.q1 : a.q2;
         if (st) __syncthreads();
-        for (int e = tid; e < PB; e += TI * TJ) {
-            const int ii = e / BJ, jj = e - ii * BJ;
-            const int gi = bc_remap(i0 - HB + ii, a.mx, a.bc[0], a.bc[1]);
-            const int gj = bc_remap(j0 - HB + jj, a.my, a.bc[2], a.bc[3]);
-            const size_t g = size_t(gi) * a.my + gj;
-            double Q[MEQN], f[MEQN], gg[MEQN];
+        // all of a thread's loads before its flux evaluations and stores
+        // (one memory round trip per block, not one per pass over the box)
+        constexpr int NIT = (PB + TI * TJ - 1) / (TI * TJ);
+        double Qv[NIT][MEQN];
 #pragma unroll
-            for (int m = 0; m < MEQN; m++) Q[m] = __ldg(q + m * a.plane + g);
-            Euler::flux(a.gamma, Q, f, gg);
+        for (int it = 0; it < NIT; it++) {
+            const int e = tid + it * TI * TJ;
+            if (e < PB) {
+                const int ii = e / BJ, jj = e - ii * BJ;
+                const int gi = bc_remap(i0 - HB + ii, a.mx, a.bc[0], a.bc[1]);
+                const int gj = bc_remap(j0 - HB + jj, a.my, a.bc[2], a.bc[3]);
+                const size_t g = size_t(gi) * a.my + gj;
 #pragma unroll
-            for (int m = 0; m < MEQN; m++) {
-                qb[m * PB + e] = Q[m];
-                fb[m * PB + e] = f[m];
-                gb[m * PB + e] = gg[m];
+                for (int m = 0; m < MEQN; m++) Qv[it][m] = __ldg(q + m * a.plane + g);
+            }
+        }
+#pragma unroll
+        for (int it = 0; it < NIT; it++) {
+            const int e = tid + it * TI * TJ;
+            if (e < PB) {
+                double f[MEQN], gg[MEQN];
+                Euler::flux(a.gamma, Qv[it], f, gg);
+#pragma unroll
+                for (int m = 0; m < MEQN; m++) {
+                    qb[m * PB + e] = Qv[it][m];
+                    fb[m * PB + e] = f[m];
+                    gb[m * PB + e] = gg[m];
+                }
             }
         }
         __syncthreads();
