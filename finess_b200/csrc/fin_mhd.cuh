@@ -509,11 +509,15 @@ __global__ void __launch_bounds__(Cfg::NT, Cfg::MINB) k_mhd_stage(const __grid_c
 
     // ---- phase 0: q_in on the tile + 3-cell cross halo, A3 on the tile +
     // 5-cell frame (periodic remap) ----
-    // All of a thread's loads (state and A3) are issued before its stores:
-    // one memory round trip per tile, not one per pass over the region.
+    // All of a thread's loads (the state, A3 of q_in, and A3 of the other
+    // stage operands for the update of phase 1b) are issued before its
+    // stores: one memory round trip per tile, not one per pass over a region.
+    // The operands' part of the A3 update, a1 A + a2 B (UpdateSoln.cpp:42-47),
+    // is kept in an[] for phase 1b to add bdt L to.
     {
         constexpr int NQI = (PQ + NT - 1) / NT, NAI = (Cfg::AI * AJ + NT - 1) / NT;
-        double vq[NQI][MHD_NQ], va[NAI];
+        constexpr int NHI = (Cfg::NI * NJ + NT - 1) / NT;
+        double vq[NQI][MHD_NQ], va[NAI], vab[NHI];
 #pragma unroll
         for (int it = 0; it < NQI; it++) {
             const int e = tid + it * NT;
@@ -538,6 +542,20 @@ __global__ void __launch_bounds__(Cfg::NT, Cfg::MINB) k_mhd_stage(const __grid_c
             }
         }
 #pragma unroll
+        for (int it = 0; it < NHI; it++) {
+            const int e = tid + it * NT;
+            const int ni = e / NJ, nj = e - ni * NJ;
+            const int ci = ni - HN, cj = nj - HN;   // tile frame
+            const bool xin = ci >= 0 && ci < TI, yin = cj >= 0 && cj < TJ;
+            if (e < Cfg::NI * NJ && (xin || yin)) {
+                const size_t g = 8 * a.plane + size_t(pwrap(i0 + ci, mx)) * my + pwrap(j0 + cj, my);
+                double v = 0.0;
+                if (a.A) v = a.a1 * __ldg(a.A + g);
+                if (a.B) v = v + a.a2 * __ldg(a.B + g);
+                vab[it] = v;
+            }
+        }
+#pragma unroll
         for (int it = 0; it < NQI; it++) {
             const int e = tid + it * NT;
             const int ii = e / RJ, jj = e - ii * RJ;
@@ -546,6 +564,14 @@ __global__ void __launch_bounds__(Cfg::NT, Cfg::MINB) k_mhd_stage(const __grid_c
 #pragma unroll
                 for (int m = 0; m < MHD_NQ; m++) qs[m * PQ + e] = R(vq[it][m]);
             }
+        }
+#pragma unroll
+        for (int it = 0; it < NHI; it++) {
+            const int e = tid + it * NT;
+            const int ni = e / NJ, nj = e - ni * NJ;
+            const int ci = ni - HN, cj = nj - HN;
+            const bool xin = ci >= 0 && ci < TI, yin = cj >= 0 && cj < TJ;
+            if (e < Cfg::NI * NJ && (xin || yin)) an[e] = vab[it];
         }
 #pragma unroll
         for (int it = 0; it < NAI; it++) {
@@ -658,13 +684,7 @@ __global__ void __launch_bounds__(Cfg::NT, Cfg::MINB) k_mhd_stage(const __grid_c
             const R u1 = qs[PQ + qe] * ir, u2 = qs[2 * PQ + qe] * ir;
             const double La = double(-u1 * R(0.5) * (xm + xp) - u2 * R(0.5) * (ym + yp)) +
                               (msx * 0.5 * double(xp - xm) + msy * 0.5 * double(yp - ym));
-            const int gi = pwrap(i0 + ci, mx);
-            const int gj = pwrap(j0 + cj, my);
-            const size_t g = 8 * a.plane + size_t(gi) * my + gj;
-            double v = 0.0;
-            if (a.A) v = a.a1 * __ldg(a.A + g);
-            if (a.B) v = v + a.a2 * __ldg(a.B + g);
-            an[e] = v + a.bdt * La;
+            an[e] = an[e] + a.bdt * La;   // a1 A + a2 B from phase 0
         }
     }
     __syncthreads();
