@@ -494,7 +494,7 @@ int launch_indicator(fin_mhd* s, int buf)
     MCK(cudaMemsetAsync(s->ind_count, 0, sizeof(unsigned long long), s->stream));
     MCK(cudaMemsetAsync(s->flags, 0, flag_words(s->p.mx, s->p.my) * sizeof(unsigned), s->stream));
     const long long tiles = (long long)((s->p.mx + ICfg::TI - 1) / ICfg::TI) * ((s->p.my + ICfg::TJ - 1) / ICfg::TJ);
-    const int grid = int(tiles < 148 * 2 ? tiles : 148 * 2);
+    const int grid = int(tiles < 148 * 3 ? tiles : 148 * 3);
     k_mhd_indicator<ICfg><<<grid, ICfg::NT, smem, s->stream>>>(ia);
     s->launches++;
     s->faces = (long long)(s->p.mx + 1) * s->p.my + (long long)s->p.mx * (s->p.my + 1);

@@ -218,7 +218,7 @@ struct MhdIndArgs {
 // at most 511 faces in four 128-row matrices; layer 1 and layer 2 on
 // tcgen05 with the accumulator in TMEM, every wait bounded.
 template <class Cfg>
-__global__ void __launch_bounds__(Cfg::NT, 2) k_mhd_indicator(const __grid_constant__ MhdIndArgs ia)
+__global__ void __launch_bounds__(Cfg::NT, 3) k_mhd_indicator(const __grid_constant__ MhdIndArgs ia)
 {
     using namespace mlp;
     const MhdArgs& a = ia.m;
