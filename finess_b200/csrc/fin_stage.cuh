@@ -209,7 +209,9 @@ __device__ __forceinline__ R linear_face(const R* f, int fstr, const R* q, int q
 // about 110 registers a thread, FP32 about 70.
 // Measured on B200 at 4096^2 (stage-kernel ms, FP64 / FP32): one block per
 // SM 5.81 / 2.71; two FP64 blocks (128 registers, ~200 B spilled to L1) and
-// three FP32 blocks 4.07 / 2.44.  More resident warps beat the spills.
+// three FP32 blocks 4.07 / 2.44.  More resident warps beat the spills, up to
+// a point: four FP32 blocks (64 registers, 236 B spilled) took 2.14 ms where
+// three took 2.06 (the current kernel).
 #ifndef FIN_MINB_F64
 #define FIN_MINB_F64 2
 #endif
